@@ -1,0 +1,635 @@
+// yannq oracle implementation -- TEST INFRASTRUCTURE ONLY (see oracle.hpp).
+#include "oracle.hpp"
+
+#include <numeric>
+#include <stdexcept>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+static inline int nthreads_or_default(int nt) {
+#ifdef _OPENMP
+    return nt > 0 ? nt : omp_get_max_threads();
+#else
+    (void)nt;
+    return 1;
+#endif
+}
+
+// ---------------------------------------------------------------------------
+double normal_pair(uint64_t seed, uint32_t idx, double* second) {
+    uint32_t x[4];
+    Philox4x32::draw(seed, idx, 0u, 0u, TAG_PARAM, x);
+    const double u1 = 1.0 - draw_u53(x[0], x[1]);  // (0, 1]
+    const double u2 = draw_u53(x[2], x[3]);
+    const double r = std::sqrt(-2.0 * std::log(u1));
+    const double ang = 6.283185307179586476925286766559 * u2;
+    if (second) *second = r * std::sin(ang);
+    return r * std::cos(ang);
+}
+
+void init_params(int n, int m, bool useBias, uint64_t seed, double sd, cd* p) {
+    // Machines/RBM.hpp:325-349: a, b (if bias) then W(i, j) with i (hidden) fastest.
+    uint32_t e = 0;
+    auto draw = [&](cd& out) {
+        double im;
+        double re = normal_pair(seed, e++, &im);
+        out = cd{sd * re, sd * im};
+    };
+    const size_t nm = size_t(n) * m;
+    if (useBias) {
+        for (int i = 0; i < n; ++i) draw(p[nm + i]);
+        for (int j = 0; j < m; ++j) draw(p[nm + n + j]);
+    }
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < m; ++j) draw(p[size_t(i) * m + j]);
+}
+
+// ---------------------------------------------------------------------------
+static inline int right_of(const Ham& H, int i) {
+    if (H.kind == 2) {
+        int x = i % H.lx, y = i / H.lx;
+        return (x + 1) % H.lx + H.lx * y;
+    }
+    return (i + 1) % H.n;
+}
+static inline int down_of(const Ham& H, int i) {
+    int x = i % H.lx, y = i / H.lx;
+    return x + H.lx * ((y + 1) % H.ly);
+}
+
+double ham_enumerate(const Ham& H, const int8_t* s, std::vector<FlipTerm>& terms) {
+    terms.clear();
+    double diag = 0.;
+    for (int i = 0; i < H.n; ++i) {
+        if (H.kind == 0) {  // TFIsing.hpp:31-36
+            diag += H.J * s[i] * s[(i + 1) % H.n];
+            terms.push_back({uint64_t(1) << i, H.h});
+        } else if (H.kind == 1) {  // XXZ.hpp:40-47
+            int j = (i + 1) % H.n;
+            int zz = s[i] * s[j];
+            diag += H.J * H.h * zz;
+            terms.push_back({(uint64_t(1) << i) | (uint64_t(1) << j), H.sign * H.J * (1 - zz)});
+        } else {  // TFIsing2D: right and down bonds of every site, then the field
+            diag += H.J * s[i] * s[right_of(H, i)];
+            diag += H.J * s[i] * s[down_of(H, i)];
+            terms.push_back({uint64_t(1) << i, H.h});
+        }
+    }
+    return diag;
+}
+
+std::map<uint64_t, double> ham_column(const Ham& H, uint64_t col) {
+    std::map<uint64_t, double> res;
+    auto z = [&](int i) { return 1 - 2 * int((col >> i) & 1u); };
+    for (int i = 0; i < H.n; ++i) {
+        if (H.kind == 0) {  // TFIsing.hpp:53-65
+            res[col ^ (uint64_t(1) << i)] += H.h;
+            res[col] += H.J * z(i) * z((i + 1) % H.n);
+        } else if (H.kind == 1) {  // XXZ.hpp:51-64
+            int j = (i + 1) % H.n;
+            int zz = z(i) * z(j);
+            uint64_t x = (uint64_t(1) << i) | (uint64_t(1) << j);
+            res[col] += H.J * H.h * zz;
+            res[col ^ x] += H.sign * H.J * (1 - zz);
+        } else {
+            res[col ^ (uint64_t(1) << i)] += H.h;
+            res[col] += H.J * z(i) * z(right_of(H, i)) + H.J * z(i) * z(down_of(H, i));
+        }
+    }
+    return res;
+}
+
+cd ham_eloc(const Ham& H, const RBM& q, const int8_t* s, const cd* th) {
+    cd acc = 0.;
+    for (int i = 0; i < H.n; ++i) {
+        if (H.kind == 0) {
+            acc += H.J * s[i] * s[(i + 1) % H.n];
+            acc += H.h * std::exp(q.logRatio1(s, th, i));
+        } else if (H.kind == 1) {
+            int j = (i + 1) % H.n;
+            int zz = s[i] * s[j];
+            acc += H.J * H.h * zz;
+            acc += H.sign * H.J * (1 - zz) * std::exp(q.logRatio2(s, th, i, j));
+        } else {
+            acc += H.J * s[i] * s[right_of(H, i)];
+            acc += H.J * s[i] * s[down_of(H, i)];
+            acc += H.h * std::exp(q.logRatio1(s, th, i));
+        }
+    }
+    return acc;
+}
+
+// ---------------------------------------------------------------------------
+void random_sigma(int n, int nup, uint64_t seed, uint32_t epoch, uint32_t chain, int8_t* s) {
+    uint32_t x[4];
+    if (nup < 0) {  // Utilities/Utility.hpp:63-74
+        for (int i = 0; i < n; ++i) {
+            Philox4x32::draw(seed, uint32_t(i), epoch, chain, TAG_INIT, x);
+            s[i] = (x[0] & 1u) ? int8_t(-1) : int8_t(1);
+        }
+        return;
+    }
+    // Utilities/Utility.hpp:77-88: nup entries -1, the rest +1, then shuffled
+    for (int i = 0; i < n; ++i) s[i] = (i < nup) ? int8_t(-1) : int8_t(1);
+    for (int i = n - 1; i >= 1; --i) {
+        Philox4x32::draw(seed, uint32_t(i), epoch, chain, TAG_SHUF, x);
+        int j = int(draw_site(x[0], uint32_t(i + 1)));
+        std::swap(s[i], s[j]);
+    }
+}
+
+void sample(const RBM& q, const SampleSpec& sp, int8_t* chain_sigma, int8_t* out_sigma, cd* out_theta,
+            uint64_t* acc, int nthreads) {
+    const int n = q.n, m = q.m;
+    const int L = sp.sweep_len > 0 ? sp.sweep_len : n;
+    const int total = sp.n_discard + sp.n_sweeps;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads_or_default(nthreads))
+    for (int c = 0; c < sp.n_chains; ++c) {
+        std::vector<int8_t> s(n);
+        std::vector<cd> th(m);
+        int8_t* cs = chain_sigma + size_t(c) * n;
+        if (sp.reinit)
+            random_sigma(n, sp.nup, sp.seed, sp.epoch, uint32_t(c), s.data());
+        else
+            std::copy(cs, cs + n, s.begin());
+        q.theta(s.data(), th.data());
+        uint64_t nacc = 0;
+        uint32_t x[4];
+        for (int sw = 0; sw < total; ++sw) {
+            for (int p = 0; p < L; ++p) {
+                const uint32_t g = uint32_t(sw) * uint32_t(L) + uint32_t(p);
+                Philox4x32::draw(sp.seed, g, sp.epoch, uint32_t(c), TAG_SWEEP, x);
+                const double u = draw_u53(x[2], x[3]);
+                if (sp.move == MOVE_LOCAL) {  // LocalSweeper.hpp:42-52
+                    int k = int(draw_site(x[0], uint32_t(n)));
+                    double pr = std::min(1.0, std::exp(1.0 * 2.0 * q.logRatio1(s.data(), th.data(), k).real()));
+                    if (u < pr) {
+                        q.flip1(s.data(), th.data(), k);
+                        ++nacc;
+                    }
+                } else {  // SwapSweeper.hpp:39-56 (any pair) or its neighbour-pair variant
+                    int k = int(draw_site(x[0], uint32_t(n)));
+                    int l = (sp.move == MOVE_EXCHANGE_ANY) ? int(draw_site(x[1], uint32_t(n))) : (k + 1) % n;
+                    if (s[k] == s[l]) continue;
+                    double pr =
+                        std::min(1.0, std::exp(1.0 * 2.0 * q.logRatio2(s.data(), th.data(), k, l).real()));
+                    if (u < pr) {
+                        q.flip2(s.data(), th.data(), k, l);
+                        ++nacc;
+                    }
+                }
+            }
+            if (sw >= sp.n_discard) {  // SamplerMT.hpp:165-173 (recorded in (sweep, chain) order)
+                size_t idx = size_t(sw - sp.n_discard) * sp.n_chains + c;
+                std::copy(s.begin(), s.end(), out_sigma + idx * n);
+                std::copy(th.begin(), th.end(), out_theta + idx * m);
+            }
+        }
+        std::copy(s.begin(), s.end(), cs);
+        if (acc) acc[c] = nacc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+int cholesky_lower(int nn, cd* A) {
+    for (int j = 0; j < nn; ++j) {
+        cd* rj = A + size_t(j) * nn;
+        double d = rj[j].real();
+        for (int k = 0; k < j; ++k) d -= std::norm(rj[k]);
+        if (!(d > 0.0)) return j + 1;
+        const double ljj = std::sqrt(d);
+        rj[j] = ljj;
+#pragma omp parallel for schedule(static)
+        for (int i = j + 1; i < nn; ++i) {
+            cd* ri = A + size_t(i) * nn;
+            cd acc = ri[j];
+            for (int k = 0; k < j; ++k) acc -= ri[k] * std::conj(rj[k]);
+            ri[j] = acc / ljj;
+        }
+    }
+    return 0;
+}
+
+void cholesky_solve(int nn, const cd* L, cd* x) {
+    for (int i = 0; i < nn; ++i) {  // L y = b
+        const cd* ri = L + size_t(i) * nn;
+        cd acc = x[i];
+        for (int k = 0; k < i; ++k) acc -= ri[k] * x[k];
+        x[i] = acc / ri[i].real();
+    }
+    for (int i = nn - 1; i >= 0; --i) {  // L^H x = y
+        cd acc = x[i];
+        for (int k = i + 1; k < nn; ++k) acc -= std::conj(L[size_t(k) * nn + i]) * x[k];
+        x[i] = acc / L[size_t(i) * nn + i].real();
+    }
+}
+
+template <class ApplyFn>
+int conjugate_gradient(size_t dim, ApplyFn&& apply, const cd* b, cd* x, double tol, int maxit, double* relres) {
+    std::vector<cd> r(b, b + dim), p(dim), tmp(dim);
+    std::fill(x, x + dim, cd{});
+    auto dotc = [&](const std::vector<cd>& u, const std::vector<cd>& v) {
+        cd s = 0.;
+        for (size_t i = 0; i < dim; ++i) s += std::conj(u[i]) * v[i];
+        return s;
+    };
+    double rhsNorm2 = 0.;
+    for (size_t i = 0; i < dim; ++i) rhsNorm2 += std::norm(b[i]);
+    if (rhsNorm2 == 0.) {
+        if (relres) *relres = 0.;
+        return 0;
+    }
+    const double threshold = tol * tol * rhsNorm2;
+    double residualNorm2 = rhsNorm2;
+    if (residualNorm2 < threshold) {
+        if (relres) *relres = std::sqrt(residualNorm2 / rhsNorm2);
+        return 0;
+    }
+    p = r;
+    double absNew = dotc(r, p).real();
+    int i = 0;
+    while (i < maxit) {
+        apply(p.data(), tmp.data());
+        cd alpha = absNew / dotc(p, tmp);
+        for (size_t k = 0; k < dim; ++k) {
+            x[k] += alpha * p[k];
+            r[k] -= alpha * tmp[k];
+        }
+        residualNorm2 = 0.;
+        for (size_t k = 0; k < dim; ++k) residualNorm2 += std::norm(r[k]);
+        if (residualNorm2 < threshold) break;
+        double absOld = absNew;
+        absNew = dotc(r, r).real();
+        double beta = absNew / absOld;
+        for (size_t k = 0; k < dim; ++k) p[k] = r[k] + beta * p[k];
+        ++i;
+    }
+    if (relres) *relres = std::sqrt(residualNorm2 / rhsNorm2);
+    return i;
+}
+
+SRResult sr_step(const RBM& q, const Ham& H, int ns, const int8_t* sig, const cd* th, double shift, int mode,
+                 int solver, double cgtol, int nthreads) {
+    const int nt = nthreads_or_default(nthreads);
+    const size_t P = q.dim();
+    SRResult R;
+    std::vector<cd> O(size_t(ns) * P);
+    R.elocs.resize(ns);
+    // GroundState/utils.hpp:12-51 (constructDelta) and :108-126 (constructObs -> Energy::eachSample)
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (int s = 0; s < ns; ++s) {
+        q.logDeriv(sig + size_t(s) * q.n, th + size_t(s) * q.m, O.data() + size_t(s) * P);
+        R.elocs[s] = ham_eloc(H, q, sig + size_t(s) * q.n, th + size_t(s) * q.m);
+    }
+    // Observables/Energy.hpp:53-58
+    double e = 0., e2 = 0.;
+    cd emean = 0.;
+    for (int s = 0; s < ns; ++s) {
+        e += R.elocs[s].real();
+        e2 += R.elocs[s].real() * R.elocs[s].real();
+        emean += R.elocs[s];
+    }
+    e /= ns;
+    e2 /= ns;
+    emean /= double(ns);
+    R.energy = e;
+    R.energy_var = e2 - e * e;
+    // SRMat.hpp:97-102: column mean, centring, energyGrad = O~^H E / Ns
+    R.oloc.assign(P, cd{});
+    for (int s = 0; s < ns; ++s)
+        for (size_t p = 0; p < P; ++p) R.oloc[p] += O[size_t(s) * P + p];
+    for (size_t p = 0; p < P; ++p) R.oloc[p] /= double(ns);
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (int s = 0; s < ns; ++s)
+        for (size_t p = 0; p < P; ++p) O[size_t(s) * P + p] -= R.oloc[p];
+    R.grad.assign(P, cd{});
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (long long p = 0; p < (long long)P; ++p) {
+        cd acc = 0.;
+        for (int s = 0; s < ns; ++s) acc += std::conj(O[size_t(s) * P + p]) * R.elocs[s];
+        R.grad[p] = acc / double(ns);
+    }
+    R.v.assign(P, cd{});
+    if (mode == SR_S) {
+        if (solver == SOLVE_LLT) {  // SRMat.hpp:142-149 corrMat + :231-237 solveExact
+            std::vector<cd> S(P * P);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+            for (long long a = 0; a < (long long)P; ++a)
+                for (size_t b = 0; b <= size_t(a); ++b) {
+                    cd acc = 0.;
+                    for (int s = 0; s < ns; ++s) acc += std::conj(O[size_t(s) * P + a]) * O[size_t(s) * P + b];
+                    S[size_t(a) * P + b] = acc / double(ns);
+                }
+            for (size_t a = 0; a < P; ++a) S[a * P + a] += shift;
+            R.status = cholesky_lower(int(P), S.data());
+            if (R.status) return R;
+            R.v = R.grad;
+            cholesky_solve(int(P), S.data(), R.v.data());
+        } else {  // SRMat.hpp:170-189 apply + :197-208 solveCG
+            auto apply = [&](const cd* x, cd* y) {
+                std::vector<cd> r(ns);
+#pragma omp parallel for schedule(static) num_threads(nt)
+                for (int s = 0; s < ns; ++s) {
+                    cd acc = 0.;
+                    for (size_t p = 0; p < P; ++p) acc += O[size_t(s) * P + p] * x[p];
+                    r[s] = acc / double(ns);
+                }
+#pragma omp parallel for schedule(static) num_threads(nt)
+                for (long long p = 0; p < (long long)P; ++p) {
+                    cd acc = 0.;
+                    for (int s = 0; s < ns; ++s) acc += std::conj(O[size_t(s) * P + p]) * r[s];
+                    y[p] = acc + shift * x[p];
+                }
+            };
+            R.cg_iters = conjugate_gradient(P, apply, R.grad.data(), R.v.data(), cgtol, int(2 * P), &R.cg_relres);
+        }
+    } else {  // sample-space dual (push-through identity); no reference counterpart
+        std::vector<cd> T(size_t(ns) * ns);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+        for (int a = 0; a < ns; ++a)
+            for (int b = 0; b <= a; ++b) {
+                cd acc = 0.;
+                const cd* ra = O.data() + size_t(a) * P;
+                const cd* rb = O.data() + size_t(b) * P;
+                for (size_t p = 0; p < P; ++p) acc += ra[p] * std::conj(rb[p]);
+                T[size_t(a) * ns + b] = acc / double(ns);
+            }
+        for (int a = 0; a < ns; ++a) T[size_t(a) * ns + a] += shift;
+        R.status = cholesky_lower(ns, T.data());
+        if (R.status) return R;
+        std::vector<cd> y(ns);
+        for (int s = 0; s < ns; ++s) y[s] = (R.elocs[s] - emean) / double(ns);
+        cholesky_solve(ns, T.data(), y.data());
+#pragma omp parallel for schedule(static) num_threads(nt)
+        for (long long p = 0; p < (long long)P; ++p) {
+            cd acc = 0.;
+            for (int s = 0; s < ns; ++s) acc += std::conj(O[size_t(s) * P + p]) * y[s];
+            R.v[p] = acc;
+        }
+    }
+    return R;
+}
+
+// ---------------------------------------------------------------------------
+std::vector<uint64_t> basis_full(int n) {
+    std::vector<uint64_t> b(size_t(1) << n);
+    std::iota(b.begin(), b.end(), uint64_t(0));
+    return b;
+}
+
+std::vector<uint64_t> basis_jz(int n, int nup) {
+    // Basis/BasisJz.hpp:25-30: next integer with the same popcount (Gosper's hack)
+    std::vector<uint64_t> b;
+    if (nup == 0) {
+        b.push_back(0);
+        return b;
+    }
+    uint64_t v = (uint64_t(1) << nup) - 1;
+    const uint64_t last = v << (n - nup);
+    while (true) {
+        b.push_back(v);
+        if (v == last) break;
+        uint64_t t = v | (v - 1);
+        v = (t + 1) | (((~t & (t + 1)) - 1) >> (__builtin_ctzll(v) + 1));
+    }
+    return b;
+}
+
+namespace {
+struct CSR {
+    std::vector<size_t> ptr;
+    std::vector<uint32_t> col;
+    std::vector<double> val;
+};
+// ED/ConstructSparseMat.hpp:32-57: row idx gets the column map of basis[idx]
+// restricted to the basis via lower_bound (duplicates summed).
+CSR build_csr(const Ham& H, const std::vector<uint64_t>& basis, int nt) {
+    const size_t dim = basis.size();
+    std::vector<std::vector<std::pair<uint32_t, double>>> rows(dim);
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nt)
+    for (long long idx = 0; idx < (long long)dim; ++idx) {
+        auto mcol = ham_column(H, basis[idx]);
+        auto it = basis.begin();
+        std::map<uint32_t, double> acc;
+        for (auto& kv : mcol) {
+            it = std::lower_bound(it, basis.end(), kv.first);
+            if (it == basis.end()) break;
+            acc[uint32_t(it - basis.begin())] += kv.second;
+        }
+        rows[idx].assign(acc.begin(), acc.end());
+    }
+    CSR A;
+    A.ptr.resize(dim + 1, 0);
+    for (size_t i = 0; i < dim; ++i) A.ptr[i + 1] = A.ptr[i] + rows[i].size();
+    A.col.resize(A.ptr[dim]);
+    A.val.resize(A.ptr[dim]);
+    for (size_t i = 0; i < dim; ++i)
+        for (size_t k = 0; k < rows[i].size(); ++k) {
+            A.col[A.ptr[i] + k] = rows[i][k].first;
+            A.val[A.ptr[i] + k] = rows[i][k].second;
+        }
+    return A;
+}
+}  // namespace
+
+ExactResult exact_sr(const RBM& q, const Ham& H, const std::vector<uint64_t>& basis, int nthreads) {
+    const int nt = nthreads_or_default(nthreads);
+    const size_t dim = basis.size(), P = q.dim();
+    ExactResult X;
+    std::vector<cd> psi(dim);
+    std::vector<cd> O(dim * P);
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (long long s = 0; s < (long long)dim; ++s) {
+        std::vector<int8_t> sg(q.n);
+        std::vector<cd> th(q.m);
+        for (int i = 0; i < q.n; ++i) sg[i] = ((basis[s] >> i) & 1u) ? int8_t(-1) : int8_t(1);
+        q.theta(sg.data(), th.data());
+        psi[s] = q.coeff(sg.data(), th.data());
+        q.logDeriv(sg.data(), th.data(), O.data() + size_t(s) * P);
+    }
+    double nrm = 0.;
+    for (auto& v : psi) nrm += std::norm(v);
+    nrm = std::sqrt(nrm);
+    for (auto& v : psi) v /= nrm;
+    CSR A = build_csr(H, basis, nt);
+    std::vector<cd> k(dim);
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (long long i = 0; i < (long long)dim; ++i) {
+        cd acc = 0.;
+        for (size_t e = A.ptr[i]; e < A.ptr[i + 1]; ++e) acc += A.val[e] * psi[A.col[e]];
+        k[i] = acc;
+    }
+    cd t = 0.;
+    double kk = 0.;
+    for (size_t i = 0; i < dim; ++i) {
+        t += std::conj(psi[i]) * k[i];
+        kk += std::norm(k[i]);
+    }
+    X.energy = t.real();
+    X.energy_var = kk - X.energy * X.energy;
+    X.oloc.assign(P, cd{});
+    X.grad.assign(P, cd{});
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (long long p = 0; p < (long long)P; ++p) {
+        cd ol = 0., g = 0.;
+        for (size_t s = 0; s < dim; ++s) {
+            const cd o = O[s * P + p];
+            ol += std::norm(psi[s]) * o;
+            g += std::conj(psi[s] * o) * k[s];
+        }
+        X.oloc[p] = ol;
+        X.grad[p] = g;
+    }
+    for (size_t p = 0; p < P; ++p) X.grad[p] -= t * std::conj(X.oloc[p]);
+    X.S.assign(P * P, cd{});
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+    for (long long a = 0; a < (long long)P; ++a)
+        for (size_t b = 0; b < P; ++b) {
+            cd acc = 0.;
+            for (size_t s = 0; s < dim; ++s) acc += std::norm(psi[s]) * std::conj(O[s * P + a]) * O[s * P + b];
+            X.S[size_t(a) * P + b] = acc - std::conj(X.oloc[a]) * X.oloc[b];
+        }
+    return X;
+}
+
+// Lanczos with full reorthogonalisation; smallest Ritz value by Sturm bisection.
+static double tridiag_min_eig(const std::vector<double>& al, const std::vector<double>& be) {
+    const int k = int(al.size());
+    double lo = 1e300, hi = -1e300;
+    for (int i = 0; i < k; ++i) {
+        double r = (i > 0 ? std::fabs(be[i - 1]) : 0.) + (i + 1 < k ? std::fabs(be[i]) : 0.);
+        lo = std::min(lo, al[i] - r);
+        hi = std::max(hi, al[i] + r);
+    }
+    auto count_below = [&](double x) {
+        int c = 0;
+        double d = 1.;
+        for (int i = 0; i < k; ++i) {
+            double b2 = i > 0 ? be[i - 1] * be[i - 1] : 0.;
+            d = al[i] - x - (i > 0 ? b2 / d : 0.);
+            if (d == 0.) d = 1e-300;
+            if (d < 0) ++c;
+        }
+        return c;
+    };
+    for (int it = 0; it < 200; ++it) {
+        double mid = 0.5 * (lo + hi);
+        if (count_below(mid) >= 1)
+            hi = mid;
+        else
+            lo = mid;
+        if (hi - lo < 1e-14 * std::max(1.0, std::fabs(mid))) break;
+    }
+    return 0.5 * (lo + hi);
+}
+
+double ed_ground_energy(const Ham& H, const std::vector<uint64_t>& basis, int maxit, int nthreads) {
+    const int nt = nthreads_or_default(nthreads);
+    CSR A = build_csr(H, basis, nt);
+    const size_t dim = basis.size();
+    if (dim == 1) return A.val.empty() ? 0. : A.val[0];
+    maxit = std::min<int>(maxit, int(dim));
+    std::vector<std::vector<double>> V;
+    std::vector<double> v(dim), w(dim), al, be;
+    double nrm = 0.;
+    for (size_t i = 0; i < dim; ++i) {
+        v[i] = normal_pair(0x4c414e43ULL, uint32_t(i), nullptr);
+        nrm += v[i] * v[i];
+    }
+    nrm = std::sqrt(nrm);
+    for (auto& x : v) x /= nrm;
+    double prev = 0.;
+    for (int it = 0; it < maxit; ++it) {
+        V.push_back(v);
+#pragma omp parallel for schedule(static) num_threads(nt)
+        for (long long i = 0; i < (long long)dim; ++i) {
+            double acc = 0.;
+            for (size_t e = A.ptr[i]; e < A.ptr[i + 1]; ++e) acc += A.val[e] * v[A.col[e]];
+            w[i] = acc;
+        }
+        double a = 0.;
+        for (size_t i = 0; i < dim; ++i) a += w[i] * v[i];
+        al.push_back(a);
+        for (int pass = 0; pass < 2; ++pass)
+            for (auto& u : V) {
+                double c = 0.;
+                for (size_t i = 0; i < dim; ++i) c += u[i] * w[i];
+                for (size_t i = 0; i < dim; ++i) w[i] -= c * u[i];
+            }
+        double b = 0.;
+        for (size_t i = 0; i < dim; ++i) b += w[i] * w[i];
+        b = std::sqrt(b);
+        double cur = tridiag_min_eig(al, be);
+        if ((it > 10 && std::fabs(cur - prev) < 1e-13 * std::max(1.0, std::fabs(cur))) || b < 1e-12) return cur;
+        prev = cur;
+        be.push_back(b);
+        for (size_t i = 0; i < dim; ++i) v[i] = w[i] / b;
+    }
+    return tridiag_min_eig(al, std::vector<double>(be.begin(), be.begin() + (al.size() - 1)));
+}
+
+// ---------------------------------------------------------------------------
+namespace {
+struct FFActs {
+    std::vector<double> in, z1, a1, z2;
+};
+void ff_fwd(const FFNet& f, const int8_t* s, FFActs& A) {
+    const int L = f.L, C = f.conv_out, K = f.conv_k, F = f.fc_out, I = L * C;
+    A.in.assign(L, 0.);
+    for (int r = 0; r < L; ++r) A.in[r] = double(s[r]);
+    // layers/Conv1D.hpp:144-171 (inChannels = 1, stride 1, no bias)
+    A.z1.assign(I, 0.);
+    for (int oc = 0; oc < C; ++oc)
+        for (int r = 0; r < L; ++r)
+            for (int ki = 0; ki < K; ++ki)
+                A.z1[r + oc * L] += f.p[ki + size_t(K) * oc] * A.in[(r + ki - K / 2 + L) % L];
+    A.a1.resize(I);
+    for (int i = 0; i < I; ++i) A.a1[i] = logCosh(A.z1[i]);  // activations.hpp:83-87
+    // layers/FullyConnected.hpp:150-157: z = W^T x, W (I x F) column-major
+    const double* Wfc = f.p + size_t(K) * C;
+    A.z2.assign(F, 0.);
+    for (int o = 0; o < F; ++o) {
+        double acc = 0.;
+        for (int i = 0; i < I; ++i) acc += Wfc[i + size_t(I) * o] * A.a1[i];
+        A.z2[o] = acc;
+    }
+}
+}  // namespace
+
+double ff_forward(const FFNet& f, const int8_t* s) {
+    FFActs A;
+    ff_fwd(f, s, A);
+    double r = 0.;
+    for (double z : A.z2) r += logCosh(z);  // LnCosh then Sum (= fc_out * Mean, layers/Mean.hpp:92-103)
+    return r;
+}
+
+void ff_backward(const FFNet& f, const int8_t* s, double* der) {
+    // Machines/FeedForward.hpp:186-205 with dout = 1 at the output
+    FFActs A;
+    ff_fwd(f, s, A);
+    const int L = f.L, C = f.conv_out, K = f.conv_k, F = f.fc_out, I = L * C;
+    std::vector<double> d2(F), d1(I, 0.), dz1(I);
+    for (int o = 0; o < F; ++o) d2[o] = 1.0 * std::tanh(A.z2[o]);  // Sum, then LnCosh Jacobian
+    const double* Wfc = f.p + size_t(K) * C;
+    double* der_fc = der + size_t(K) * C;
+    for (int o = 0; o < F; ++o)  // FullyConnected.hpp:170-178
+        for (int i = 0; i < I; ++i) der_fc[i + size_t(I) * o] = A.a1[i] * d2[o];
+    for (int i = 0; i < I; ++i) {
+        double acc = 0.;
+        for (int o = 0; o < F; ++o) acc += Wfc[i + size_t(I) * o] * d2[o];
+        d1[i] = acc;
+    }
+    for (int i = 0; i < I; ++i) dz1[i] = d1[i] * std::tanh(A.z1[i]);
+    for (int k = 0; k < K * C; ++k) der[k] = 0.;  // Conv1D.hpp:197-212
+    for (int oc = 0; oc < C; ++oc)
+        for (int r = 0; r < L; ++r)
+            for (int ki = 0; ki < K; ++ki)
+                der[ki + size_t(K) * oc] += A.in[(r + ki - K / 2 + L) % L] * dz1[r + oc * L];
+}
+
+}  // namespace orc

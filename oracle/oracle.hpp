@@ -1,0 +1,247 @@
+// yannq oracle: a CPU restatement of the reference's VMC hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  Nothing in the product library (libyannq_b200.so)
+// links, includes or calls this code; it is the checker used by tests/, by the
+// smoke check and by the CPU-baseline leg of bench.py.
+//
+// Each routine restates the reference algorithm named beside it (paths are
+// relative to the reference project root).  The reference itself cannot be
+// built here (it needs Eigen3, TBB, MKL, cereal, nlohmann/json), so this
+// restatement stands in for it; its own fidelity is pinned by the reference's
+// known-answer and property tests re-expressed in tests/test_oracle_*.py, by
+// exact diagonalisation and by the closed-form energy of the periodic
+// transverse-field Ising chain.
+//
+// Conventions (all follow the reference):
+//   * spins sigma_i = +-1 stored as int8; bit i of a basis index set <=> sigma_i = -1
+//     (Utilities/Utility.hpp:91-110)
+//   * RBM parameters p = [W column-major (m x n) | a (n) | b (m)]
+//     (Machines/RBM.hpp:271-291)
+//   * complex numbers are interleaved (re, im) doubles at the C boundary.
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "philox.hpp"
+
+namespace orc {
+
+using cd = std::complex<double>;
+
+// ---------------------------------------------------------------------------
+// Utilities/Utility.hpp:14-24 -- stable log(cosh(x)) for real x
+inline double logCosh(double x) {
+    const double xp = std::fabs(x);
+    if (xp <= 12.) return std::log(std::cosh(xp));
+    return xp - std::log(2.);
+}
+// Utilities/Utility.hpp:27-37 -- complex: logCosh(Re) + log(cos(Im) + i tanh(Re) sin(Im))
+inline cd logCosh(cd x) {
+    const double xr = x.real(), xi = x.imag();
+    cd res = logCosh(xr);
+    res += std::log(cd{std::cos(xi), std::tanh(xr) * std::sin(xi)});
+    return res;
+}
+
+// ---------------------------------------------------------------------------
+// Machines/RBM.hpp -- a read-only view of an RBM<complex<double>>.
+struct RBM {
+    int n = 0, m = 0;
+    bool useBias = true;
+    const cd* p = nullptr;  // [W col-major | a | b]
+
+    inline cd W(int j, int i) const { return p[size_t(i) * m + j]; }  // W(j,i), j<m, i<n
+    inline cd A(int i) const { return useBias ? p[size_t(n) * m + i] : cd{}; }
+    inline cd B(int j) const { return useBias ? p[size_t(n) * m + n + j] : cd{}; }
+    inline size_t dim() const { return useBias ? size_t(n) * m + n + m : size_t(n) * m; }
+
+    // RBM.hpp:137-141  theta = W sigma + b.  Summation order (i ascending, then
+    // + b) is fixed so that the device sampler can reproduce theta bit for bit.
+    void theta(const int8_t* s, cd* th) const {
+        for (int j = 0; j < m; ++j) {
+            cd acc = 0.;
+            for (int i = 0; i < n; ++i) acc += W(j, i) * double(s[i]);
+            th[j] = acc + B(j);
+        }
+    }
+    // RBM.hpp:367-378
+    cd logCoeff(const int8_t* s, const cd* th) const {
+        cd r = 0.;
+        for (int i = 0; i < n; ++i) r += A(i) * double(s[i]);
+        for (int j = 0; j < m; ++j) r += logCosh(th[j]);
+        return r;
+    }
+    // RBM.hpp:380-388  psi = exp(a.sigma) prod_j cosh(theta_j)
+    cd coeff(const int8_t* s, const cd* th) const {
+        cd r = 0.;
+        for (int i = 0; i < n; ++i) r += A(i) * double(s[i]);
+        cd prod = 1.;
+        for (int j = 0; j < m; ++j) prod *= std::cosh(th[j]);
+        return std::exp(r) * prod;
+    }
+    // RBM.hpp:390-406  O = [sigma_i tanh(theta_j) (i*m+j) | sigma | tanh(theta)]
+    void logDeriv(const int8_t* s, const cd* th, cd* out) const {
+        std::vector<cd> t(m);
+        for (int j = 0; j < m; ++j) t[j] = std::tanh(th[j]);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < m; ++j) out[size_t(i) * m + j] = double(s[i]) * t[j];
+        if (!useBias) return;
+        for (int i = 0; i < n; ++i) out[size_t(n) * m + i] = double(s[i]);
+        for (int j = 0; j < m; ++j) out[size_t(n) * m + n + j] = t[j];
+    }
+
+    // States/RBMState.hpp:48-63  log psi(sigma^k) - log psi(sigma)
+    cd logRatio1(const int8_t* s, const cd* th, int k) const {
+        cd res = -2.0 * A(k) * double(s[k]);
+        for (int j = 0; j < m; ++j) res += logCosh(th[j] - 2.0 * double(s[k]) * W(j, k)) - logCosh(th[j]);
+        return res;
+    }
+    // States/RBMState.hpp:78-94
+    cd logRatio2(const int8_t* s, const cd* th, int k, int l) const {
+        cd res = -2.0 * A(k) * double(s[k]) - 2.0 * A(l) * double(s[l]);
+        for (int j = 0; j < m; ++j) {
+            cd t = th[j] - 2.0 * double(s[k]) * W(j, k) - 2.0 * double(s[l]) * W(j, l);
+            res += logCosh(t) - logCosh(th[j]);
+        }
+        return res;
+    }
+    // States/RBMState.hpp:108-127
+    cd logRatioVec(const int8_t* s, const cd* th, int nf, const int* f) const {
+        cd res = 0.;
+        for (int e = 0; e < nf; ++e) res -= 2.0 * A(f[e]) * double(s[f[e]]);
+        for (int j = 0; j < m; ++j) {
+            cd t = th[j];
+            for (int e = 0; e < nf; ++e) t -= 2.0 * double(s[f[e]]) * W(j, f[e]);
+            res += logCosh(t) - logCosh(th[j]);
+        }
+        return res;
+    }
+    // States/RBMState.hpp:248-255  theta first, then sigma
+    void flip1(int8_t* s, cd* th, int k) const {
+        for (int j = 0; j < m; ++j) th[j] -= 2.0 * double(s[k]) * W(j, k);
+        s[k] = int8_t(-s[k]);
+    }
+    // States/RBMState.hpp:257-266
+    void flip2(int8_t* s, cd* th, int k, int l) const {
+        for (int j = 0; j < m; ++j) th[j] += -2.0 * double(s[k]) * W(j, k) - 2.0 * double(s[l]) * W(j, l);
+        s[k] = int8_t(-s[k]);
+        s[l] = int8_t(-s[l]);
+    }
+    // States/RBMState.hpp:268-281
+    void flipVec(int8_t* s, cd* th, int nf, const int* f) const {
+        for (int e = 0; e < nf; ++e)
+            for (int j = 0; j < m; ++j) th[j] -= 2.0 * double(s[f[e]]) * W(j, f[e]);
+        for (int e = 0; e < nf; ++e) s[f[e]] = int8_t(-s[f[e]]);
+    }
+};
+
+// Machines/RBM.hpp:325-349 -- draw order a[0..n), b[0..m), then W column by column,
+// each complex entry (re, im).  The normal draws come from Philox + Box-Muller
+// (reference: std::normal_distribution over an unseeded engine).
+void init_params(int n, int m, bool useBias, uint64_t seed, double sd, cd* p);
+double normal_pair(uint64_t seed, uint32_t idx, double* second);
+
+// ---------------------------------------------------------------------------
+// Hamiltonians.  kind: 0 = TFIsing (1D ring, Hamiltonians/TFIsing.hpp),
+// 1 = XXZ (1D ring, Hamiltonians/XXZ.hpp), 2 = TFIsing2D (periodic Lx x Ly; no
+// reference counterpart, built on the same duck-typed concept).
+struct Ham {
+    int kind = 0;
+    int n = 0;        // number of sites
+    int lx = 0, ly = 0;  // 2D extents (kind 2)
+    double J = 0., h = 0.;  // TFI: J zz coupling, h field.  XXZ: J, h = Delta
+    double sign = 1.;       // XXZ sign rule (-1 when signRule)
+};
+
+// Off-diagonal flip enumeration of the state form (the "mock state" technique of
+// Tests/HamiltonianHelper.hpp:44-92): each requested ratio becomes a (mask, coeff)
+// entry; the diagonal sum is returned separately.  Entries with coefficient 0 are
+// kept, as the reference state form requests them.
+struct FlipTerm {
+    uint64_t mask;
+    double coeff;
+};
+double ham_enumerate(const Ham& H, const int8_t* s, std::vector<FlipTerm>& terms);
+// Column form: Hamiltonians/TFIsing.hpp:53-65, Hamiltonians/XXZ.hpp:51-64 (std::map, zeros kept)
+std::map<uint64_t, double> ham_column(const Ham& H, uint64_t col);
+// State form: Hamiltonians/TFIsing.hpp:28-39, XXZ.hpp:37-49, with ratio = exp(logRatio)
+cd ham_eloc(const Ham& H, const RBM& q, const int8_t* s, const cd* th);
+
+// ---------------------------------------------------------------------------
+// Samplers/LocalSweeper.hpp:32-53, Samplers/SwapSweeper.hpp:28-57, Samplers/SamplerMT.hpp:155-204
+enum Move { MOVE_LOCAL = 0, MOVE_EXCHANGE_ANY = 1, MOVE_EXCHANGE_NN = 2 };
+struct SampleSpec {
+    int n_chains = 1;
+    int move = MOVE_LOCAL;
+    int nup = -1;          // >=0: reinitialise with fixed magnetisation (randomSigma(n, nup))
+    uint64_t seed = 0;
+    uint32_t epoch = 0;
+    int reinit = 1;        // draw fresh chains (RunRBM.hpp:166 sampler.randomize)
+    int n_sweeps = 1;      // recorded sweeps
+    int n_discard = 0;     // thermalisation sweeps
+    int sweep_len = 0;     // proposals per sweep (0 -> n, LocalSweeper nSweep_=1)
+};
+void random_sigma(int n, int nup, uint64_t seed, uint32_t epoch, uint32_t chain, int8_t* s);
+// chain_sigma: n_chains x n, in/out.  Outputs sample-major (sweep, chain).
+void sample(const RBM& q, const SampleSpec& sp, int8_t* chain_sigma, int8_t* out_sigma, cd* out_theta,
+            uint64_t* acc, int nthreads);
+
+// ---------------------------------------------------------------------------
+// Dense complex linear algebra restated without Eigen/MKL.
+// Lower Cholesky in place (Eigen::LLT semantics): returns 0 on success, k+1 if pivot k <= 0.
+int cholesky_lower(int nn, cd* A /* row-major nn x nn, lower used */);
+void cholesky_solve(int nn, const cd* L, cd* x);  // x <- (L L^H)^{-1} x
+// Eigen::ConjugateGradient<..., Lower|Upper, IdentityPreconditioner>: relative residual
+// ||r||/||b|| < tol, at most maxit iterations (Eigen default 2*dim), x0 = 0.
+
+// GroundState/SRMat.hpp:89-237 + GroundState/utils.hpp:12-51 restated.
+struct SRResult {
+    double energy = 0., energy_var = 0.;
+    std::vector<cd> elocs, oloc, grad, v;
+    int status = 0;
+    int cg_iters = 0;
+    double cg_relres = 0.;
+};
+enum SRMode { SR_S = 0, SR_T = 1 };
+enum SRSolver { SOLVE_LLT = 0, SOLVE_CG = 1 };
+// Builds O and E_loc from (sigma, theta) samples, centres O, forms F = O~^H E / Ns and
+// solves (S + shift) v = F (S-mode, SRMat::solveExact / solveCG) or, in T-mode, the
+// sample-space dual v = O~^H (O~ O~^H / Ns + shift)^{-1} (E - <E>) / Ns.
+SRResult sr_step(const RBM& q, const Ham& H, int ns, const int8_t* sig, const cd* th, double shift, int mode,
+                 int solver, double cgtol, int nthreads);
+
+// GroundState/SRMatExact.hpp:97-132 restated (basis = sorted list of indices).
+struct ExactResult {
+    double energy = 0., energy_var = 0.;
+    std::vector<cd> oloc, grad, S;  // S is P x P row-major
+};
+ExactResult exact_sr(const RBM& q, const Ham& H, const std::vector<uint64_t>& basis, int nthreads);
+
+// Basis/BasisFull.hpp:126-153, Basis/BasisJz.hpp:25-104
+std::vector<uint64_t> basis_full(int n);
+std::vector<uint64_t> basis_jz(int n, int nup);
+// ED: sparse H over a basis (ED/ConstructSparseMat.hpp:32-57) + Lanczos (the reference has no eigensolver).
+double ed_ground_energy(const Ham& H, const std::vector<uint64_t>& basis, int maxit, int nthreads);
+
+// ---------------------------------------------------------------------------
+// FeedForward: Conv1D(periodic) -> LnCosh -> FullyConnected -> LnCosh -> Sum
+// (Machines/FeedForward.hpp:152-205; layers/Conv1D.hpp:144-225;
+//  layers/FullyConnected.hpp:150-179; layers/activations.hpp:74-107; layers/Mean.hpp:92-125)
+struct FFNet {
+    int L = 0;          // input length (sites)
+    int conv_out = 0;   // output channels (input channels = 1)
+    int conv_k = 0;     // kernel size
+    int fc_out = 0;     // fully connected output width
+    // params: [conv kernel (conv_k x conv_out, column-major) | fc weight ((L*conv_out) x fc_out, column-major)]
+    const double* p = nullptr;
+    size_t dim() const { return size_t(conv_k) * conv_out + size_t(L) * conv_out * fc_out; }
+};
+double ff_forward(const FFNet& f, const int8_t* s);
+void ff_backward(const FFNet& f, const int8_t* s, double* der);
+
+}  // namespace orc

@@ -1,0 +1,304 @@
+"""ctypes front end of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
+CPU-baseline leg of bench.py, never by the product package.  Complex arrays
+cross the boundary as numpy complex128 (interleaved doubles).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+# Hamiltonian kinds (oracle.hpp)
+TFI, XXZ, TFI2D = 0, 1, 2
+MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN = 0, 1, 2
+SR_S, SR_T = 0, 1
+SOLVE_LLT, SOLVE_CG = 0, 1
+
+
+def build(quiet: bool = True) -> str:
+    """Compile liboracle.so with the committed Makefile (no-op when up to date)."""
+    out = subprocess.run(["make", "-C", _HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def _declare(L):
+    vp, i, d, u64, u32 = C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_uint32
+    sig = {
+        "orc_philox": (None, [vp, vp, vp]),
+        "orc_logcosh": (None, [vp, vp]),
+        "orc_logcosh_real": (d, [d]),
+        "orc_init_params": (None, [i, i, i, u64, d, vp]),
+        "orc_theta": (None, [i, i, i, vp, vp, vp]),
+        "orc_logpsi": (None, [i, i, i, vp, vp, vp]),
+        "orc_psi": (None, [i, i, i, vp, vp, vp]),
+        "orc_logratio": (None, [i, i, i, vp, vp, vp, i, vp, vp]),
+        "orc_flip": (None, [i, i, i, vp, vp, vp, i, vp]),
+        "orc_logderiv": (None, [i, i, i, vp, vp, vp, vp]),
+        "orc_ham_enumerate": (d, [i, i, i, i, d, d, d, vp, vp, vp, i, vp]),
+        "orc_ham_column": (i, [i, i, i, i, d, d, d, u64, vp, vp, i]),
+        "orc_eloc": (None, [i, i, i, i, d, d, d, i, i, vp, i, vp, vp, vp, i]),
+        "orc_random_sigma": (None, [i, i, u64, u32, u32, vp]),
+        "orc_sample": (None, [i, i, i, vp, i, i, i, u64, u32, i, i, i, i, vp, vp, vp, vp, i]),
+        "orc_sr_step": (i, [i, i, i, i, d, d, d, i, i, vp, i, vp, vp, d, i, i, d, vp, vp, vp, vp, vp, i]),
+        "orc_cholesky_solve": (i, [i, vp, vp]),
+        "orc_exact": (i, [i, i, i, i, d, d, d, i, i, vp, i, i, vp, vp, vp, vp, i]),
+        "orc_basis": (i, [i, i, i, vp, i]),
+        "orc_ed_ground": (d, [i, i, i, i, d, d, d, i, i, i, i]),
+        "orc_ff_forward": (d, [i, i, i, i, vp, vp]),
+        "orc_ff_backward": (None, [i, i, i, i, vp, vp, vp]),
+        "orc_ff_batch": (None, [i, i, i, i, vp, i, vp, vp, vp, i]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+
+# ---------------------------------------------------------------------------
+class Ham:
+    """Hamiltonian descriptor with the reference's sign conventions.
+
+    TFI:   E_loc = sum_i J s_i s_{i+1} + h ratio(i)         (TFIsing(n, J, h))
+    XXZ:   E_loc = sum_i J Delta zz_i + sign J (1 - zz_i) ratio(i, i+1)
+    TFI2D: E_loc = sum_i J s_i (s_right + s_down) + h ratio(i)  on an lx x ly torus
+    """
+
+    def __init__(self, kind, n, J, h, sign=1.0, lx=0, ly=0):
+        self.kind, self.n, self.J, self.h, self.sign, self.lx, self.ly = kind, n, J, h, sign, lx, ly
+
+    @classmethod
+    def tfi(cls, n, J, h):
+        return cls(TFI, n, J, h)
+
+    @classmethod
+    def xxz(cls, n, J, delta, sign_rule=False):
+        return cls(XXZ, n, J, delta, -1.0 if sign_rule else 1.0)
+
+    @classmethod
+    def tfi2d(cls, lx, ly, J, h):
+        return cls(TFI2D, lx * ly, J, h, 1.0, lx, ly)
+
+    def args(self):
+        return (self.kind, self.n, self.lx, self.ly, self.J, self.h, self.sign)
+
+
+def rbm_dim(n, m, use_bias=True):
+    return n * m + (n + m if use_bias else 0)
+
+
+def philox(ctr, key):
+    c = np.asarray(ctr, dtype=np.uint32)
+    k = np.asarray(key, dtype=np.uint32)
+    o = np.zeros(4, dtype=np.uint32)
+    lib().orc_philox(_p(c), _p(k), _p(o))
+    return o
+
+
+def logcosh(z):
+    zz = np.asarray([complex(z).real, complex(z).imag], dtype=np.float64)
+    o = np.zeros(2)
+    lib().orc_logcosh(_p(zz), _p(o))
+    return complex(o[0], o[1])
+
+
+def logcosh_real(x):
+    return lib().orc_logcosh_real(float(x))
+
+
+def init_params(n, m, seed, sd, use_bias=True):
+    p = np.zeros(rbm_dim(n, m, use_bias), dtype=np.complex128)
+    lib().orc_init_params(n, m, int(use_bias), seed, sd, _p(p))
+    return p
+
+
+def _s8(sigma):
+    return np.ascontiguousarray(sigma, dtype=np.int8)
+
+
+def theta(n, m, params, sigma, use_bias=True):
+    th = np.zeros(m, dtype=np.complex128)
+    lib().orc_theta(n, m, int(use_bias), _p(params), _p(_s8(sigma)), _p(th))
+    return th
+
+
+def logpsi(n, m, params, sigma, use_bias=True):
+    o = np.zeros(2)
+    lib().orc_logpsi(n, m, int(use_bias), _p(params), _p(_s8(sigma)), _p(o))
+    return complex(o[0], o[1])
+
+
+def psi(n, m, params, sigma, use_bias=True):
+    o = np.zeros(2)
+    lib().orc_psi(n, m, int(use_bias), _p(params), _p(_s8(sigma)), _p(o))
+    return complex(o[0], o[1])
+
+
+def logratio(n, m, params, sigma, th, flips, use_bias=True):
+    f = np.asarray(flips, dtype=np.int32)
+    o = np.zeros(2)
+    lib().orc_logratio(n, m, int(use_bias), _p(params), _p(_s8(sigma)), _p(th), len(f), _p(f), _p(o))
+    return complex(o[0], o[1])
+
+
+def flip(n, m, params, sigma, th, flips, use_bias=True):
+    """In place on sigma (int8 array) and th (complex128 array)."""
+    f = np.asarray(flips, dtype=np.int32)
+    lib().orc_flip(n, m, int(use_bias), _p(params), _p(sigma), _p(th), len(f), _p(f))
+
+
+def logderiv(n, m, params, sigma, th, use_bias=True):
+    o = np.zeros(rbm_dim(n, m, use_bias), dtype=np.complex128)
+    lib().orc_logderiv(n, m, int(use_bias), _p(params), _p(_s8(sigma)), _p(th), _p(o))
+    return o
+
+
+def ham_enumerate(ham, sigma, cap=4096):
+    masks = np.zeros(cap, dtype=np.uint64)
+    coeffs = np.zeros(cap)
+    cnt = C.c_int(0)
+    d = lib().orc_ham_enumerate(*ham.args(), _p(_s8(sigma)), _p(masks), _p(coeffs), cap, C.byref(cnt))
+    return d, masks[: cnt.value].copy(), coeffs[: cnt.value].copy()
+
+
+def ham_column(ham, col, cap=4096):
+    rows = np.zeros(cap, dtype=np.uint64)
+    vals = np.zeros(cap)
+    c = lib().orc_ham_column(*ham.args(), int(col), _p(rows), _p(vals), cap)
+    return rows[:c].copy(), vals[:c].copy()
+
+
+def eloc(ham, m, params, sigma, th, use_bias=True, nthreads=0):
+    sigma = _s8(sigma)
+    ns = sigma.shape[0]
+    th = np.ascontiguousarray(th, dtype=np.complex128)
+    o = np.zeros(ns, dtype=np.complex128)
+    lib().orc_eloc(*ham.args(), m, int(use_bias), _p(params), ns, _p(sigma), _p(th), _p(o), nthreads or os.cpu_count())
+    return o
+
+
+def random_sigma(n, nup, seed, epoch, chain):
+    s = np.zeros(n, dtype=np.int8)
+    lib().orc_random_sigma(n, nup, seed, epoch, chain, _p(s))
+    return s
+
+
+def sample(n, m, params, n_chains, move=MOVE_LOCAL, nup=-1, seed=0, epoch=0, reinit=True, n_sweeps=1,
+           n_discard=0, sweep_len=0, chain_sigma=None, use_bias=True, nthreads=0):
+    """Restated SamplerMT (nTmps = 1).  Returns (sigma[Ns, n], theta[Ns, m], chain_sigma, acc)."""
+    cs = np.zeros((n_chains, n), dtype=np.int8) if chain_sigma is None else np.ascontiguousarray(chain_sigma, np.int8)
+    ns = n_chains * n_sweeps
+    osig = np.zeros((ns, n), dtype=np.int8)
+    oth = np.zeros((ns, m), dtype=np.complex128)
+    acc = np.zeros(n_chains, dtype=np.uint64)
+    lib().orc_sample(n, m, int(use_bias), _p(params), n_chains, move, nup, seed, epoch, int(reinit), n_sweeps,
+                     n_discard, sweep_len, _p(cs), _p(osig), _p(oth), _p(acc), nthreads or os.cpu_count())
+    return osig, oth, cs, acc
+
+
+def sr_step(ham, m, params, sigma, th, shift, mode=SR_S, solver=SOLVE_LLT, cgtol=1e-4, use_bias=True, nthreads=0):
+    sigma = _s8(sigma)
+    ns, n = sigma.shape
+    P = rbm_dim(n, m, use_bias)
+    th = np.ascontiguousarray(th, dtype=np.complex128)
+    v = np.zeros(P, np.complex128)
+    g = np.zeros(P, np.complex128)
+    ol = np.zeros(P, np.complex128)
+    el = np.zeros(ns, np.complex128)
+    st = np.zeros(4)
+    status = lib().orc_sr_step(*ham.args(), m, int(use_bias), _p(params), ns, _p(sigma), _p(th), shift, mode, solver,
+                               cgtol, _p(v), _p(g), _p(ol), _p(el), _p(st), nthreads or os.cpu_count())
+    return dict(status=status, v=v, grad=g, oloc=ol, elocs=el, energy=st[0], energy_var=st[1],
+                cg_iters=int(st[2]), cg_relres=st[3])
+
+
+def cholesky_solve(A, b):
+    A = np.array(A, dtype=np.complex128, order="C")
+    x = np.array(b, dtype=np.complex128)
+    st = lib().orc_cholesky_solve(A.shape[0], _p(A), _p(x))
+    return st, x
+
+
+def exact(ham, m, params, basis_kind=0, nup=0, with_S=True, use_bias=True, nthreads=0):
+    P = rbm_dim(ham.n, m, use_bias)
+    st = np.zeros(2)
+    ol = np.zeros(P, np.complex128)
+    g = np.zeros(P, np.complex128)
+    S = np.zeros((P, P), np.complex128) if with_S else None
+    dim = lib().orc_exact(*ham.args(), m, int(use_bias), _p(params), basis_kind, nup, _p(st), _p(ol), _p(g), _p(S),
+                          nthreads or os.cpu_count())
+    return dict(energy=st[0], energy_var=st[1], oloc=ol, grad=g, S=S, dim=dim)
+
+
+def sigma_of(index, n):
+    """Utilities/Utility.hpp:91-99 toSigma: bit i set <=> sigma_i = -1."""
+    index = int(index)
+    return np.array([1 - 2 * ((index >> i) & 1) for i in range(n)], dtype=np.int8)
+
+
+def index_of(sigma):
+    """Utilities/Utility.hpp:102-110 toValue."""
+    return int(sum(((1 - int(x)) // 2) << i for i, x in enumerate(sigma)))
+
+
+def basis(n, basis_kind=0, nup=0):
+    from math import comb
+    cap = (1 << n) if basis_kind == 0 else comb(n, nup)
+    out = np.zeros(cap, dtype=np.uint64)
+    c = lib().orc_basis(n, basis_kind, nup, _p(out), cap)
+    return out[:c]
+
+
+def ed_ground(ham, basis_kind=0, nup=0, maxit=300, nthreads=0):
+    return lib().orc_ed_ground(*ham.args(), basis_kind, nup, maxit, nthreads or os.cpu_count())
+
+
+def ff_dim(L, conv_out, conv_k, fc_out):
+    return conv_k * conv_out + L * conv_out * fc_out
+
+
+def ff_forward(L, conv_out, conv_k, fc_out, params, sigma):
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    return lib().orc_ff_forward(L, conv_out, conv_k, fc_out, _p(p), _p(_s8(sigma)))
+
+
+def ff_backward(L, conv_out, conv_k, fc_out, params, sigma):
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    der = np.zeros(ff_dim(L, conv_out, conv_k, fc_out))
+    lib().orc_ff_backward(L, conv_out, conv_k, fc_out, _p(p), _p(_s8(sigma)), _p(der))
+    return der
+
+
+def ff_batch(L, conv_out, conv_k, fc_out, params, sigma, want_der=True, nthreads=0):
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    sigma = _s8(sigma)
+    B = sigma.shape[0]
+    lp = np.zeros(B)
+    der = np.zeros((B, ff_dim(L, conv_out, conv_k, fc_out))) if want_der else None
+    lib().orc_ff_batch(L, conv_out, conv_k, fc_out, _p(p), B, _p(sigma), _p(lp), _p(der), nthreads or os.cpu_count())
+    return lp, der
