@@ -1,0 +1,323 @@
+#!/usr/bin/env python
+"""VMC iterations/s of one variational Monte Carlo step (sample -> E_loc -> O ->
+SR solve -> SGD update) on one B200, mixed precision vs plain FP64.
+
+Workload (the precision configuration): 2D transverse-field Ising model on a
+periodic 12 x 12 lattice (N = 144), H = -sum ZZ - 3 sum X, RBM alpha = 2
+(M = 288, P = 41,904), parameters N(0, 0.01^2) from the seed; 1024 persistent
+Metropolis chains of single-spin flips, 64 thermalisation sweeps before timing,
+then per iteration 8 decorrelation + 8 recorded sweeps -> 8192 samples; SR in
+the sample-space form T = O~ O~^H / Ns + 1e-3 I (Ns < P), Cholesky, SGD lr 0.01.
+
+  mixed: complex64 sampling / E_loc / O, BF16x3 tcgen05 Gram with FP32
+         accumulation, FP64 Cholesky + 2 iterative-refinement steps, FP64 means.
+  fp64:  complex128 end to end, FP64 SIMT Gram, FP64 Cholesky.
+
+--impl reference times the CPU restatement of the reference path (OpenMP
+oracle + numpy BLAS/LAPACK for the dense algebra) on a bounded sample of the
+same workload and extrapolates to one iteration.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W = dict(workload="tfi2d_12x12_rbm_alpha2", lx=12, ly=12, J=-1.0, h=-3.0, alpha=2, chains=1024, n_sweeps=8,
+         n_discard=8, therm=64, shift=1e-3, lr=0.01, seed=20261203, init_sd=0.01)
+METRIC = "VMC iters/s (sample+E_loc+O+SR) mixed vs FP64 plain, same B200, equal E err"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while timing."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device, self.rows, self.proc = device, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    lrank = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return ws, rank, lrank, pg
+
+
+def _barrier(pg):
+    if pg:
+        pg.barrier()
+
+
+def _max(pg, x):
+    if not pg:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _build_problem(api, ctx, precision):
+    n = W["lx"] * W["ly"]
+    m = W["alpha"] * n
+    dtype = api.C64 if precision == "mixed" else api.C128
+    q = api.RBM(ctx, n, m, True, dtype)
+    q.init_random(W["seed"], W["init_sd"])
+    H = api.Hamiltonian.tfi2d(ctx, W["lx"], W["ly"], W["J"], W["h"])
+    S = api.Sampler(q, W["chains"], api.MOVE_LOCAL)
+    sr = api.SR(q, H, S, api.SR_T, api.PREC_MIXED if precision == "mixed" else api.PREC_FP64)
+    return q, H, S, sr
+
+
+def _run_precision(api, ctx, precision, steps, warmup, pg, device, with_e2e):
+    import numpy as np
+
+    q, H, S, sr = _build_problem(api, ctx, precision)
+    ir = 2 if precision == "mixed" else 0
+    epoch = 0
+
+    def it(reinit, n_discard):
+        nonlocal epoch
+        r = sr.iteration(W["n_sweeps"], n_discard, W["seed"], epoch, W["shift"], W["lr"], reinit=reinit, ir_steps=ir)
+        epoch += 1
+        return r
+
+    it(True, W["therm"])  # thermalisation of the persistent chains (untimed)
+    for _ in range(max(0, warmup - 1)):
+        it(False, W["n_discard"])
+    ctx.synchronize()
+    _barrier(pg)
+    clocks = ClockSampler(device)
+    clocks.start()
+    l0 = api.launch_count()
+    stage_sum = {k: 0.0 for k in api.STAGES}
+    energies = []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r = it(False, W["n_discard"])
+        energies.append(r.energy)
+        for k in stage_sum:
+            stage_sum[k] += ctx.stage_ms(k)
+    ctx.synchronize()
+    wall = time.perf_counter() - t0
+    launches = (api.launch_count() - l0) // max(1, steps)
+    clk = clocks.stop()
+    _barrier(pg)
+    dev_ms = _max(pg, stage_sum["total"]) / steps
+    out = dict(ms_per_step=dev_ms, wall_ms_per_step=1e3 * wall / steps, stages_ms={k: v / steps for k, v in
+                                                                                     stage_sum.items()},
+               energy_per_site=float(np.mean(energies)) / (W["lx"] * W["ly"]), launches=launches, clocks=clk,
+               accept_rate=r.accept_rate, P=q.dim, Ns=W["chains"] * W["n_sweeps"])
+    if with_e2e:
+        # end to end through the public API: parameters from pinned host memory in,
+        # updated parameters and the energy back, every step
+        pin = api.PinnedArray((q.dim,), np.complex128)
+        q.get_params(pin.array)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            q.set_params(pin.array)
+            it(False, W["n_discard"])
+            q.get_params(pin.array)
+        ctx.synchronize()
+        e2e_ms = 1e3 * (time.perf_counter() - t0) / steps
+        out["e2e_ms"] = _max(pg, e2e_ms)
+        out["h2d_bytes"] = q.dim * 16
+        out["d2h_bytes"] = q.dim * 16 + 8 * 8 + W["chains"] * 8
+        pin.free()
+    for x in (sr, S, H, q):
+        x.close()
+    return out
+
+
+def cpu_sample(steps=1, warmup=0):
+    """Reference CPU path (oracle restatement + numpy BLAS/LAPACK) on a bounded
+    sample of the workload, extrapolated to one full iteration.  Returns
+    (iterations/s, cores, description)."""
+    import numpy as np
+
+    from oracle import pyoracle as orc
+
+    orc.build()
+    n = W["lx"] * W["ly"]
+    m = W["alpha"] * n
+    P = n * m + n + m
+    Ns = W["chains"] * W["n_sweeps"]
+    cores = os.cpu_count() or 1
+    ham = orc.Ham.tfi2d(W["lx"], W["ly"], W["J"], W["h"])
+    p = orc.init_params(n, m, W["seed"], W["init_sd"])
+    ch = max(cores, 16)
+    nb, nc = 512, 2048
+    times = []
+    for rep in range(warmup + steps):
+        t = time.perf_counter()
+        s, th, _, _ = orc.sample(n, m, p, ch, seed=W["seed"], epoch=rep, n_sweeps=W["n_sweeps"],
+                                 n_discard=W["n_discard"], nthreads=cores)
+        t_samp = (time.perf_counter() - t) * (W["chains"] / ch)
+        t = time.perf_counter()
+        e = orc.eloc(ham, m, p, s, th, nthreads=cores)
+        t_eloc = (time.perf_counter() - t) * (Ns / len(s))
+        t = time.perf_counter()
+        O = np.array([orc.logderiv(n, m, p, a, b) for a, b in zip(s[:64], th[:64])])
+        t_o = (time.perf_counter() - t) * (Ns / 64)
+        A = np.tile(O, (nb // 64, 1)) - O.mean(0)
+        t = time.perf_counter()
+        Tb = A @ A.conj().T / Ns
+        t_t = (time.perf_counter() - t) * ((Ns * Ns / 2) / (nb * nb))
+        X = np.random.default_rng(0).normal(size=(nc, nc)) + 1j * np.random.default_rng(1).normal(size=(nc, nc))
+        G = X @ X.conj().T / nc + np.eye(nc)
+        t = time.perf_counter()
+        np.linalg.cholesky(G)
+        t_c = (time.perf_counter() - t) * (Ns / nc) ** 3
+        t = time.perf_counter()
+        A.conj().T @ np.ones(nb)
+        t_v = (time.perf_counter() - t) * (Ns / nb) * 2
+        tot = t_samp + t_eloc + t_o + t_t + t_c + t_v
+        if rep >= warmup:
+            times.append(tot)
+        del Tb
+    sample = (f"{ch} chains x {W['n_discard'] + W['n_sweeps']} sweeps, E_loc on {ch * W['n_sweeps']} samples, "
+              f"O on 64 rows, a {nb}x{nb} block of T and a {nc}x{nc} Cholesky timed, each scaled to the "
+              f"Ns={Ns}, P={P} iteration; OpenMP oracle + numpy BLAS")
+    return 1.0 / statistics.mean(times), cores, sample
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, lrank, pg = _dist()
+    warmup = max(3, args.warmup)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        v, cores, sample = cpu_sample(steps=args.steps, warmup=min(warmup, 1))
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": 0,
+                          "steps": args.steps, "warmup": warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": W["workload"], "Ns": W["chains"] * W["n_sweeps"],
+                                     "chains": W["chains"], "inputs": "larger than L2"},
+                          "cpu_baseline": {"value": v, "unit": "iters/s", "cores": cores, "kind": "port",
+                                           "sample": sample},
+                          "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    from yannq_b200 import api
+
+    ctx = api.Context(lrank)
+    res = {}
+    precs = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
+    for prec in precs:
+        res[prec] = _run_precision(api, ctx, prec, args.steps, warmup, pg, lrank, with_e2e=(prec == precs[0]))
+    head = res[precs[0]]
+    peaks, src = _peaks()
+    Ns, P = head["Ns"], head["P"]
+    if precs[0] == "mixed":
+        flops = 12.0 * Ns * Ns * P  # three BF16 products of the complex Hermitian lower triangle (4 Ns^2 P each)
+        t_ms = head["stages_ms"]["gram"]
+        ach = flops / (t_ms * 1e-3) / 1e12
+        roof = {"kernel": "gram_tc_kernel (tcgen05 BF16x3 T = O~O~^H)", "bound": "tensor", "achieved": ach,
+                "peak": peaks.get("bf16_tflops"), "unit": "TFLOP/s", "frac": ach / peaks.get("bf16_tflops"),
+                "peak_source": src, "traffic": None}
+    else:
+        flops = 4.0 * Ns * Ns * P
+        t_ms = head["stages_ms"]["gram"]
+        ach = flops / (t_ms * 1e-3) / 1e12
+        roof = {"kernel": "gram_fp64_kernel (FP64 SIMT T = O~O~^H)", "bound": "fp64", "achieved": ach, "peak": None,
+                "unit": "TFLOP/s", "frac": None, "peak_source": "FP64 peak not measured", "traffic": None}
+    value = ws * 1e3 / head["ms_per_step"]
+    line = {"metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": ws, "steps": args.steps, "warmup": warmup,
+            "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64+bf16x3+f64" if precs[0] == "mixed" else "c128",
+            "data": "synthetic (seeded Philox parameters and chains)",
+            "config": {"workload": W["workload"], "precision": precs[0], "N": W["lx"] * W["ly"], "M": Ns and
+                       W["alpha"] * W["lx"] * W["ly"], "P": P, "Ns": Ns, "chains": W["chains"],
+                       "sweeps": f"{W['n_discard']} discard + {W['n_sweeps']} recorded per step, {W['therm']} therm",
+                       "sr": "T-form, shift 1e-3, Cholesky", "parallelism": f"replicas{ws}",
+                       "inputs": "larger than L2 (O~ and operands >= 2.7 GB)"},
+            "gpu_launches": head["launches"], "clocks": head["clocks"], "roofline": roof,
+            "stages_ms": head["stages_ms"], "energy_per_site": head["energy_per_site"],
+            "accept_rate": head["accept_rate"]}
+    if "e2e_ms" in head:
+        line["e2e"] = {"value": ws * 1e3 / head["e2e_ms"], "unit": "iters/s", "h2d_bytes_per_step": head["h2d_bytes"],
+                       "d2h_bytes_per_step": head["d2h_bytes"]}
+    if len(precs) == 2:
+        f = res["fp64"]
+        line["fp64_plain"] = {"value": ws * 1e3 / f["ms_per_step"], "ms_per_step": f["ms_per_step"],
+                              "stages_ms": f["stages_ms"], "energy_per_site": f["energy_per_site"],
+                              "gpu_launches": f["launches"]}
+        line["mixed_over_fp64"] = f["ms_per_step"] / head["ms_per_step"]
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_sample(steps=1, warmup=0)
+        line["cpu_baseline"] = {"value": v, "unit": "iters/s", "cores": cores, "kind": "port", "sample": sample}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

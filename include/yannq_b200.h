@@ -1,0 +1,195 @@
+/*
+ * yannq_b200.h -- C ABI of libyannq_b200.so, the B200 (sm_100a) backend of the
+ * variational Monte Carlo step of yannq (sample -> E_loc -> O -> SR solve -> update).
+ *
+ * Every entry point returns an int status (YQ_OK = 0 or a YQ_E_* code); the
+ * message of the last failure on the calling thread is available through
+ * yq_last_error().  Handles are opaque.  One context owns one CUDA stream; calls
+ * on one context are not reentrant, distinct contexts may be used from distinct
+ * threads.  Complex arrays are interleaved (re, im) doubles on the host side.
+ *
+ * Each declaration names the reference interface it replaces (paths are relative
+ * to the yannq project root).  The reference binds these through its own
+ * header-only templates; the headers under include/yannq_gpu are the C++ adapters that let
+ * an existing RunRBM-style driver call them.
+ */
+#ifndef YANNQ_B200_H
+#define YANNQ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------- */
+enum {
+    YQ_OK = 0,
+    YQ_E_ARG = 1,         /* bad argument (shape, kind, null pointer)             */
+    YQ_E_CUDA = 2,        /* CUDA runtime error                                    */
+    YQ_E_NOMEM = 3,       /* device allocation failed                              */
+    YQ_E_NOT_PD = 4,      /* Cholesky met a non-positive pivot (LLT failure)       */
+    YQ_E_NONFINITE = 5,   /* NaN/Inf detected in E_loc, O, S/T or the update      */
+    YQ_E_TIMEOUT = 6,     /* a bounded device-side wait gave up                    */
+    YQ_E_STATE = 7,       /* call order violated (e.g. solve before construct)    */
+    YQ_E_UNSUPPORTED = 8  /* configuration not built into this library            */
+};
+
+enum { YQ_C64 = 0, YQ_C128 = 1 };                             /* RBM<complex<float|double>> */
+enum { YQ_HAM_TFI = 0, YQ_HAM_XXZ = 1, YQ_HAM_TFI2D = 2 };    /* Hamiltonian kinds          */
+enum { YQ_MOVE_LOCAL = 0, YQ_MOVE_EXCHANGE_ANY = 1, YQ_MOVE_EXCHANGE_NN = 2 };
+enum { YQ_SR_AUTO = 0, YQ_SR_S = 1, YQ_SR_T = 2 };             /* S = <O^H O>, T = O O^H dual */
+enum { YQ_PREC_FP64 = 0, YQ_PREC_MIXED = 1 };
+enum { YQ_SOLVE_LLT = 0, YQ_SOLVE_CG = 1 };
+
+typedef struct yq_ctx_s* yq_ctx;
+typedef struct yq_rbm_s* yq_rbm;
+typedef struct yq_ham_s* yq_ham;
+typedef struct yq_sampler_s* yq_sampler;
+typedef struct yq_sr_s* yq_sr;
+
+/* Message of the last failed call on this thread (always NUL-terminated). */
+int yq_last_error(char* buf, size_t len);
+/* Library version string, e.g. "yannq_b200 0.1 sm_100a". */
+const char* yq_version(void);
+/* Number of kernels this library has launched in the process so far (no
+ * reference counterpart; used to report launches per VMC step). */
+int yq_launch_count(uint64_t* out);
+/* Page-locked host buffers for the host<->device copies of parameters and
+ * samples (no reference counterpart: the reference is host-only). */
+int yq_host_alloc(size_t bytes, void** out);
+int yq_host_free(void* p);
+
+/* ---- context --------------------------------------------------------------- */
+/* No reference counterpart (the reference is host-only); owns the device and stream. */
+int yq_ctx_create(int device, yq_ctx* out);
+int yq_ctx_destroy(yq_ctx ctx);
+int yq_ctx_synchronize(yq_ctx ctx);
+/* Device time (ms) of the named stage of the last yq_vmc_iteration / yq_sample /
+ * yq_sr_construct / yq_sr_solve call, measured with CUDA events on the context's
+ * stream.  stage: 0 sample, 1 E_loc, 2 O, 3 S/T, 4 Cholesky+solve, 5 update,
+ * 6 total, 7 mean + F.  (The reference times sampling and solving with
+ * std::chrono: Runners/RunRBM.hpp:169-214.) */
+int yq_ctx_stage_ms(yq_ctx ctx, int stage, float* ms);
+
+/* ---- RBM machine (Machines/RBM.hpp) ---------------------------------------- */
+/* RBM<T>(n, m, useBias) -- Machines/RBM.hpp:48-53; dtype YQ_C64 or YQ_C128. */
+int yq_rbm_create(yq_ctx ctx, int n, int m, int use_bias, int dtype, yq_rbm* out);
+int yq_rbm_destroy(yq_rbm q);
+/* getDim() -- Machines/RBM.hpp:120-126 */
+int yq_rbm_dim(yq_rbm q, size_t* dim);
+/* setParams / getParams / updateParams -- Machines/RBM.hpp:261-291; host vector of
+ * getDim() complex values in the layout [W column-major (m x n) | a | b]. */
+int yq_rbm_set_params(yq_rbm q, const double* params);
+int yq_rbm_get_params(yq_rbm q, double* params);
+int yq_rbm_update_params(yq_rbm q, const double* delta);
+/* initializeRandom(re, sigma) -- Machines/RBM.hpp:325-349: draw order a, b, W by
+ * columns, each entry (re, im) ~ N(0, sd^2); the normal draws are Philox4x32-10
+ * keyed by seed (Box-Muller), identical to the oracle's. */
+int yq_rbm_init_random(yq_rbm q, uint64_t seed, double sd);
+/* calcTheta over a batch -- Machines/RBM.hpp:137-141.  sigma: ns x n int8 (+-1). */
+int yq_rbm_theta(yq_rbm q, int ns, const int8_t* sigma, double* theta);
+/* logCoeff over a batch -- Machines/RBM.hpp:367-378 (ns complex). */
+int yq_rbm_log_psi(yq_rbm q, int ns, const int8_t* sigma, double* out);
+/* logRatio(k), logRatio(k, l) -- States/RBMState.hpp:48-94: for each sample s
+ * flip sites flips[s*nflip .. s*nflip+nflip) (nflip 1 or 2); out: ns complex
+ * log psi(sigma') - log psi(sigma) (defined modulo 2 pi i). */
+int yq_rbm_log_ratio(yq_rbm q, int ns, const int8_t* sigma, const double* theta, int nflip, const int* flips,
+                     double* out);
+/* logDeriv over a batch -- Machines/RBM.hpp:390-406 / constructDelta
+ * (GroundState/utils.hpp:12-51): out ns x getDim() complex, row per sample. */
+int yq_rbm_log_deriv(yq_rbm q, int ns, const int8_t* sigma, const double* theta, double* out);
+
+/* ---- Hamiltonians (Hamiltonians/TFIsing.hpp, Hamiltonians/XXZ.hpp) -------- */
+/* kind YQ_HAM_TFI: TFIsing(n, J, h); YQ_HAM_XXZ: XXZ(n, J, Delta = h, signRule);
+ * YQ_HAM_TFI2D: periodic lx x ly square lattice (no reference counterpart; same
+ * duck-typed concept: E_loc = sum J s_i (s_right + s_down) + h ratio(i)). */
+int yq_ham_create(yq_ctx ctx, int kind, int n, int lx, int ly, double J, double h, int sign_rule, yq_ham* out);
+int yq_ham_destroy(yq_ham H);
+/* The state form's off-diagonal flips for each sample, in the order the
+ * reference's operator()(State) requests them (Hamiltonians/TFIsing.hpp:28-39,
+ * XXZ.hpp:37-49), zero coefficients included: per sample n terms of (site_a,
+ * site_b or -1, coeff) and the diagonal sum.  Arrays: ns*n ints / doubles, ns doubles. */
+int yq_ham_enumerate(yq_ham H, int ns, const int8_t* sigma, int* site_a, int* site_b, double* coeff, double* diag);
+/* Energy::eachSample over a batch -- Observables/Energy.hpp:47-51 with
+ * State = RBMStateRef(sigma, theta) (GroundState/utils.hpp:108-126). out: ns complex. */
+int yq_eloc(yq_ham H, yq_rbm q, int ns, const int8_t* sigma, const double* theta, double* out);
+
+/* ---- sampler (Samplers/SamplerMT.hpp + LocalSweeper / SwapSweeper) ------- */
+/* SamplerMT(qs, nTmps = 1, nChainsPer = n_chains, sweeper) -- SamplerMT.hpp:44-60.
+ * move: LocalSweeper (LocalSweeper.hpp:32-53), SwapSweeper with two independent
+ * sites (SwapSweeper.hpp:28-57) or with a neighbouring pair (i, i+1).  nup >= 0
+ * initialises chains with randomSigma(n, nup) (Utilities/Utility.hpp:77-88),
+ * otherwise randomSigma(n).  sweep_len 0 means n proposals per sweep. */
+int yq_sampler_create(yq_rbm q, int n_chains, int move, int nup, int sweep_len, yq_sampler* out);
+int yq_sampler_destroy(yq_sampler S);
+/* Recompute theta from sigma in FP64 every k recorded/discarded sweeps (0 = never
+ * inside one call, as the reference: States/RBMState.hpp:248-255). */
+int yq_sampler_set_resync(yq_sampler S, int every_sweeps);
+int yq_sampler_set_chains(yq_sampler S, const int8_t* sigma);  /* n_chains x n */
+int yq_sampler_get_chains(yq_sampler S, int8_t* sigma);
+/* randomize + sample(nSweeps, nDiscard) -- SamplerMT.hpp:103-110, :180-204.
+ * reinit != 0 draws fresh chains first (RunRBM.hpp:166).  Samples stay on the
+ * device, ordered (sweep, chain); n_samples = n_chains * n_sweeps. */
+int yq_sample(yq_sampler S, int n_sweeps, int n_discard, uint64_t seed, uint32_t epoch, int reinit);
+int yq_sampler_num_samples(yq_sampler S, int* ns);
+/* Copy the last samples to the host: sigma ns x n int8, theta ns x m complex (may be null). */
+int yq_sampler_get_samples(yq_sampler S, int8_t* sigma, double* theta);
+/* Accepted proposals per chain in the last yq_sample (LocalSweeper::sweep's return). */
+int yq_sampler_get_accepts(yq_sampler S, uint64_t* acc);
+/* Replace the device samples by host ones (for SR on externally supplied samples). */
+int yq_sampler_put_samples(yq_sampler S, int ns, const int8_t* sigma, const double* theta);
+
+/* ---- stochastic reconfiguration (GroundState/SRMat.hpp) ------------------- */
+/* SRMat<Machine, Hamiltonian>(qs, ham) -- SRMat.hpp:83-87, bound to a sampler.
+ * mode: S = O~^H O~ / Ns (P x P), T = O~ O~^H / Ns (Ns x Ns, push-through dual),
+ * AUTO picks T when Ns < P.  precision: FP64 everywhere, or MIXED (c64 sampling
+ * and O, BF16x3 tensor-core S/T with FP32 accumulation, FP64 Cholesky + iterative
+ * refinement, FP64 means). */
+int yq_sr_create(yq_rbm q, yq_ham H, yq_sampler S, int mode, int precision, yq_sr* out);
+int yq_sr_destroy(yq_sr sr);
+/* constructFromSamples -- SRMat.hpp:89-103 (E_loc, O, mean, centring, F). */
+int yq_sr_construct(yq_sr sr);
+/* eloc() / elocVar() -- SRMat.hpp:151-159 */
+int yq_sr_energy(yq_sr sr, double* energy, double* energy_var);
+/* elocs, oloc(), energyGrad() to host: which 0 elocs (Ns), 1 oloc (P), 2 grad (P), 3 v (P). */
+int yq_sr_get(yq_sr sr, int which, double* out);
+/* solveExact(shift) (SRMat.hpp:231-237, Eigen::LLT) in S-mode, or its sample-space
+ * dual in T-mode; solver YQ_SOLVE_CG uses SRMat::apply (SRMat.hpp:170-208) with
+ * relative-residual tolerance cg_tol.  v (P complex, may be null) receives the
+ * solution; iterations/relres (may be null) the CG statistics. */
+int yq_sr_solve(yq_sr sr, double shift, int solver, double cg_tol, double* v, int* iterations, double* relres);
+/* corrMat() -- SRMat.hpp:142-149: the Hermitian matrix the last LLT solve used
+ * (S or T, including the shift), lower triangle, dim x dim complex row-major. */
+int yq_sr_matrix(yq_sr sr, int* dim, double* out);
+
+/* ---- one VMC iteration (Runners/RunRBM.hpp:151-221) ----------------------- */
+typedef struct {
+    int n_sweeps;          /* recorded sweeps (samples = n_chains * n_sweeps)       */
+    int n_discard;         /* thermalisation sweeps per iteration                   */
+    int reinit;            /* randomize chains every iteration (reference default) */
+    uint64_t seed;
+    uint32_t epoch;        /* iteration index ll (also the Philox epoch)           */
+    double shift;          /* lambda = max(lambda0 decay^ll, lambda_min) by caller */
+    double lr;             /* SGD eta = max(alpha / t^p, 1e-4) by caller            */
+    int solver;            /* YQ_SOLVE_LLT or YQ_SOLVE_CG                           */
+    double cg_tol;
+    int ir_steps;          /* iterative-refinement steps (mixed precision)          */
+} yq_iter_params;
+
+typedef struct {
+    double energy, energy_var;
+    double update_norm;    /* ||v|| (RunRBM.hpp:205 nv)                             */
+    double cg_err;
+    double accept_rate;
+    int status;            /* 0 or the YQ_E_* code recorded by the device checks    */
+} yq_iter_result;
+
+/* sampler.randomize + sample + constructFromSamples + solve + update params by -lr v. */
+int yq_vmc_iteration(yq_sr sr, const yq_iter_params* p, yq_iter_result* r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* YANNQ_B200_H */

@@ -1,0 +1,166 @@
+"""GPU parity of the RBM and Hamiltonian kernels against the oracle (C-ABI calls).
+
+FP64 path: theta and parameter initialisation bit-exact; log psi, log ratios,
+log derivatives and E_loc within 1e-12 relative; flip enumeration bit-exact.
+complex64 path: within 1e-5 relative.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from yannq_b200 import api
+
+    c = api.Context(0)
+    yield c
+    c.close()
+
+
+def _rbm(api, ctx, orc, n, m, seed, sd, dtype):
+    q = api.RBM(ctx, n, m, True, dtype)
+    p = orc.init_params(n, m, seed, sd)
+    q.set_params(p)
+    return q, p
+
+
+def _rand_sigma(rng, ns, n):
+    return rng.choice(np.array([-1, 1], np.int8), size=(ns, n))
+
+
+def test_init_params_bit_exact(ctx, orc):
+    from yannq_b200 import api
+
+    for n, m in [(16, 32), (144, 288)]:
+        q = api.RBM(ctx, n, m, True, api.C128)
+        q.init_random(20261203, 0.01)
+        np.testing.assert_array_equal(q.get_params(), orc.init_params(n, m, 20261203, 0.01))
+        q.close()
+
+
+@pytest.mark.parametrize("n,m", [(10, 10), (16, 32), (64, 256), (144, 288)])
+def test_theta_bit_exact(ctx, orc, n, m):
+    from yannq_b200 import api
+
+    q, p = _rbm(api, ctx, orc, n, m, 5, 0.3, api.C128)
+    rng = np.random.default_rng(n)
+    s = _rand_sigma(rng, 17, n)
+    got = q.theta(s)
+    want = np.array([orc.theta(n, m, p, x) for x in s])
+    np.testing.assert_array_equal(got, want)
+    q.close()
+
+
+@pytest.mark.parametrize("dtype", [1, 0])
+def test_log_psi_and_ratios(ctx, orc, dtype):
+    from yannq_b200 import api
+
+    n = m = 10
+    q, p = _rbm(api, ctx, orc, n, m, 7, 1.0, dtype)  # Tests/TestRBMStates.cpp: N = M = 10, N(0, 1)
+    rng = np.random.default_rng(1)
+    s = _rand_sigma(rng, 64, n)
+    th = np.array([orc.theta(n, m, p, x) for x in s])
+    tol = TOL64 if dtype == api.C128 else TOL32
+    lp = q.log_psi(s)
+    want = np.array([orc.logpsi(n, m, p, x) for x in s])
+    assert np.max(np.abs(np.exp(lp - want) - 1)) < 1e-12  # log psi is always evaluated in FP64
+    for nf in (1, 2):
+        flips = np.array([rng.choice(n, nf, replace=False) for _ in range(len(s))], np.int32)
+        got = q.log_ratio(s, th, flips)
+        ref = np.array([orc.logratio(n, m, p, x, t, f) for x, t, f in zip(s, th, flips)])
+        # compare modulo 2 pi i (Tests/TestRBMStates.cpp IsSameRatio)
+        assert np.max(np.abs(np.exp(got - ref) - 1)) < tol
+
+
+def test_log_deriv(ctx, orc):
+    from yannq_b200 import api
+
+    n, m = 12, 24
+    q, p = _rbm(api, ctx, orc, n, m, 3, 0.5, api.C128)
+    rng = np.random.default_rng(2)
+    s = _rand_sigma(rng, 9, n)
+    th = np.array([orc.theta(n, m, p, x) for x in s])
+    got = q.log_deriv(s, th)
+    want = np.array([orc.logderiv(n, m, p, x, t) for x, t in zip(s, th)])
+    assert np.max(np.abs(got - want)) <= TOL64 * max(1.0, np.max(np.abs(want)))
+
+
+HAMS = [
+    ("tfi", lambda o: o.Ham.tfi(12, -1.0, -1.0)),
+    ("tfi_h", lambda o: o.Ham.tfi(12, 1.0, 0.2)),
+    ("xxz", lambda o: o.Ham.xxz(12, 1.0, 1.0, True)),
+    ("xxz_d", lambda o: o.Ham.xxz(10, 0.7, 1.3, False)),
+    ("tfi2d", lambda o: o.Ham.tfi2d(3, 4, -1.0, -3.0)),
+]
+
+
+def _dev_ham(api, ctx, h):
+    if h.kind == 2:
+        return api.Hamiltonian.tfi2d(ctx, h.lx, h.ly, h.J, h.h)
+    if h.kind == 1:
+        return api.Hamiltonian.xxz(ctx, h.n, h.J, h.h, h.sign < 0)
+    return api.Hamiltonian.tfi(ctx, h.n, h.J, h.h)
+
+
+@pytest.mark.parametrize("name,mk", HAMS, ids=[h[0] for h in HAMS])
+def test_flip_enumeration_bit_exact(ctx, orc, name, mk):
+    """Every configuration of the 2^n basis: the device's (mask, coeff) list and
+    diagonal equal the oracle's state-form enumeration, which equals the
+    reference column form (tests/test_oracle_ham.py)."""
+    from yannq_b200 import api
+
+    h = mk(orc)
+    H = _dev_ham(api, ctx, h)
+    n = h.n
+    cols = np.arange(1 << n)
+    sig = np.array([orc.sigma_of(c, n) for c in cols])
+    a, b, c, d = H.enumerate(sig)
+    for k in range(0, len(cols), 7):
+        dg, masks, coeffs = orc.ham_enumerate(h, sig[k])
+        gm = np.array([(1 << int(x)) | ((1 << int(y)) if y >= 0 else 0) for x, y in zip(a[k], b[k])], np.uint64)
+        np.testing.assert_array_equal(gm, masks)
+        np.testing.assert_array_equal(c[k], coeffs)
+        assert d[k] == dg
+    H.close()
+
+
+@pytest.mark.parametrize("name,mk", HAMS, ids=[h[0] for h in HAMS])
+@pytest.mark.parametrize("dtype", [1, 0])
+def test_eloc_parity(ctx, orc, name, mk, dtype):
+    from yannq_b200 import api
+
+    h = mk(orc)
+    n, m = h.n, 2 * h.n
+    q, p = _rbm(api, ctx, orc, n, m, 11, 0.2, dtype)
+    H = _dev_ham(api, ctx, h)
+    rng = np.random.default_rng(3)
+    s = _rand_sigma(rng, 200, n)
+    th = np.array([orc.theta(n, m, p, x) for x in s])
+    got = H.eloc(q, s, th)
+    want = orc.eloc(h, m, p, s, th)
+    scale = np.abs(h.J) * n + np.abs(h.h) * n
+    tol = TOL64 if dtype == api.C128 else TOL32
+    assert np.max(np.abs(got - want)) / scale < tol
+    H.close()
+    q.close()
+
+
+def test_eloc_full_size_2d(ctx, orc):
+    """12 x 12 torus, alpha = 2 (the precision workload's machine): FP64 kernel vs oracle."""
+    from yannq_b200 import api
+
+    h = orc.Ham.tfi2d(12, 12, -1.0, -3.0)
+    n, m = 144, 288
+    q, p = _rbm(api, ctx, orc, n, m, 20261203, 0.01, api.C128)
+    H = _dev_ham(api, ctx, h)
+    rng = np.random.default_rng(4)
+    s = _rand_sigma(rng, 32, n)
+    th = np.array([orc.theta(n, m, p, x) for x in s])
+    got = H.eloc(q, s, th)
+    want = orc.eloc(h, m, p, s, th)
+    assert np.max(np.abs(got - want)) / (4 * n) < TOL64

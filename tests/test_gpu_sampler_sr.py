@@ -1,0 +1,209 @@
+"""GPU parity of the sampler and the SR step against the oracle (C-ABI calls).
+
+* FP64 sampler: with the same Philox streams the device chains equal the
+  oracle's restated SamplerMT draw for draw (sigma bit-exact, theta within
+  1e-13 relative) for local, any-pair and neighbour-pair moves.
+* complex64 sampler: chi^2 against exact |psi|^2.
+* SR (FP64): E_loc, oloc, F, S/T and the solution v against the oracle's
+  restated SRMat on identical samples; S-mode LLT, T-mode dual and CG agree.
+* A whole yq_vmc_iteration trajectory (sample, SR, SGD) tracks the oracle loop.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from yannq_b200 import api
+
+    c = api.Context(0)
+    yield c
+    c.close()
+
+
+def _mk(api, ctx, orc, n, m, seed, sd, dtype):
+    q = api.RBM(ctx, n, m, True, dtype)
+    p = orc.init_params(n, m, seed, sd)
+    q.set_params(p)
+    return q, p
+
+
+@pytest.mark.parametrize("move,nup", [(0, -1), (1, 5), (2, 5)])
+def test_sampler_fp64_matches_oracle_draw_for_draw(ctx, orc, move, nup):
+    from yannq_b200 import api
+
+    n, m = 10, 20
+    q, p = _mk(api, ctx, orc, n, m, 21, 0.3, api.C128)
+    S = api.Sampler(q, 32, move, nup)
+    S.sample(6, 4, seed=99, epoch=3, reinit=True)
+    s, th = S.get_samples()
+    os_, oth, ocs, oacc = orc.sample(n, m, p, 32, move=move, nup=nup, seed=99, epoch=3, reinit=True, n_sweeps=6,
+                                     n_discard=4)
+    np.testing.assert_array_equal(s, os_)
+    assert np.max(np.abs(th - oth)) <= 1e-13 * max(1.0, np.max(np.abs(oth)))
+    np.testing.assert_array_equal(S.get_accepts(), oacc)
+    np.testing.assert_array_equal(S.get_chains(), ocs)
+    # continue the chains without re-initialisation
+    S.sample(3, 0, seed=99, epoch=4, reinit=False)
+    s2, _ = S.get_samples()
+    os2, _, _, _ = orc.sample(n, m, p, 32, move=move, nup=nup, seed=99, epoch=4, reinit=False, n_sweeps=3,
+                              n_discard=0, chain_sigma=ocs)
+    np.testing.assert_array_equal(s2, os2)
+    S.close()
+    q.close()
+
+
+def test_sampler_fp64_full_size_draw_for_draw(ctx, orc):
+    """12 x 12 lattice, alpha = 2: the first 8 chains of the precision workload."""
+    from yannq_b200 import api
+
+    n, m = 144, 288
+    q, p = _mk(api, ctx, orc, n, m, 20261203, 0.01, api.C128)
+    S = api.Sampler(q, 8, 0, -1)
+    S.sample(2, 2, seed=20261203, epoch=0, reinit=True)
+    s, th = S.get_samples()
+    os_, oth, _, _ = orc.sample(n, m, p, 8, seed=20261203, epoch=0, reinit=True, n_sweeps=2, n_discard=2)
+    np.testing.assert_array_equal(s, os_)
+    assert np.max(np.abs(th - oth)) <= 1e-13 * max(1.0, np.max(np.abs(oth)))
+
+
+@pytest.mark.parametrize("move", [0, 2])
+def test_sampler_c64_distribution(ctx, orc, move):
+    from yannq_b200 import api
+
+    n, m = 6, 6
+    q, p = _mk(api, ctx, orc, n, m, 3, 0.25, api.C64)
+    nup = -1 if move == 0 else 3
+    S = api.Sampler(q, 512, move, nup)
+    S.sample(40, 100, seed=17, epoch=0, reinit=True)
+    s, _ = S.get_samples(theta=False)
+    basis = orc.basis(n)
+    psi = np.array([orc.psi(n, m, p, orc.sigma_of(b, n)) for b in basis])
+    pr = np.abs(psi) ** 2
+    if move:
+        pr = np.where([bin(b).count("1") == 3 for b in range(1 << n)], pr, 0)
+        assert np.all((s == -1).sum(1) == 3)
+    pr /= pr.sum()
+    counts = np.bincount([orc.index_of(x) for x in s], minlength=1 << n)
+    N = len(s)
+    sel = pr * N > 20
+    chi2 = (((counts - N * pr) ** 2) / (N * pr))[sel].sum()
+    dof = sel.sum() - 1
+    assert chi2 < 4 * dof + 30, (chi2, dof)
+
+
+def _sr_case(api, ctx, orc, ham_o, n, m, chains, sweeps, mode):
+    q, p = _mk(api, ctx, orc, n, m, 8, 0.1, api.C128)
+    s, th, _, _ = orc.sample(n, m, p, chains, seed=5, n_sweeps=sweeps, n_discard=20)
+    if ham_o.kind == 0:
+        H = api.Hamiltonian.tfi(ctx, n, ham_o.J, ham_o.h)
+    else:
+        H = api.Hamiltonian.xxz(ctx, n, ham_o.J, ham_o.h, ham_o.sign < 0)
+    S = api.Sampler(q, chains)
+    S.put_samples(s, th)
+    sr = api.SR(q, H, S, mode, api.PREC_FP64)
+    sr.construct()
+    return q, p, s, th, H, S, sr
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_sr_fp64_matches_oracle(ctx, orc, mode):
+    from yannq_b200 import api
+
+    n, m = 8, 16
+    h = orc.Ham.tfi(n, -1.0, -1.0)
+    # S-mode: Ns = 256 > P = 152; T-mode forced on the same samples
+    q, p, s, th, H, S, sr = _sr_case(api, ctx, orc, h, n, m, 32, 8, mode)
+    P = q.dim
+    ref = orc.sr_step(h, m, p, s, th, 1e-3, orc.SR_S, orc.SOLVE_LLT)
+    e, var = sr.energy()
+    assert e == pytest.approx(ref["energy"], rel=1e-12)
+    assert var == pytest.approx(ref["energy_var"], rel=1e-9, abs=1e-12)
+    np.testing.assert_allclose(sr.get(0, len(s)), ref["elocs"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(sr.get(1, P), ref["oloc"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(sr.get(2, P), ref["grad"], rtol=1e-10, atol=1e-13)
+    v, _, _ = sr.solve(1e-3, api.SOLVE_LLT)
+    assert np.max(np.abs(v - ref["v"])) <= 1e-9 * np.max(np.abs(ref["v"]))
+    for x in (sr, S, H, q):
+        x.close()
+
+
+def test_sr_matrix_and_cg(ctx, orc):
+    from yannq_b200 import api
+
+    n, m = 6, 12
+    h = orc.Ham.xxz(n, 1.0, 1.0, True)
+    q, p, s, th, H, S, sr = _sr_case(api, ctx, orc, h, n, m, 16, 4, api.SR_T)  # Ns = 64 < P = 90
+    O = np.array([orc.logderiv(n, m, p, a, b) for a, b in zip(s, th)])
+    Oc = O - O.mean(0)
+    T = sr.matrix()
+    Tw = Oc @ Oc.conj().T / len(s)
+    low = np.tril_indices(len(s))
+    assert np.max(np.abs(T[low] - Tw[low])) < 1e-12 * np.max(np.abs(Tw))
+    ref = orc.sr_step(h, m, p, s, th, 1e-2, orc.SR_S, orc.SOLVE_LLT)
+    v_llt, _, _ = sr.solve(1e-2, api.SOLVE_LLT)
+    v_cg, it, rr = sr.solve(1e-2, api.SOLVE_CG, 1e-12)
+    assert rr < 1e-12 and it > 0
+    for v in (v_llt, v_cg):
+        assert np.max(np.abs(v - ref["v"])) <= 1e-8 * np.max(np.abs(ref["v"]))
+    for x in (sr, S, H, q):
+        x.close()
+
+
+def test_not_positive_definite_is_reported(ctx, orc):
+    """Shift 0 with Ns < P makes T singular (rank <= Ns - 1 after centring): the
+    Cholesky reports YQ_E_NOT_PD instead of returning garbage."""
+    from yannq_b200 import api
+
+    n, m = 6, 12
+    h = orc.Ham.tfi(n, -1.0, -1.0)
+    q, p, s, th, H, S, sr = _sr_case(api, ctx, orc, h, n, m, 8, 4, api.SR_T)
+    with pytest.raises(api.YQError) as e:
+        sr.solve(0.0, api.SOLVE_LLT)
+    assert e.value.code == api.E_NOT_PD
+    v, _, _ = sr.solve(1e-3, api.SOLVE_LLT)  # the context stays usable
+    assert np.all(np.isfinite(v))
+    for x in (sr, S, H, q):
+        x.close()
+
+
+def test_vmc_iterations_track_oracle_loop(ctx, orc):
+    """Runners/RunRBM.hpp:151-221 on the device vs the oracle loop, FP64:
+    identical samples each iteration, parameters within 1e-9 after 3 updates."""
+    from yannq_b200 import api
+
+    n, m = 8, 16
+    h = orc.Ham.tfi(n, -1.0, -1.0)
+    q, p = _mk(api, ctx, orc, n, m, 20261203, 0.01, api.C128)
+    H = api.Hamiltonian.tfi(ctx, n, -1.0, -1.0)
+    S = api.Sampler(q, 16)
+    sr = api.SR(q, H, S, api.SR_AUTO, api.PREC_FP64)
+    pp = p.copy()
+    for it in range(3):
+        r = sr.iteration(n_sweeps=16, n_discard=16, seed=7, epoch=it, shift=1e-3, lr=0.01, reinit=True)
+        s, th, _, _ = orc.sample(n, m, pp, 16, seed=7, epoch=it, n_sweeps=16, n_discard=16)
+        ref = orc.sr_step(h, m, pp, s, th, 1e-3, orc.SR_T, orc.SOLVE_LLT)
+        pp = pp - 0.01 * ref["v"]
+        assert r.energy == pytest.approx(ref["energy"], rel=1e-11)
+        got = q.get_params()
+        assert np.max(np.abs(got - pp)) < 1e-9 * np.max(np.abs(pp))
+        assert r.update_norm == pytest.approx(np.linalg.norm(ref["v"]), rel=1e-8)
+    for x in (sr, S, H, q):
+        x.close()
+
+
+def test_vmc_converges_towards_ed(ctx, orc):
+    from yannq_b200 import api
+
+    n, m = 10, 20
+    e0 = orc.ed_ground(orc.Ham.tfi(n, -1.0, -1.0))
+    q = api.RBM(ctx, n, m, True, api.C128)
+    q.init_random(1, 0.01)
+    H = api.Hamiltonian.tfi(ctx, n, -1.0, -1.0)
+    S = api.Sampler(q, 64)
+    sr = api.SR(q, H, S, api.SR_AUTO, api.PREC_FP64)
+    es = [sr.iteration(16, 16, 3, it, 1e-3, 0.05).energy for it in range(60)]
+    assert np.mean(es[-10:]) < es[0]
+    assert abs(np.mean(es[-10:]) - e0) / abs(e0) < 0.02

@@ -1,0 +1,373 @@
+"""ctypes binding of libyannq_b200.so (include/yannq_b200.h).
+
+This is the Python-side harness over the C ABI used by the tests and by
+bench.py; the product is the shared library and its C/C++ headers.  There is no
+fallback: importing this module fails if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libyannq_b200.so")
+
+OK, E_ARG, E_CUDA, E_NOMEM, E_NOT_PD, E_NONFINITE, E_TIMEOUT, E_STATE, E_UNSUPPORTED = range(9)
+C64, C128 = 0, 1
+HAM_TFI, HAM_XXZ, HAM_TFI2D = 0, 1, 2
+MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN = 0, 1, 2
+SR_AUTO, SR_S, SR_T = 0, 1, 2
+PREC_FP64, PREC_MIXED = 0, 1
+SOLVE_LLT, SOLVE_CG = 0, 1
+STAGES = {"sample": 0, "eloc": 1, "O": 2, "gram": 3, "solve": 4, "update": 5, "total": 6, "mean": 7}
+
+
+class YQError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"yannq_b200 error {code}: {msg}")
+        self.code = code
+
+
+class IterParams(C.Structure):
+    _fields_ = [("n_sweeps", C.c_int), ("n_discard", C.c_int), ("reinit", C.c_int), ("seed", C.c_uint64),
+                ("epoch", C.c_uint32), ("shift", C.c_double), ("lr", C.c_double), ("solver", C.c_int),
+                ("cg_tol", C.c_double), ("ir_steps", C.c_int)]
+
+
+class IterResult(C.Structure):
+    _fields_ = [("energy", C.c_double), ("energy_var", C.c_double), ("update_norm", C.c_double),
+                ("cg_err", C.c_double), ("accept_rate", C.c_double), ("status", C.c_int)]
+
+
+# every symbol declared in include/yannq_b200.h with its argument types
+_vp, _i, _d, _u64, _u32, _sz = C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_uint32, C.c_size_t
+SIGNATURES = {
+    "yq_last_error": [C.c_char_p, _sz],
+    "yq_version": [],
+    "yq_launch_count": [_vp],
+    "yq_host_alloc": [_sz, _vp],
+    "yq_host_free": [_vp],
+    "yq_ctx_create": [_i, _vp],
+    "yq_ctx_destroy": [_vp],
+    "yq_ctx_synchronize": [_vp],
+    "yq_ctx_stage_ms": [_vp, _i, _vp],
+    "yq_rbm_create": [_vp, _i, _i, _i, _i, _vp],
+    "yq_rbm_destroy": [_vp],
+    "yq_rbm_dim": [_vp, _vp],
+    "yq_rbm_set_params": [_vp, _vp],
+    "yq_rbm_get_params": [_vp, _vp],
+    "yq_rbm_update_params": [_vp, _vp],
+    "yq_rbm_init_random": [_vp, _u64, _d],
+    "yq_rbm_theta": [_vp, _i, _vp, _vp],
+    "yq_rbm_log_psi": [_vp, _i, _vp, _vp],
+    "yq_rbm_log_ratio": [_vp, _i, _vp, _vp, _i, _vp, _vp],
+    "yq_rbm_log_deriv": [_vp, _i, _vp, _vp, _vp],
+    "yq_ham_create": [_vp, _i, _i, _i, _i, _d, _d, _i, _vp],
+    "yq_ham_destroy": [_vp],
+    "yq_ham_enumerate": [_vp, _i, _vp, _vp, _vp, _vp, _vp],
+    "yq_eloc": [_vp, _vp, _i, _vp, _vp, _vp],
+    "yq_sampler_create": [_vp, _i, _i, _i, _i, _vp],
+    "yq_sampler_destroy": [_vp],
+    "yq_sampler_set_resync": [_vp, _i],
+    "yq_sampler_set_chains": [_vp, _vp],
+    "yq_sampler_get_chains": [_vp, _vp],
+    "yq_sample": [_vp, _i, _i, _u64, _u32, _i],
+    "yq_sampler_num_samples": [_vp, _vp],
+    "yq_sampler_get_samples": [_vp, _vp, _vp],
+    "yq_sampler_get_accepts": [_vp, _vp],
+    "yq_sampler_put_samples": [_vp, _i, _vp, _vp],
+    "yq_sr_create": [_vp, _vp, _vp, _i, _i, _vp],
+    "yq_sr_destroy": [_vp],
+    "yq_sr_construct": [_vp],
+    "yq_sr_energy": [_vp, _vp, _vp],
+    "yq_sr_get": [_vp, _i, _vp],
+    "yq_sr_solve": [_vp, _d, _i, _d, _vp, _vp, _vp],
+    "yq_sr_matrix": [_vp, _vp, _vp],
+    "yq_vmc_iteration": [_vp, _vp, _vp],
+}
+
+_lib = None
+
+
+def lib():
+    """Load libyannq_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C yannq_b200/csrc` "
+                              "(or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_char_p if name == "yq_version" else C.c_int
+        _lib = L
+    return _lib
+
+
+def last_error():
+    buf = C.create_string_buffer(4096)
+    lib().yq_last_error(buf, 4096)
+    return buf.value.decode()
+
+
+def check(code):
+    if code != OK:
+        raise YQError(code, last_error())
+
+
+def launch_count():
+    v = C.c_uint64()
+    check(lib().yq_launch_count(C.byref(v)))
+    return v.value
+
+
+class PinnedArray:
+    """numpy view of a page-locked host buffer from yq_host_alloc."""
+
+    def __init__(self, shape, dtype):
+        self.dtype = np.dtype(dtype)
+        nbytes = int(np.prod(shape)) * self.dtype.itemsize
+        ptr = C.c_void_p()
+        check(lib().yq_host_alloc(nbytes, C.byref(ptr)))
+        self.ptr = ptr
+        buf = (C.c_char * nbytes).from_address(ptr.value)
+        self.array = np.frombuffer(buf, dtype=self.dtype).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            self.array = None
+            check(lib().yq_host_free(self.ptr))
+            self.ptr = None
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _s8(x):
+    return np.ascontiguousarray(x, dtype=np.int8)
+
+
+def _c128(x):
+    return np.ascontiguousarray(x, dtype=np.complex128)
+
+
+class Context:
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        check(lib().yq_ctx_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            check(lib().yq_ctx_destroy(self.h))
+            self.h = None
+
+    def synchronize(self):
+        check(lib().yq_ctx_synchronize(self.h))
+
+    def stage_ms(self, stage):
+        v = C.c_float()
+        check(lib().yq_ctx_stage_ms(self.h, STAGES.get(stage, stage), C.byref(v)))
+        return v.value
+
+
+class RBM:
+    """RBM<complex<float|double>>(n, m, useBias) on the device (Machines/RBM.hpp)."""
+
+    def __init__(self, ctx, n, m, use_bias=True, dtype=C128):
+        self.ctx, self.n, self.m, self.use_bias, self.dtype = ctx, n, m, use_bias, dtype
+        h = C.c_void_p()
+        check(lib().yq_rbm_create(ctx.h, n, m, int(use_bias), dtype, C.byref(h)))
+        self.h = h
+        d = C.c_size_t()
+        check(lib().yq_rbm_dim(h, C.byref(d)))
+        self.dim = d.value
+
+    def close(self):
+        if self.h:
+            check(lib().yq_rbm_destroy(self.h))
+            self.h = None
+
+    def set_params(self, p):
+        p = _c128(p)
+        assert p.shape == (self.dim,)
+        check(lib().yq_rbm_set_params(self.h, _p(p)))
+
+    def get_params(self, out=None):
+        out = np.zeros(self.dim, np.complex128) if out is None else out
+        check(lib().yq_rbm_get_params(self.h, _p(out)))
+        return out
+
+    def update_params(self, d):
+        check(lib().yq_rbm_update_params(self.h, _p(_c128(d))))
+
+    def init_random(self, seed, sd):
+        check(lib().yq_rbm_init_random(self.h, seed, sd))
+
+    def theta(self, sigma):
+        s = _s8(sigma).reshape(-1, self.n)
+        out = np.zeros((s.shape[0], self.m), np.complex128)
+        check(lib().yq_rbm_theta(self.h, s.shape[0], _p(s), _p(out)))
+        return out
+
+    def log_psi(self, sigma):
+        s = _s8(sigma).reshape(-1, self.n)
+        out = np.zeros(s.shape[0], np.complex128)
+        check(lib().yq_rbm_log_psi(self.h, s.shape[0], _p(s), _p(out)))
+        return out
+
+    def log_ratio(self, sigma, theta, flips):
+        s = _s8(sigma).reshape(-1, self.n)
+        th = _c128(theta).reshape(s.shape[0], self.m)
+        f = np.ascontiguousarray(flips, dtype=np.int32).reshape(s.shape[0], -1)
+        out = np.zeros(s.shape[0], np.complex128)
+        check(lib().yq_rbm_log_ratio(self.h, s.shape[0], _p(s), _p(th), f.shape[1], _p(f), _p(out)))
+        return out
+
+    def log_deriv(self, sigma, theta):
+        s = _s8(sigma).reshape(-1, self.n)
+        th = _c128(theta).reshape(s.shape[0], self.m)
+        out = np.zeros((s.shape[0], self.dim), np.complex128)
+        check(lib().yq_rbm_log_deriv(self.h, s.shape[0], _p(s), _p(th), _p(out)))
+        return out
+
+
+class Hamiltonian:
+    def __init__(self, ctx, kind, n, J, h, sign_rule=False, lx=0, ly=0):
+        self.ctx, self.kind, self.n = ctx, kind, n
+        hh = C.c_void_p()
+        check(lib().yq_ham_create(ctx.h, kind, n, lx, ly, J, h, int(sign_rule), C.byref(hh)))
+        self.h = hh
+
+    @classmethod
+    def tfi(cls, ctx, n, J, h):
+        return cls(ctx, HAM_TFI, n, J, h)
+
+    @classmethod
+    def xxz(cls, ctx, n, J, delta, sign_rule=False):
+        return cls(ctx, HAM_XXZ, n, J, delta, sign_rule)
+
+    @classmethod
+    def tfi2d(cls, ctx, lx, ly, J, h):
+        return cls(ctx, HAM_TFI2D, lx * ly, J, h, False, lx, ly)
+
+    def close(self):
+        if self.h:
+            check(lib().yq_ham_destroy(self.h))
+            self.h = None
+
+    def enumerate(self, sigma):
+        s = _s8(sigma).reshape(-1, self.n)
+        ns = s.shape[0]
+        a = np.zeros((ns, self.n), np.int32)
+        b = np.zeros((ns, self.n), np.int32)
+        c = np.zeros((ns, self.n))
+        d = np.zeros(ns)
+        check(lib().yq_ham_enumerate(self.h, ns, _p(s), _p(a), _p(b), _p(c), _p(d)))
+        return a, b, c, d
+
+    def eloc(self, rbm, sigma, theta):
+        s = _s8(sigma).reshape(-1, self.n)
+        th = _c128(theta).reshape(s.shape[0], rbm.m)
+        out = np.zeros(s.shape[0], np.complex128)
+        check(lib().yq_eloc(self.h, rbm.h, s.shape[0], _p(s), _p(th), _p(out)))
+        return out
+
+
+class Sampler:
+    def __init__(self, rbm, n_chains, move=MOVE_LOCAL, nup=-1, sweep_len=0):
+        self.rbm, self.n_chains = rbm, n_chains
+        h = C.c_void_p()
+        check(lib().yq_sampler_create(rbm.h, n_chains, move, nup, sweep_len, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            check(lib().yq_sampler_destroy(self.h))
+            self.h = None
+
+    def set_resync(self, every):
+        check(lib().yq_sampler_set_resync(self.h, every))
+
+    def set_chains(self, sigma):
+        check(lib().yq_sampler_set_chains(self.h, _p(_s8(sigma))))
+
+    def get_chains(self):
+        out = np.zeros((self.n_chains, self.rbm.n), np.int8)
+        check(lib().yq_sampler_get_chains(self.h, _p(out)))
+        return out
+
+    def sample(self, n_sweeps, n_discard, seed, epoch=0, reinit=True):
+        check(lib().yq_sample(self.h, n_sweeps, n_discard, seed, epoch, int(reinit)))
+
+    def num_samples(self):
+        v = C.c_int()
+        check(lib().yq_sampler_num_samples(self.h, C.byref(v)))
+        return v.value
+
+    def get_samples(self, theta=True):
+        ns = self.num_samples()
+        s = np.zeros((ns, self.rbm.n), np.int8)
+        th = np.zeros((ns, self.rbm.m), np.complex128) if theta else None
+        check(lib().yq_sampler_get_samples(self.h, _p(s), _p(th)))
+        return s, th
+
+    def get_accepts(self):
+        out = np.zeros(self.n_chains, np.uint64)
+        check(lib().yq_sampler_get_accepts(self.h, _p(out)))
+        return out
+
+    def put_samples(self, sigma, theta):
+        s = _s8(sigma)
+        th = _c128(theta)
+        check(lib().yq_sampler_put_samples(self.h, s.shape[0], _p(s), _p(th)))
+
+
+class SR:
+    def __init__(self, rbm, ham, sampler, mode=SR_AUTO, precision=PREC_FP64):
+        self.rbm = rbm
+        h = C.c_void_p()
+        check(lib().yq_sr_create(rbm.h, ham.h, sampler.h, mode, precision, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            check(lib().yq_sr_destroy(self.h))
+            self.h = None
+
+    def construct(self):
+        check(lib().yq_sr_construct(self.h))
+
+    def energy(self):
+        e, v = C.c_double(), C.c_double()
+        check(lib().yq_sr_energy(self.h, C.byref(e), C.byref(v)))
+        return e.value, v.value
+
+    def get(self, which, size):
+        out = np.zeros(size, np.complex128)
+        check(lib().yq_sr_get(self.h, which, _p(out)))
+        return out
+
+    def solve(self, shift, solver=SOLVE_LLT, cg_tol=1e-4):
+        v = np.zeros(self.rbm.dim, np.complex128)
+        it, rr = C.c_int(), C.c_double()
+        check(lib().yq_sr_solve(self.h, shift, solver, cg_tol, _p(v), C.byref(it), C.byref(rr)))
+        return v, it.value, rr.value
+
+    def matrix(self):
+        d = C.c_int()
+        check(lib().yq_sr_matrix(self.h, C.byref(d), None))
+        out = np.zeros((d.value, d.value), np.complex128)
+        check(lib().yq_sr_matrix(self.h, C.byref(d), _p(out)))
+        return out
+
+    def iteration(self, n_sweeps, n_discard, seed, epoch, shift, lr, reinit=True, solver=SOLVE_LLT, cg_tol=1e-4,
+                  ir_steps=0):
+        p = IterParams(n_sweeps, n_discard, int(reinit), seed, epoch, shift, lr, solver, cg_tol, ir_steps)
+        r = IterResult()
+        check(lib().yq_vmc_iteration(self.h, C.byref(p), C.byref(r)))
+        return r

@@ -1,0 +1,349 @@
+// tcgen05 Gram kernel of the mixed-precision SR path (see gram_tc.hpp).
+//
+// One CTA per 128 x 256 output tile of the lower triangle of T (T_re tiles read
+// A rows from X, T_im tiles from Y; B rows always from X).  Warp roles:
+//   warp 0       TMA producer: 4-stage ring of {A 128x64, B 256x64} BF16 tiles,
+//                128-byte swizzle, completion counted on "full" mbarriers;
+//   warp 1       TMEM allocator and single-thread MMA issuer: 4 x
+//                tcgen05.mma.cta_group::1.kind::f16 (M128 N256 K16) per stage,
+//                tcgen05.commit releases the stage ("empty") and finally "done";
+//   warps 2..5   epilogue: tcgen05.ld 32x32b.x32 from TMEM, scale, FP64 store.
+// K runs over three segments (hi.hi, hi.lo, lo.hi) of the split operands.
+// Every mbarrier wait is bounded: on timeout the kernel sets DS_TIMEOUT in the
+// status word, the other roles stop at their next wait, and TMEM is released.
+// No cluster launch and no multicast: each CTA fetches its own tiles.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <mutex>
+
+#include "gram_tc.hpp"
+#include "internal.hpp"
+
+namespace yq {
+
+// ---------------------------------------------------------------------------
+// Operand split: X = [Re | Im], Y = [Im | -Re]; x = hi + lo with hi = bf16(x),
+// lo = bf16(x - hi).
+__device__ __forceinline__ void split_bf16(float v, uint16_t& hi, uint16_t& lo) {
+    __nv_bfloat16 h = __float2bfloat16_rn(v);
+    __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+}
+
+__global__ void split_operands_kernel(const c64* __restrict__ O, int ns, size_t P, size_t rows_pad, size_t kpad,
+                                      uint16_t* __restrict__ xh, uint16_t* __restrict__ xl, uint16_t* __restrict__ yh,
+                                      uint16_t* __restrict__ yl) {
+    for (size_t row = blockIdx.y; row < rows_pad; row += gridDim.y) {
+        for (size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x; k < kpad; k += size_t(gridDim.x) * blockDim.x) {
+            float xv = 0.f, yv = 0.f;
+            if (row < size_t(ns)) {
+                if (k < P) {
+                    c64 o = O[row * P + k];
+                    xv = o.re;
+                    yv = o.im;
+                } else if (k < 2 * P) {
+                    c64 o = O[row * P + (k - P)];
+                    xv = o.im;
+                    yv = -o.re;
+                }
+            }
+            uint16_t a, b;
+            const size_t q = row * kpad + k;
+            split_bf16(xv, a, b);
+            xh[q] = a;
+            xl[q] = b;
+            split_bf16(yv, a, b);
+            yh[q] = a;
+            yl[q] = b;
+        }
+    }
+}
+
+void gram_tc_prepare_operands(const c64* O, int ns, size_t P, uint16_t* xh, uint16_t* xl, uint16_t* yh, uint16_t* yl,
+                              cudaStream_t st) {
+    const size_t kpad = gram_tc_kpad(P), rows = gram_tc_rows(ns);
+    dim3 g(std::min<unsigned>(64u, cdiv_u(kpad, 256)), unsigned(std::min<size_t>(rows, 65535)));
+    split_operands_kernel<<<g, 256, 0, st>>>(O, ns, P, rows, kpad, xh, xl, yh, yl);
+    YQ_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+constexpr int TC_STAGES = 4;
+constexpr int TC_BNW = 256;                        // output columns per tile
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;      // 16 KiB
+constexpr int TC_B_BYTES = TC_BNW * TC_BK * 2;     // 32 KiB
+constexpr int TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;
+constexpr int TC_TMEM_COLS = 256;
+constexpr int TC_THREADS = 192;
+constexpr size_t TC_SMEM = size_t(TC_STAGES) * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+
+struct TcParams {
+    int ns, nt;            // samples, 128-row tiles per half
+    int tiles_per_half;
+    int kb_per_seg;        // kpad / 64
+    c128* G;
+    size_t ldg;
+    double alpha, shift;
+    int* status;
+    unsigned wait_cap;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait; false on timeout or when another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort_flag, unsigned cap,
+                                          int* status) {
+    for (unsigned it = 0; it < cap; ++it) {
+        if (mbar_try(a, parity)) return true;
+        if (*abort_flag) return false;
+    }
+    *abort_flag = 1;
+    atomicOr(status, DS_TIMEOUT);
+    return false;
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+        : "memory");
+}
+// K-major operand tile with 128-byte swizzle: rows of 128 B, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= uint64_t((saddr >> 4) & 0x3FFFu);  // start address
+    d |= uint64_t(1) << 16;                  // leading byte offset (unused for swizzled K-major)
+    d |= uint64_t(1024 >> 4) << 32;          // stride byte offset: 8 rows x 128 B
+    d |= uint64_t(1) << 46;                  // descriptor version (sm_100)
+    d |= uint64_t(2) << 61;                  // SWIZZLE_128B
+    return d;
+}
+// kind::f16 instruction descriptor: FP32 accumulate, BF16 A and B, K-major, M = 128, N = 256.
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(TC_BNW >> 3) << 17) |
+                              (uint32_t(TC_BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(TC_IDESC), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+
+#define YQ_TMEM_LD_X32(taddr, v)                                                                                   \
+    asm volatile(                                                                                                  \
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18," \
+        "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                                            \
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),        \
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),  \
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),            \
+          "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),            \
+          "=r"(v[30]), "=r"(v[31])                                                                                 \
+        : "r"(taddr))
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    gram_tc_kernel(const __grid_constant__ CUtensorMap mXhA, const __grid_constant__ CUtensorMap mXlA,
+                   const __grid_constant__ CUtensorMap mYhA, const __grid_constant__ CUtensorMap mYlA,
+                   const __grid_constant__ CUtensorMap mXhB, const __grid_constant__ CUtensorMap mXlB, TcParams p) {
+    extern __shared__ uint8_t smem_raw[];
+    // 1024-byte aligned stage buffers, barriers after them
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - raw);
+    uint8_t* bar_area = gbase + size_t(TC_STAGES) * TC_STAGE_BYTES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(bar_area);
+    uint64_t* empty = full + TC_STAGES;
+    uint64_t* done = empty + TC_STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    // tile of this CTA
+    int t = blockIdx.x;
+    const int half = t >= p.tiles_per_half ? 1 : 0;
+    if (half) t -= p.tiles_per_half;
+    int bi = 0;
+    while (bi < p.nt && t >= (bi >> 1) + 1) {
+        t -= (bi >> 1) + 1;
+        ++bi;
+    }
+    const int bj = t;  // 256-column tile, bj <= bi / 2
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        mbar_init(smem_u32(done), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const int total_kb = 3 * p.kb_per_seg;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            for (int kb = 0; kb < total_kb; ++kb) {
+                const int stage = kb % TC_STAGES, round = kb / TC_STAGES;
+                if (round > 0 && !mbar_wait(smem_u32(&empty[stage]), uint32_t((round - 1) & 1), abort_flag,
+                                            p.wait_cap, p.status))
+                    break;
+                const uint32_t fb = smem_u32(&full[stage]);
+                mbar_expect_tx(fb, TC_STAGE_BYTES);
+                const int seg = kb / p.kb_per_seg;
+                const int kx = (kb - seg * p.kb_per_seg) * TC_BK;
+                const CUtensorMap* ma = half ? (seg == 2 ? &mYlA : &mYhA) : (seg == 2 ? &mXlA : &mXhA);
+                const CUtensorMap* mb = (seg == 1) ? &mXlB : &mXhB;
+                const uint32_t sa = smem_u32(gbase + size_t(stage) * TC_STAGE_BYTES);
+                tma_load_2d(sa, ma, kx, bi * TC_BM, fb);
+                tma_load_2d(sa + TC_A_BYTES, mb, kx, bj * TC_BNW, fb);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            for (int kb = 0; kb < total_kb; ++kb) {
+                const int stage = kb % TC_STAGES, round = kb / TC_STAGES;
+                if (!mbar_wait(smem_u32(&full[stage]), uint32_t(round & 1), abort_flag, p.wait_cap, p.status)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t sa = smem_u32(gbase + size_t(stage) * TC_STAGE_BYTES);
+                const uint32_t sb = sa + TC_A_BYTES;
+#pragma unroll
+                for (int k = 0; k < TC_BK / 16; ++k)
+                    umma_bf16(tmem, sw128_desc(sa + k * 32), sw128_desc(sb + k * 32), (kb | k) != 0 ? 1u : 0u);
+                umma_commit(smem_u32(&empty[stage]));
+            }
+            umma_commit(smem_u32(done));  // tracks every MMA issued above
+        }
+        __syncwarp();
+    } else {
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31
+        const bool ok = mbar_wait(smem_u32(done), 0u, abort_flag, p.wait_cap, p.status);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int lg = warp & 3;
+        const int r = bi * TC_BM + lg * 32 + lane;
+#pragma unroll 1
+        for (int chunk = 0; chunk < TC_BNW / 32; ++chunk) {
+            uint32_t v[32];
+            const uint32_t taddr = tmem + (uint32_t(lg * 32) << 16) + uint32_t(chunk * 32);
+            YQ_TMEM_LD_X32(taddr, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (!ok || r >= p.ns) continue;
+            double* grow = reinterpret_cast<double*>(p.G + size_t(r) * p.ldg) + half;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const int c = bj * TC_BNW + chunk * 32 + i;
+                if (c < p.ns && c <= r) {
+                    double val = p.alpha * double(__uint_as_float(v[i]));
+                    if (!half && c == r) val += p.shift;
+                    grow[2 * size_t(c)] = val;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    });
+    if (!fn) throw Error(YQ_E_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    return fn;
+}
+
+static CUtensorMap make_map(const uint16_t* base, size_t rows, size_t kpad, uint32_t box_rows) {
+    CUtensorMap m;
+    cuuint64_t dims[2] = {cuuint64_t(kpad), cuuint64_t(rows)};
+    cuuint64_t strides[1] = {cuuint64_t(kpad * 2)};
+    cuuint32_t box[2] = {cuuint32_t(TC_BK), box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = get_encode()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<uint16_t*>(base), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(YQ_E_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(int(r)));
+    return m;
+}
+
+void gram_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int ns, size_t P,
+                 c128* G, size_t ldg, double alpha, double shift, int* d_status, cudaStream_t st) {
+    const size_t kpad = gram_tc_kpad(P), rows = gram_tc_rows(ns);
+    YQ_CHECK_ARG(kpad % TC_BK == 0 && rows % TC_BM == 0, "gram_tc: operand padding");
+    YQ_CHECK_ARG(reinterpret_cast<uintptr_t>(xh) % 16 == 0 && reinterpret_cast<uintptr_t>(xl) % 16 == 0 &&
+                     reinterpret_cast<uintptr_t>(yh) % 16 == 0 && reinterpret_cast<uintptr_t>(yl) % 16 == 0,
+                 "gram_tc: operand base addresses must be 16-byte aligned");
+    CUtensorMap mXhA = make_map(xh, rows, kpad, TC_BM), mXlA = make_map(xl, rows, kpad, TC_BM);
+    CUtensorMap mYhA = make_map(yh, rows, kpad, TC_BM), mYlA = make_map(yl, rows, kpad, TC_BM);
+    CUtensorMap mXhB = make_map(xh, rows, kpad, TC_BNW), mXlB = make_map(xl, rows, kpad, TC_BNW);
+    TcParams p;
+    p.ns = ns;
+    p.nt = int(rows / TC_BM);
+    int tph = 0;
+    for (int b = 0; b < p.nt; ++b) tph += (b >> 1) + 1;
+    p.tiles_per_half = tph;
+    p.kb_per_seg = int(kpad / TC_BK);
+    p.G = G;
+    p.ldg = ldg;
+    p.alpha = alpha;
+    p.shift = shift;
+    p.status = d_status;
+    p.wait_cap = 1u << 24;
+    static bool attr = false;
+    if (!attr) {
+        YQ_CUDA(cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TC_SMEM)));
+        attr = true;
+    }
+    gram_tc_kernel<<<2 * tph, TC_THREADS, TC_SMEM, st>>>(mXhA, mXlA, mYhA, mYlA, mXhB, mXlB, p);
+    YQ_LAUNCH_CHECK();
+}
+
+}  // namespace yq

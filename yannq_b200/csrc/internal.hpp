@@ -1,0 +1,112 @@
+// Internal object model of libyannq_b200 (host side).  The C ABI in capi.cu maps
+// each opaque handle of include/yannq_b200.h onto one of these structs.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace yq {
+
+enum Stage { ST_SAMPLE = 0, ST_ELOC = 1, ST_O = 2, ST_GRAM = 3, ST_SOLVE = 4, ST_UPDATE = 5, ST_TOTAL = 6, ST_MEAN = 7,
+             ST_COUNT = 8 };
+
+// Device-side status word bits (set by kernels, read once per call by the host).
+enum : int { DS_NONFINITE = 1, DS_NOT_PD = 2, DS_TIMEOUT = 4 };
+
+}  // namespace yq
+
+struct yq_ctx_s {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start[yq::ST_COUNT] = {};
+    cudaEvent_t ev_stop[yq::ST_COUNT] = {};
+    bool ev_used[yq::ST_COUNT] = {};
+    yq::DevBuf status;  // int device status word
+    yq::DevBuf scratch; // small reduction scratch (doubles)
+
+    void stage_begin(int s);
+    void stage_end(int s);
+    int read_status_and_clear();
+};
+
+struct yq_rbm_s {
+    yq_ctx_s* ctx = nullptr;
+    int n = 0, m = 0;
+    bool use_bias = true;
+    int dtype = YQ_C128;
+    size_t P = 0;
+    yq::DevBuf p64;  // master parameters, c128 [W col-major | a | b]
+    // derived, in the compute type (c64 or c128): W (m x n col-major), a (n), b (m),
+    // tau = tanh(2W) (m x n col-major), tauT (n x m), and Lk = sum_j logcosh(2 W_jk) (c128)
+    yq::DevBuf W, a, b, tau, tauT, Lk;
+    uint64_t version = 1, prepared = 0;
+    void prepare();  // refresh derived arrays after a parameter change
+    size_t csize() const { return dtype == YQ_C64 ? sizeof(yq::c64) : sizeof(yq::c128); }
+};
+
+struct yq_ham_s {
+    yq_ctx_s* ctx = nullptr;
+    int kind = 0, n = 0, lx = 0, ly = 0;
+    double J = 0., h = 0., sign = 1.;
+};
+
+struct yq_sampler_s {
+    yq_rbm_s* q = nullptr;
+    int n_chains = 0, move = 0, nup = -1, sweep_len = 0, resync = 0;
+    bool have_chains = false;
+    yq::DevBuf chains;   // n_chains x n int8
+    yq::DevBuf sigma;    // ns x n int8
+    yq::DevBuf theta;    // ns x m compute type
+    yq::DevBuf acc;      // n_chains u64
+    int ns = 0;
+    uint64_t proposals = 0;  // per chain, last call
+};
+
+struct yq_sr_s {
+    yq_rbm_s* q = nullptr;
+    yq_ham_s* H = nullptr;
+    yq_sampler_s* S = nullptr;
+    int mode_req = YQ_SR_AUTO, precision = YQ_PREC_FP64;
+    int mode = YQ_SR_T;  // resolved at construct
+    int ns = 0;
+    bool constructed = false, solved = false;
+    // per-sample data
+    yq::DevBuf eloc;    // ns c128
+    yq::DevBuf tanhs;   // ns x m compute type
+    yq::DevBuf O;       // ns x P compute type, centred (row per sample)
+    yq::DevBuf part;    // split-reduction partials (c128)
+    yq::DevBuf oloc, grad, v, work_p;   // P c128
+    yq::DevBuf y, rhs, work_s;          // max(ns, dim_pad) c128
+    yq::DevBuf s1, s2, s3, s4;          // solver scratch vectors
+    yq::DevBuf stats;   // double[8]: E, var, mean.re, mean.im, |v|, acc...
+    // dense SR matrix and Cholesky factor (lower, row-major, dim_pad x dim_pad)
+    int dim = 0, dim_pad = 0;
+    yq::DevBuf G, Linv;
+    // mixed precision operands (BF16 hi/lo planes of [Re|Im] and [Im|-Re])
+    yq::DevBuf xh, xl, yh, yl;
+    double host_stats[8] = {};
+};
+
+namespace yq {
+// kernels launched from the objects (defined in the .cu files)
+void rbm_prepare(yq_rbm_s* q);
+void rbm_theta(yq_rbm_s* q, int ns, const int8_t* d_sigma, void* d_theta, bool out_c128);
+void rbm_log_psi(yq_rbm_s* q, int ns, const int8_t* d_sigma, c128* d_out);
+void rbm_log_ratio(yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_theta, int nflip, const int* d_flips,
+                   c128* d_out);
+void rbm_log_deriv(yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_theta, c128* d_out);
+void rbm_init_params_host(int n, int m, bool bias, uint64_t seed, double sd, c128* p);
+
+void sampler_run(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, uint32_t epoch, int reinit);
+
+void ham_enumerate(yq_ham_s* H, int ns, const int8_t* d_sigma, int* d_a, int* d_b, double* d_c, double* d_diag);
+void ham_eloc(yq_ham_s* H, yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_theta, c128* d_out);
+
+void sr_construct(yq_sr_s* sr);
+void sr_solve(yq_sr_s* sr, double shift, int solver, double cg_tol, int ir_steps, int* iters, double* relres);
+void sr_update_params(yq_sr_s* sr, double lr);
+void sr_form_matrix_public(yq_sr_s* sr, double shift);
+}  // namespace yq

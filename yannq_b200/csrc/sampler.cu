@@ -1,0 +1,361 @@
+// Persistent Metropolis sampler: one warp per chain.
+//
+// Restates Samplers/SamplerMT.hpp (nTmps = 1) driving LocalSweeper
+// (Samplers/LocalSweeper.hpp:32-53) or SwapSweeper (Samplers/SwapSweeper.hpp:28-57,
+// plus a neighbour-pair variant).  Per chain the warp holds
+//   sigma           int8 in shared memory (one row per warp),
+//   theta_j, t_j    = theta and tanh(theta) for j = lane + 32 r in registers,
+// and evaluates the reference's acceptance min(1, exp(2 beta Re logRatio)) with
+// the product form of ratio.cuh: per proposal one column of tau = tanh(2W)
+// (coalesced, L2-resident), one log per lane and a butterfly warp sum.  On an
+// accepted move theta follows the reference's incremental update exactly
+// (States/RBMState.hpp:248-266) and t follows tanh's addition formula; t is
+// recomputed from theta at the end of every sweep, theta itself from sigma in
+// FP64 every `resync` sweeps when requested.
+//
+// Random numbers: Philox4x32-10 with counter (proposal, epoch, chain, tag); the
+// next proposal's columns are prefetched into L1 while the current one is scored.
+#include "internal.hpp"
+#include "ratio.cuh"
+
+namespace yq {
+
+template <typename R>
+struct SampArgs {
+    int n, m, n_chains, L, n_total, n_discard, resync, reinit, nup, nstride;
+    bool bias;
+    uint64_t seed;
+    uint32_t epoch;
+    const c128* p64;
+    const cplx<R>* W;
+    const cplx<R>* tau;
+    const c128* Lk;
+    int8_t* chains;
+    int8_t* out_sigma;
+    cplx<R>* out_theta;
+    unsigned long long* acc;
+};
+
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+template <typename R>
+__device__ __forceinline__ R warp_allsum(R v) {
+    // xor butterfly: every lane ends with the bitwise identical sum
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename R>
+struct LogGroup {
+    static constexpr int G = 8;
+};
+template <>
+struct LogGroup<float> {
+    static constexpr int G = 2;
+};
+
+template <typename R, int JPL>
+__device__ __forceinline__ void theta_fp64(const SampArgs<R>& A, const int8_t* s, int lane, cplx<R> (&th)[JPL]) {
+    const size_t nm = size_t(A.n) * A.m;
+#pragma unroll
+    for (int r = 0; r < JPL; ++r) {
+        const int j = lane + 32 * r;
+        if (j < A.m) {
+            double ar = 0., ai = 0.;
+            for (int i = 0; i < A.n; ++i) {
+                c128 w = A.p64[size_t(i) * A.m + j];
+                double sv = double(s[i]);
+                ar += w.re * sv;
+                ai += w.im * sv;
+            }
+            if (A.bias) {
+                c128 b = A.p64[nm + A.n + j];
+                ar += b.re;
+                ai += b.im;
+            }
+            th[r] = mk(R(ar), R(ai));
+        } else {
+            th[r] = mk(R(0), R(0));
+        }
+    }
+}
+
+template <typename R, int MOVE, int JPL>
+__global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
+    extern __shared__ int8_t smem_sig[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (c >= A.n_chains) return;  // warp-uniform
+    const int n = A.n, m = A.m;
+    int8_t* s = smem_sig + warp * A.nstride;
+    int8_t* cs = A.chains + size_t(c) * n;
+
+    // ---- chain initialisation (SamplerMT::randomize, Utilities/Utility.hpp:63-88)
+    if (A.reinit) {
+        if (A.nup < 0) {
+            for (int i = lane; i < n; i += 32) {
+                U4 x = draw(A.seed, uint32_t(i), A.epoch, uint32_t(c), TAG_INIT);
+                s[i] = (x.x & 1u) ? int8_t(-1) : int8_t(1);
+            }
+        } else {
+            if (lane == 0) {
+                for (int i = 0; i < n; ++i) s[i] = (i < A.nup) ? int8_t(-1) : int8_t(1);
+                for (int i = n - 1; i >= 1; --i) {
+                    U4 x = draw(A.seed, uint32_t(i), A.epoch, uint32_t(c), TAG_SHUF);
+                    int j = int(draw_site(x.x, uint32_t(i + 1)));
+                    int8_t tmp = s[i];
+                    s[i] = s[j];
+                    s[j] = tmp;
+                }
+            }
+        }
+    } else {
+        for (int i = lane; i < n; i += 32) s[i] = cs[i];
+    }
+    __syncwarp();
+
+    cplx<R> th[JPL], t[JPL];
+    theta_fp64<R, JPL>(A, s, lane, th);
+#pragma unroll
+    for (int r = 0; r < JPL; ++r) t[r] = ctanh(th[r]);
+
+    unsigned long long nacc = 0;
+    const uint32_t L = uint32_t(A.L);
+    const R two = R(2);
+    constexpr int G = LogGroup<R>::G;
+
+    // prefetch of the first proposal's columns
+    {
+        U4 x0 = draw(A.seed, 0u, A.epoch, uint32_t(c), TAG_SWEEP);
+        int k0 = int(draw_site(x0.x, uint32_t(n)));
+#pragma unroll
+        for (int r = 0; r < JPL; ++r) {
+            int j = lane + 32 * r;
+            if (j < m) {
+                prefetch_l1(A.tau + size_t(k0) * m + j);
+                prefetch_l1(A.W + size_t(k0) * m + j);
+            }
+        }
+    }
+
+    for (int sw = 0; sw < A.n_total; ++sw) {
+        for (uint32_t p = 0; p < L; ++p) {
+            const uint32_t g = uint32_t(sw) * L + p;
+            U4 x = draw(A.seed, g, A.epoch, uint32_t(c), TAG_SWEEP);
+            // prefetch the next proposal's columns into L1
+            {
+                U4 xn = draw(A.seed, g + 1u, A.epoch, uint32_t(c), TAG_SWEEP);
+                int kn = int(draw_site(xn.x, uint32_t(n)));
+                int ln = (MOVE == YQ_MOVE_EXCHANGE_ANY) ? int(draw_site(xn.y, uint32_t(n))) : (kn + 1) % n;
+#pragma unroll
+                for (int r = 0; r < JPL; ++r) {
+                    int j = lane + 32 * r;
+                    if (j < m) {
+                        prefetch_l1(A.tau + size_t(kn) * m + j);
+                        prefetch_l1(A.W + size_t(kn) * m + j);
+                        if (MOVE != YQ_MOVE_LOCAL) {
+                            prefetch_l1(A.tau + size_t(ln) * m + j);
+                            prefetch_l1(A.W + size_t(ln) * m + j);
+                        }
+                    }
+                }
+            }
+            const R u = draw_uniform<R>(x);
+            const int k = int(draw_site(x.x, uint32_t(n)));
+            if (MOVE == YQ_MOVE_LOCAL) {
+                const R sk = R(s[k]);
+                const cplx<R>* tk = A.tau + size_t(k) * m;
+                cplx<R> tv[JPL], d[JPL];
+#pragma unroll
+                for (int r = 0; r < JPL; ++r) {
+                    int j = lane + 32 * r;
+                    tv[r] = (j < m) ? tk[j] : mk(R(0), R(0));
+                    cplx<R> tt = t[r] * tv[r];
+                    d[r] = mk(R(1) - sk * tt.re, -sk * tt.im);
+                }
+                R ls = R(0);
+                cplx<R> pr = mk(R(1), R(0));
+#pragma unroll
+                for (int r = 0; r < JPL; ++r) {
+                    pr = pr * d[r];
+                    if ((r % G) == G - 1 || r == JPL - 1) {
+                        ls += log(norm2(pr));
+                        pr = mk(R(1), R(0));
+                    }
+                }
+                ls = warp_allsum(ls);
+                double base = A.Lk[k].re;
+                if (A.bias) base -= 2.0 * double(sk) * A.p64[size_t(n) * m + k].re;
+                const R logr = R(0.5) * ls + R(base);
+                // LocalSweeper.hpp:45-47: p = min(1, exp(beta * 2 * Re logRatio)); accept if u < p
+                if (u < exp(two * logr)) {
+                    const cplx<R>* wk = A.W + size_t(k) * m;
+#pragma unroll
+                    for (int r = 0; r < JPL; ++r) {
+                        int j = lane + 32 * r;
+                        if (j < m) {
+                            cplx<R> w = wk[j];
+                            th[r] = th[r] - (two * sk) * w;
+                            t[r] = cdiv(t[r] - sk * tv[r], d[r]);
+                        }
+                    }
+                    __syncwarp();
+                    if (lane == 0) s[k] = int8_t(-s[k]);
+                    __syncwarp();
+                    ++nacc;
+                }
+            } else {
+                const int l = (MOVE == YQ_MOVE_EXCHANGE_ANY) ? int(draw_site(x.y, uint32_t(n))) : (k + 1) % n;
+                const int8_t sk8 = s[k], sl8 = s[l];
+                if (sk8 == sl8) continue;  // SwapSweeper.hpp:43-46: the slot is consumed
+                const R sk = R(sk8), sl = R(sl8);
+                const cplx<R>* tk = A.tau + size_t(k) * m;
+                const cplx<R>* tl = A.tau + size_t(l) * m;
+                cplx<R> tx[JPL], ty[JPL], d[JPL];
+#pragma unroll
+                for (int r = 0; r < JPL; ++r) {
+                    int j = lane + 32 * r;
+                    cplx<R> a = (j < m) ? tk[j] : mk(R(0), R(0));
+                    cplx<R> b = (j < m) ? tl[j] : mk(R(0), R(0));
+                    tx[r] = sk * a;
+                    ty[r] = sl * b;
+                    d[r] = one<R>() + tx[r] * ty[r] - t[r] * (tx[r] + ty[r]);
+                }
+                R ls = R(0);
+                cplx<R> pr = mk(R(1), R(0));
+#pragma unroll
+                for (int r = 0; r < JPL; ++r) {
+                    pr = pr * d[r];
+                    if ((r % G) == G - 1 || r == JPL - 1) {
+                        ls += log(norm2(pr));
+                        pr = mk(R(1), R(0));
+                    }
+                }
+                ls = warp_allsum(ls);
+                double base = A.Lk[k].re + A.Lk[l].re;
+                if (A.bias)
+                    base -= 2.0 * double(sk) * A.p64[size_t(n) * m + k].re +
+                            2.0 * double(sl) * A.p64[size_t(n) * m + l].re;
+                const R logr = R(0.5) * ls + R(base);
+                if (u < exp(two * logr)) {
+                    const cplx<R>* wk = A.W + size_t(k) * m;
+                    const cplx<R>* wl = A.W + size_t(l) * m;
+#pragma unroll
+                    for (int r = 0; r < JPL; ++r) {
+                        int j = lane + 32 * r;
+                        if (j < m) {
+                            cplx<R> a = wk[j], b = wl[j];
+                            // States/RBMState.hpp:261-262: theta += -2 s_k W_k - 2 s_l W_l
+                            cplx<R> dd = mk(-(two * sk) * a.re - (two * sl) * b.re, -(two * sk) * a.im - (two * sl) * b.im);
+                            th[r] = th[r] + dd;
+                            cplx<R> sxy = tx[r] + ty[r];
+                            t[r] = cdiv(t[r] * (one<R>() + tx[r] * ty[r]) - sxy, d[r]);
+                        }
+                    }
+                    __syncwarp();
+                    if (lane == 0) {
+                        s[k] = int8_t(-sk8);
+                        s[l] = int8_t(-sl8);
+                    }
+                    __syncwarp();
+                    ++nacc;
+                }
+            }
+        }
+        // ---- end of sweep: record (SamplerMT.hpp:196-201), resync
+        if (sw >= A.n_discard) {
+            const size_t idx = size_t(sw - A.n_discard) * A.n_chains + c;
+            for (int i = lane; i < n; i += 32) A.out_sigma[idx * n + i] = s[i];
+#pragma unroll
+            for (int r = 0; r < JPL; ++r) {
+                int j = lane + 32 * r;
+                if (j < m) A.out_theta[idx * m + j] = th[r];
+            }
+        }
+        if (A.resync > 0 && ((sw + 1) % A.resync) == 0) theta_fp64<R, JPL>(A, s, lane, th);
+#pragma unroll
+        for (int r = 0; r < JPL; ++r) t[r] = ctanh(th[r]);
+    }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) cs[i] = s[i];
+    if (lane == 0) A.acc[c] = nacc;
+}
+
+template <typename R, int MOVE, int JPL>
+static void launch_t(const SampArgs<R>& A, cudaStream_t st) {
+    const int warps = 4;
+    dim3 grid(cdiv_u(A.n_chains, warps));
+    size_t smem = size_t(warps) * A.nstride;
+    metropolis_kernel<R, MOVE, JPL><<<grid, warps * 32, smem, st>>>(A);
+    YQ_LAUNCH_CHECK();
+}
+
+template <typename R, int MOVE>
+static void dispatch_jpl(const SampArgs<R>& A, cudaStream_t st) {
+    const int need = (A.m + 31) / 32;
+#define YQ_JPL(J)                        \
+    if (need <= J) {                     \
+        launch_t<R, MOVE, J>(A, st);     \
+        return;                          \
+    }
+    YQ_JPL(1) YQ_JPL(2) YQ_JPL(4) YQ_JPL(8) YQ_JPL(9) YQ_JPL(12) YQ_JPL(16) YQ_JPL(32)
+#undef YQ_JPL
+            throw Error(YQ_E_UNSUPPORTED, "sampler: m > 1024 hidden units is not built");
+}
+
+template <typename R>
+static void run_t(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, uint32_t epoch, int reinit) {
+    yq_rbm_s* q = S->q;
+    SampArgs<R> A;
+    A.n = q->n;
+    A.m = q->m;
+    A.n_chains = S->n_chains;
+    A.L = S->sweep_len > 0 ? S->sweep_len : q->n;
+    A.n_total = n_discard + n_sweeps;
+    A.n_discard = n_discard;
+    A.resync = S->resync;
+    A.reinit = reinit;
+    A.nup = S->nup;
+    A.nstride = (q->n + 15) & ~15;
+    A.bias = q->use_bias;
+    A.seed = seed;
+    A.epoch = epoch;
+    A.p64 = q->p64.as<c128>();
+    A.W = q->W.as<cplx<R>>();
+    A.tau = q->tau.as<cplx<R>>();
+    A.Lk = q->Lk.as<c128>();
+    A.chains = S->chains.as<int8_t>();
+    A.out_sigma = S->sigma.as<int8_t>();
+    A.out_theta = S->theta.as<cplx<R>>();
+    A.acc = S->acc.as<unsigned long long>();
+    cudaStream_t st = q->ctx->stream;
+    switch (S->move) {
+        case YQ_MOVE_LOCAL: dispatch_jpl<R, YQ_MOVE_LOCAL>(A, st); break;
+        case YQ_MOVE_EXCHANGE_ANY: dispatch_jpl<R, YQ_MOVE_EXCHANGE_ANY>(A, st); break;
+        default: dispatch_jpl<R, YQ_MOVE_EXCHANGE_NN>(A, st); break;
+    }
+}
+
+void sampler_run(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, uint32_t epoch, int reinit) {
+    yq_rbm_s* q = S->q;
+    YQ_CHECK_ARG(n_sweeps > 0 && n_discard >= 0, "sample: n_sweeps must be > 0 and n_discard >= 0");
+    YQ_CHECK_ARG(reinit || S->have_chains, "sample: reinit = 0 needs chains (set_chains or an earlier sample)");
+    const long long L = S->sweep_len > 0 ? S->sweep_len : q->n;
+    YQ_CHECK_ARG((long long)(n_sweeps + n_discard) * L < (1LL << 32) - 1, "sample: too many proposals per call");
+    rbm_prepare(q);
+    const size_t ns = size_t(S->n_chains) * n_sweeps;
+    S->sigma.ensure(ns * q->n);
+    S->theta.ensure(ns * q->m * q->csize());
+    if (q->dtype == YQ_C64)
+        run_t<float>(S, n_sweeps, n_discard, seed, epoch, reinit);
+    else
+        run_t<double>(S, n_sweeps, n_discard, seed, epoch, reinit);
+    S->have_chains = true;
+    S->ns = int(ns);
+    S->proposals = uint64_t(n_sweeps + n_discard) * uint64_t(L);
+}
+
+}  // namespace yq

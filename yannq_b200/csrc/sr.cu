@@ -1,0 +1,874 @@
+// Stochastic reconfiguration on the device (GroundState/SRMat.hpp):
+//   E_loc -> FP64 statistics -> structured column mean of O -> centred O writer
+//   -> F = O~^H (E - <E>) / Ns -> S = O~^H O~ / Ns (P x P) or its sample-space dual
+//   T = O~ O~^H / Ns (Ns x Ns) -> blocked FP64 Cholesky -> triangular solves ->
+//   v (= O~^H y in T-mode) -> SGD update of the FP64 master parameters.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "gram_tc.hpp"
+#include "internal.hpp"
+
+namespace yq {
+
+static constexpr int NB = 64;  // Cholesky block size
+
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void tanh_kernel(size_t count, const cplx<R>* __restrict__ th, cplx<R>* __restrict__ t) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += size_t(gridDim.x) * blockDim.x)
+        t[i] = ctanh(th[i]);
+}
+
+// Observables/Energy.hpp:53-58 with compensated (Kahan) FP64 sums:
+// stats = {E = <Re E_loc>, Var = <Re E_loc^2> - E^2, <E_loc>.re, <E_loc>.im}
+__global__ void energy_stats_kernel(int ns, const c128* __restrict__ e, double* __restrict__ stats,
+                                    int* __restrict__ status) {
+    __shared__ double sh[4][256];
+    double s[4] = {0, 0, 0, 0}, c[4] = {0, 0, 0, 0};
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+        double v[4] = {e[i].re, e[i].re * e[i].re, e[i].re, e[i].im};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            double y = v[q] - c[q];
+            double t = s[q] + y;
+            c[q] = (t - s[q]) - y;
+            s[q] = t;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) sh[q][threadIdx.x] = s[q];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot[4];
+        for (int q = 0; q < 4; ++q) {
+            double ss = 0., cc = 0.;
+            for (int k = 0; k < blockDim.x; ++k) {
+                double y = sh[q][k] - cc;
+                double t = ss + y;
+                cc = (t - ss) - y;
+                ss = t;
+            }
+            tot[q] = ss / ns;
+        }
+        stats[0] = tot[0];
+        stats[1] = tot[1] - tot[0] * tot[0];
+        stats[2] = tot[2];
+        stats[3] = tot[3];
+        if (!isfinite(tot[0]) || !isfinite(tot[3])) atomicOr(status, DS_NONFINITE);
+    }
+}
+
+// Column mean of O without forming O (the RBM's O row is [s_i t_j | s | t]):
+// partial sums over sample chunks of s_i t_j for i in [0, n] (i = n: s := 1, the
+// b block) and j in [0, m] (j = m: t := 1, the a block).
+template <typename R>
+__global__ void oloc_partial_kernel(int n, int m, int ns, int chunk, const int8_t* __restrict__ sigma,
+                                    const cplx<R>* __restrict__ t, c128* __restrict__ part) {
+    const int j = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int i = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int split = blockIdx.z;
+    if (i > n || j > m) return;
+    const int s0 = split * chunk, s1 = min(ns, s0 + chunk);
+    double ar = 0., ai = 0.;
+    for (int s = s0; s < s1; ++s) {
+        double sv = (i < n) ? double(sigma[size_t(s) * n + i]) : 1.0;
+        if (j < m) {
+            cplx<R> tv = t[size_t(s) * m + j];
+            ar += sv * double(tv.re);
+            ai += sv * double(tv.im);
+        } else {
+            ar += sv;
+        }
+    }
+    part[size_t(split) * (n + 1) * (m + 1) + size_t(i) * (m + 1) + j] = mk(ar, ai);
+}
+
+__global__ void oloc_reduce_kernel(int n, int m, bool bias, int nsplit, double inv_ns, const c128* __restrict__ part,
+                                   c128* __restrict__ oloc) {
+    const size_t cnt = size_t(n + 1) * (m + 1);
+    for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < cnt; q += size_t(gridDim.x) * blockDim.x) {
+        c128 acc = mk(0., 0.);
+        for (int sp = 0; sp < nsplit; ++sp) acc = acc + part[size_t(sp) * cnt + q];
+        acc = inv_ns * acc;
+        int i = int(q / (m + 1)), j = int(q % (m + 1));
+        const size_t nm = size_t(n) * m;
+        if (i < n && j < m)
+            oloc[size_t(i) * m + j] = acc;
+        else if (bias && i < n && j == m)
+            oloc[nm + i] = acc;
+        else if (bias && i == n && j < m)
+            oloc[nm + n + j] = acc;
+    }
+}
+
+// Centred log-derivative rows O~[s, p] = O[s, p] - oloc[p] (GroundState/utils.hpp:12-51 and
+// SRMat.hpp:99-100).  Row-major, P contiguous; two complex values per thread.
+template <typename R>
+__global__ void __launch_bounds__(256) o_writer_kernel(int n, int m, bool bias, size_t P, int ns,
+                                                       const int8_t* __restrict__ sigma,
+                                                       const cplx<R>* __restrict__ t, const c128* __restrict__ oloc,
+                                                       cplx<R>* __restrict__ O) {
+    const size_t nm = size_t(n) * m;
+    for (int s = blockIdx.y; s < ns; s += gridDim.y)
+    for (size_t p0 = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 2; p0 < P;
+         p0 += size_t(gridDim.x) * blockDim.x * 2) {
+        const int8_t* sg = sigma + size_t(s) * n;
+        const cplx<R>* ts = t + size_t(s) * m;
+        cplx<R>* row = O + size_t(s) * P;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            size_t p = p0 + e;
+            if (p >= P) break;
+            cplx<R> v;
+            if (p < nm) {
+                int i = int(p / m), j = int(p - size_t(i) * m);
+                R sv = R(sg[i]);
+                v = mk(sv * ts[j].re, sv * ts[j].im);
+            } else if (p < nm + n) {
+                v = mk(R(sg[p - nm]), R(0));
+            } else {
+                v = ts[p - nm - n];
+            }
+            c128 o = oloc[p];
+            row[p] = mk(v.re - R(o.re), v.im - R(o.im));
+        }
+    }
+}
+
+// out_p (partials) = sum_s conj(O~[s, p]) y_s over sample chunks.
+template <typename R>
+__global__ void ohy_partial_kernel(size_t P, int ns, int chunk, const cplx<R>* __restrict__ O,
+                                   const c128* __restrict__ yv, c128* __restrict__ part) {
+    const size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int split = blockIdx.y;
+    if (p >= P) return;
+    const int s0 = split * chunk, s1 = min(ns, s0 + chunk);
+    double ar = 0., ai = 0.;
+    for (int s = s0; s < s1; ++s) {
+        cplx<R> o = O[size_t(s) * P + p];
+        c128 y = yv[s];
+        // conj(o) * y
+        ar += double(o.re) * y.re + double(o.im) * y.im;
+        ai += double(o.re) * y.im - double(o.im) * y.re;
+    }
+    part[size_t(split) * P + p] = mk(ar, ai);
+}
+
+__global__ void reduce_parts_kernel(size_t P, int nsplit, double alpha, const c128* __restrict__ part,
+                                    const c128* __restrict__ addv, double beta, c128* __restrict__ out) {
+    for (size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += size_t(gridDim.x) * blockDim.x) {
+        c128 acc = mk(0., 0.);
+        for (int sp = 0; sp < nsplit; ++sp) acc = acc + part[size_t(sp) * P + p];
+        acc = alpha * acc;
+        if (addv) acc = acc + beta * addv[p];
+        out[p] = acc;
+    }
+}
+
+// out_s = alpha * sum_p O~[s, p] x_p  (one block per sample row)
+template <typename R>
+__global__ void ox_kernel(size_t P, int ns, const cplx<R>* __restrict__ O, const c128* __restrict__ x, double alpha,
+                          c128* __restrict__ out) {
+    __shared__ c128 red[8];
+    const int s = blockIdx.x;
+    const cplx<R>* row = O + size_t(s) * P;
+    double ar = 0., ai = 0.;
+    for (size_t p = threadIdx.x; p < P; p += blockDim.x) {
+        cplx<R> o = row[p];
+        c128 xv = x[p];
+        ar += double(o.re) * xv.re - double(o.im) * xv.im;
+        ai += double(o.re) * xv.im + double(o.im) * xv.re;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ar += __shfl_xor_sync(0xffffffffu, ar, o);
+        ai += __shfl_xor_sync(0xffffffffu, ai, o);
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mk(ar, ai);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        c128 r = red[0];
+        for (int w = 1; w < int(blockDim.x >> 5); ++w) r = r + red[w];
+        out[s] = alpha * r;
+    }
+}
+
+// y_s = (E_s - <E>) / Ns  (centred right-hand side of the T-mode solve)
+__global__ void centred_rhs_kernel(int ns, int ns_pad, const c128* __restrict__ e, const double* __restrict__ stats,
+                                   c128* __restrict__ y) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ns_pad) return;
+    if (s >= ns) {
+        y[s] = mk(0., 0.);
+        return;
+    }
+    y[s] = (1.0 / ns) * (e[s] - mk(stats[2], stats[3]));
+}
+
+// ---------------------------------------------------------------------------
+// FP64 complex Gram matrix, lower tiles only:  C(r, c) = alpha sum_k Z(r, k) conj(Z(c, k))
+// (+ C if accumulate) (+ shift on the diagonal).  Z(r, k) = Z[r ld + k] (kmode 0, rows
+// K-contiguous: T-mode and the Cholesky trailing update) or conj(Z[k ld + r])
+// (kmode 1: S = O~^H O~ from row-major O~).  64 x 64 tiles, 4 x 4 per thread.
+template <typename R, int KMODE>
+__global__ void __launch_bounds__(256) gram_fp64_kernel(const cplx<R>* __restrict__ Z, size_t ldz, int nrows, int K,
+                                                        c128* __restrict__ C, size_t ldc, double alpha,
+                                                        int accumulate, double shift) {
+    __shared__ c128 As[16][64 + 1];
+    __shared__ c128 Bs[16][64 + 1];
+    // lower-triangular tile index -> (bi, bj), bi >= bj
+    const long long tix = blockIdx.x;
+    long long bi = (long long)((sqrt(8.0 * double(tix) + 1.0) - 1.0) * 0.5);
+    while (bi * (bi + 1) / 2 > tix) --bi;
+    while ((bi + 1) * (bi + 2) / 2 <= tix) ++bi;
+    const long long bj = tix - bi * (bi + 1) / 2;
+    const int r0 = int(bi) * 64, c0 = int(bj) * 64;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    c128 acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = mk(0., 0.);
+
+    for (int k0 = 0; k0 < K; k0 += 16) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = tid + 256 * q;
+            int row, kk;
+            if (KMODE == 0) {
+                row = e >> 4;
+                kk = e & 15;
+            } else {
+                kk = e >> 6;
+                row = e & 63;
+            }
+            const int k = k0 + kk;
+            c128 va = mk(0., 0.), vb = mk(0., 0.);
+            if (k < K) {
+                const int ra = r0 + row, rb = c0 + row;
+                if (KMODE == 0) {
+                    if (ra < nrows) va = cast<double>(Z[size_t(ra) * ldz + k]);
+                    if (rb < nrows) vb = cast<double>(Z[size_t(rb) * ldz + k]);
+                } else {
+                    if (ra < nrows) va = conj(cast<double>(Z[size_t(k) * ldz + ra]));
+                    if (rb < nrows) vb = conj(cast<double>(Z[size_t(k) * ldz + rb]));
+                }
+            }
+            As[kk][row] = va;
+            Bs[kk][row] = vb;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int kk = 0; kk < 16; ++kk) {
+            c128 a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    // a * conj(b)
+                    acc[i][j].re += a[i].re * b[j].re + a[i].im * b[j].im;
+                    acc[i][j].im += a[i].im * b[j].re - a[i].re * b[j].im;
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = r0 + ty + 16 * i, c = c0 + tx + 16 * j;
+            if (r < nrows && c < nrows && r >= c) {
+                c128 v = alpha * acc[i][j];
+                c128* dst = C + size_t(r) * ldc + c;
+                if (accumulate) v = v + *dst;
+                if (r == c) v.re += shift;
+                *dst = v;
+            }
+        }
+}
+
+template <typename R>
+static void gram_fp64(const cplx<R>* Z, size_t ldz, int kmode, int nrows, int K, c128* C, size_t ldc, double alpha,
+                      int accumulate, double shift, cudaStream_t st) {
+    if (nrows <= 0) return;
+    const long long nt = (nrows + 63) / 64;
+    const long long tiles = nt * (nt + 1) / 2;
+    if (kmode == 0)
+        gram_fp64_kernel<R, 0><<<unsigned(tiles), 256, 0, st>>>(Z, ldz, nrows, K, C, ldc, alpha, accumulate, shift);
+    else
+        gram_fp64_kernel<R, 1><<<unsigned(tiles), 256, 0, st>>>(Z, ldz, nrows, K, C, ldc, alpha, accumulate, shift);
+    YQ_LAUNCH_CHECK();
+}
+
+// Padding of the SR matrix to a multiple of NB: zero off-diagonal, unit diagonal.
+__global__ void pad_identity_kernel(c128* G, int dim, int dim_pad) {
+    size_t total = size_t(dim_pad) * dim_pad;
+    for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < total; q += size_t(gridDim.x) * blockDim.x) {
+        int r = int(q / dim_pad), c = int(q % dim_pad);
+        if (r >= dim || c >= dim) G[q] = mk(r == c ? 1.0 : 0.0, 0.0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Blocked right-looking Cholesky (lower, row-major, in place), NB = 64.
+// Diagonal block: unblocked factorisation in shared memory + the inverse of
+// L_kk (stored in Linv for the panel TRSM and the triangular solves).
+__global__ void __launch_bounds__(256) potrf_diag_kernel(c128* __restrict__ G, size_t ld, int k0,
+                                                         c128* __restrict__ Linv, int* __restrict__ status) {
+    extern __shared__ c128 sm[];
+    c128* A = sm;             // [64][64]
+    c128* X = sm + NB * NB;   // [64][64] inverse
+    const int tid = threadIdx.x;
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+        int r = e / NB, c = e % NB;
+        A[e] = (c <= r) ? G[size_t(k0 + r) * ld + k0 + c] : mk(0., 0.);
+        X[e] = mk(0., 0.);
+    }
+    __syncthreads();
+    for (int c = 0; c < NB; ++c) {
+        if (tid == 0) {
+            double d = A[c * NB + c].re;
+            if (!(d > 0.0)) {
+                atomicOr(status, DS_NOT_PD);
+                d = 1.0;
+            }
+            A[c * NB + c] = mk(sqrt(d), 0.0);
+        }
+        __syncthreads();
+        const double inv = 1.0 / A[c * NB + c].re;
+        for (int r = c + 1 + tid; r < NB; r += blockDim.x) A[r * NB + c] = inv * A[r * NB + c];
+        __syncthreads();
+        const int w = NB - c - 1;
+        for (int e = tid; e < w * w; e += blockDim.x) {
+            int r = c + 1 + e / w, q = c + 1 + e % w;
+            if (q <= r) A[r * NB + q] = A[r * NB + q] - A[r * NB + c] * conj(A[q * NB + c]);
+        }
+        __syncthreads();
+    }
+    // X = L^{-1} by forward substitution, one column per thread
+    if (tid < NB) {
+        const int col = tid;
+        for (int r = col; r < NB; ++r) {
+            c128 acc = mk(r == col ? 1.0 : 0.0, 0.0);
+            for (int q = col; q < r; ++q) acc = acc - A[r * NB + q] * X[q * NB + col];
+            X[r * NB + col] = (1.0 / A[r * NB + r].re) * acc;
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+        int r = e / NB, c = e % NB;
+        if (c <= r) G[size_t(k0 + r) * ld + k0 + c] = A[e];
+        Linv[e] = X[e];
+    }
+}
+
+// Panel: L[r, k0:k0+64] = A[r, k0:k0+64] L_kk^{-H} for rows r >= k0 + 64.
+__global__ void __launch_bounds__(256) trsm_panel_kernel(c128* __restrict__ G, size_t ld, int k0, int dim_pad,
+                                                         const c128* __restrict__ Linv) {
+    extern __shared__ c128 sm[];
+    c128* X = sm;             // [64][64]
+    c128* Ar = sm + NB * NB;  // [32][64]
+    const int tid = threadIdx.x;
+    const int rbase = k0 + NB + blockIdx.x * 32;
+    for (int e = tid; e < NB * NB; e += blockDim.x) X[e] = Linv[e];
+    for (int e = tid; e < 32 * NB; e += blockDim.x) {
+        int rr = e / NB, c = e % NB;
+        int r = rbase + rr;
+        Ar[e] = (r < dim_pad) ? G[size_t(r) * ld + k0 + c] : mk(0., 0.);
+    }
+    __syncthreads();
+    // thread -> (row rr = tid / 8, columns c = (tid % 8) + 8 q)
+    const int rr = tid >> 3, cg = tid & 7;
+    const int r = rbase + rr;
+    if (r >= dim_pad) return;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int c = cg + 8 * q;
+        c128 acc = mk(0., 0.);
+        for (int qq = 0; qq <= c; ++qq) acc = acc + Ar[rr * NB + qq] * conj(X[c * NB + qq]);
+        G[size_t(r) * ld + k0 + c] = acc;
+    }
+}
+
+// Forward step kb of L x = y: x_kb = Linv_kb y_kb; y_r -= L[r, kb block] x_kb for r beyond the block.
+__global__ void __launch_bounds__(256) trsv_fwd_kernel(const c128* __restrict__ G, size_t ld, int k0, int dim_pad,
+                                                       const c128* __restrict__ Linv, c128* __restrict__ y,
+                                                       c128* __restrict__ x) {
+    __shared__ c128 yb[NB], xb[NB];
+    const int tid = threadIdx.x;
+    if (tid < NB) yb[tid] = y[k0 + tid];
+    __syncthreads();
+    if (tid < NB) {
+        c128 acc = mk(0., 0.);
+        for (int q = 0; q <= tid; ++q) acc = acc + Linv[tid * NB + q] * yb[q];
+        xb[tid] = acc;
+        if (blockIdx.x == 0) x[k0 + tid] = acc;
+    }
+    __syncthreads();
+    const int r = k0 + NB + blockIdx.x * blockDim.x + tid;
+    if (r < dim_pad) {
+        c128 acc = mk(0., 0.);
+        const c128* row = G + size_t(r) * ld + k0;
+        for (int q = 0; q < NB; ++q) acc = acc + row[q] * xb[q];
+        y[r] = y[r] - acc;
+    }
+}
+
+// Backward step kb of L^H z = x: z_kb = Linv_kb^H x_kb; x_r -= sum_q conj(L[k0+q, r]) z_kb[q] for r < k0.
+__global__ void __launch_bounds__(256) trsv_bwd_kernel(const c128* __restrict__ G, size_t ld, int k0,
+                                                       const c128* __restrict__ Linv, c128* __restrict__ xv,
+                                                       c128* __restrict__ z) {
+    __shared__ c128 xb[NB], zb[NB];
+    const int tid = threadIdx.x;
+    if (tid < NB) xb[tid] = xv[k0 + tid];
+    __syncthreads();
+    if (tid < NB) {
+        c128 acc = mk(0., 0.);
+        for (int q = tid; q < NB; ++q) acc = acc + conj(Linv[q * NB + tid]) * xb[q];
+        zb[tid] = acc;
+        if (blockIdx.x == 0) z[k0 + tid] = acc;
+    }
+    __syncthreads();
+    const int r = blockIdx.x * blockDim.x + tid;
+    if (r < k0) {
+        c128 acc = mk(0., 0.);
+        for (int q = 0; q < NB; ++q) acc = acc + conj(G[size_t(k0 + q) * ld + r]) * zb[q];
+        xv[r] = xv[r] - acc;
+    }
+}
+
+static void cholesky(yq_sr_s* sr) {
+    cudaStream_t st = sr->q->ctx->stream;
+    int* status = sr->q->ctx->status.as<int>();
+    const int n = sr->dim_pad;
+    const size_t ld = size_t(n);
+    c128* G = sr->G.as<c128>();
+    const int nb = n / NB;
+    static bool attr = false;
+    if (!attr) {
+        YQ_CUDA(cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(2 * NB * NB * sizeof(c128))));
+        YQ_CUDA(cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int((NB * NB + 32 * NB) * sizeof(c128))));
+        attr = true;
+    }
+    for (int kb = 0; kb < nb; ++kb) {
+        const int k0 = kb * NB;
+        c128* Li = sr->Linv.as<c128>() + size_t(kb) * NB * NB;
+        potrf_diag_kernel<<<1, 256, 2 * NB * NB * sizeof(c128), st>>>(G, ld, k0, Li, status);
+        YQ_LAUNCH_CHECK();
+        const int rest = n - k0 - NB;
+        if (rest <= 0) break;
+        trsm_panel_kernel<<<cdiv_u(rest, 32), 256, (NB * NB + 32 * NB) * sizeof(c128), st>>>(G, ld, k0, n, Li);
+        YQ_LAUNCH_CHECK();
+        gram_fp64<double>(G + size_t(k0 + NB) * ld + k0, ld, 0, rest, NB, G + size_t(k0 + NB) * ld + k0 + NB, ld,
+                          -1.0, 1, 0.0, st);
+    }
+}
+
+// b (dim_pad) -> (L L^H)^{-1} b, using work as scratch; result in out.
+static void chol_solve(yq_sr_s* sr, c128* b, c128* work, c128* out) {
+    cudaStream_t st = sr->q->ctx->stream;
+    const int n = sr->dim_pad;
+    const size_t ld = size_t(n);
+    const c128* G = sr->G.as<c128>();
+    const int nb = n / NB;
+    for (int kb = 0; kb < nb; ++kb) {
+        const int k0 = kb * NB;
+        const int rest = n - k0 - NB;
+        trsv_fwd_kernel<<<std::max(1u, cdiv_u(std::max(rest, 0), 256)), 256, 0, st>>>(
+            G, ld, k0, n, sr->Linv.as<c128>() + size_t(kb) * NB * NB, b, work);
+        YQ_LAUNCH_CHECK();
+    }
+    for (int kb = nb - 1; kb >= 0; --kb) {
+        const int k0 = kb * NB;
+        trsv_bwd_kernel<<<std::max(1u, cdiv_u(k0, 256)), 256, 0, st>>>(G, ld, k0,
+                                                                      sr->Linv.as<c128>() + size_t(kb) * NB * NB,
+                                                                      work, out);
+        YQ_LAUNCH_CHECK();
+    }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void update_kernel(size_t P, double lr, const c128* __restrict__ v, c128* __restrict__ p64,
+                              double* __restrict__ part) {
+    __shared__ double red[8];
+    double acc = 0.;
+    for (size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += size_t(gridDim.x) * blockDim.x) {
+        c128 vv = v[p];
+        acc += vv.re * vv.re + vv.im * vv.im;
+        p64[p] = p64[p] - lr * vv;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) r += red[w];
+        part[blockIdx.x] = r;
+    }
+}
+
+__global__ void finish_norm_kernel(int nb, const double* __restrict__ part, double* __restrict__ stats,
+                                   int* __restrict__ status) {
+    double r = 0.;
+    for (int i = 0; i < nb; ++i) r += part[i];
+    stats[4] = sqrt(r);
+    if (!isfinite(r)) atomicOr(status, DS_NONFINITE);
+}
+
+// ---------------------------------------------------------------------------
+template <typename R>
+static void construct_t(yq_sr_s* sr) {
+    yq_rbm_s* q = sr->q;
+    yq_ctx_s* ctx = q->ctx;
+    cudaStream_t st = ctx->stream;
+    const int ns = sr->ns, n = q->n, m = q->m;
+    const size_t P = q->P;
+    const cplx<R>* theta = sr->S->theta.as<cplx<R>>();
+    const int8_t* sigma = sr->S->sigma.as<int8_t>();
+
+    ctx->stage_begin(ST_ELOC);
+    ham_eloc(sr->H, q, ns, sigma, theta, sr->eloc.as<c128>());
+    energy_stats_kernel<<<1, 256, 0, st>>>(ns, sr->eloc.as<c128>(), sr->stats.as<double>(), ctx->status.as<int>());
+    YQ_LAUNCH_CHECK();
+    ctx->stage_end(ST_ELOC);
+
+    ctx->stage_begin(ST_MEAN);
+    const size_t cnt = size_t(ns) * m;
+    tanh_kernel<R><<<std::min<size_t>(cdiv_u(cnt, 256), 148 * 16), 256, 0, st>>>(cnt, theta, sr->tanhs.as<cplx<R>>());
+    YQ_LAUNCH_CHECK();
+    // column mean of O, split over sample chunks (deterministic two-stage sum)
+    {
+        dim3 g(cdiv_u(m + 1, 32), cdiv_u(n + 1, 8), 1);
+        int nsplit = std::max(1, std::min(64, int((4 * 148) / std::max(1u, g.x * g.y))));
+        nsplit = std::min(nsplit, ns);
+        int chunk = (ns + nsplit - 1) / nsplit;
+        g.z = nsplit;
+        sr->part.ensure(std::max(size_t(nsplit) * (n + 1) * (m + 1), size_t(16) * P) * sizeof(c128));
+        oloc_partial_kernel<R><<<g, 256, 0, st>>>(n, m, ns, chunk, sigma, sr->tanhs.as<cplx<R>>(), sr->part.as<c128>());
+        YQ_LAUNCH_CHECK();
+        oloc_reduce_kernel<<<cdiv_u(size_t(n + 1) * (m + 1), 256), 256, 0, st>>>(
+            n, m, q->use_bias, nsplit, 1.0 / ns, sr->part.as<c128>(), sr->oloc.as<c128>());
+        YQ_LAUNCH_CHECK();
+    }
+    ctx->stage_end(ST_MEAN);
+
+    ctx->stage_begin(ST_O);
+    {
+        dim3 g(std::max(1u, std::min(64u, cdiv_u(P, 512))), unsigned(std::min(ns, 65535)));
+        o_writer_kernel<R><<<g, 256, 0, st>>>(n, m, q->use_bias, P, ns, sigma, sr->tanhs.as<cplx<R>>(),
+                                              sr->oloc.as<c128>(), sr->O.as<cplx<R>>());
+        YQ_LAUNCH_CHECK();
+    }
+    if (sr->precision == YQ_PREC_MIXED && sr->mode == YQ_SR_T)
+        gram_tc_prepare_operands(sr->O.as<c64>(), ns, P, sr->xh.as<uint16_t>(), sr->xl.as<uint16_t>(),
+                                 sr->yh.as<uint16_t>(), sr->yl.as<uint16_t>(), st);
+    ctx->stage_end(ST_O);
+
+    // F = O~^H (E - <E>) / Ns (SRMat.hpp:101-102; equal to O~^H E / Ns since O~^H 1 = 0)
+    const int vlen = std::max(ns, sr->dim_pad);
+    centred_rhs_kernel<<<cdiv_u(vlen, 256), 256, 0, st>>>(ns, vlen, sr->eloc.as<c128>(), sr->stats.as<double>(),
+                                                          sr->y.as<c128>());
+    YQ_LAUNCH_CHECK();
+    {
+        const int nsplit = std::max(1, std::min(16, int(4 * 148 / std::max(1u, cdiv_u(P, 256)))));
+        const int chunk = (ns + nsplit - 1) / nsplit;
+        dim3 g(cdiv_u(P, 256), nsplit);
+        ohy_partial_kernel<R><<<g, 256, 0, st>>>(P, ns, chunk, sr->O.as<cplx<R>>(), sr->y.as<c128>(),
+                                                 sr->part.as<c128>());
+        YQ_LAUNCH_CHECK();
+        reduce_parts_kernel<<<cdiv_u(P, 256), 256, 0, st>>>(P, nsplit, 1.0, sr->part.as<c128>(), nullptr, 0.0,
+                                                            sr->grad.as<c128>());
+        YQ_LAUNCH_CHECK();
+    }
+}
+
+void sr_construct(yq_sr_s* sr) {
+    yq_rbm_s* q = sr->q;
+    yq_sampler_s* S = sr->S;
+    YQ_CHECK_ARG(S->ns > 0, "construct: the sampler holds no samples");
+    if (sr->precision == YQ_PREC_MIXED)
+        YQ_CHECK_ARG(q->dtype == YQ_C64, "construct: mixed precision needs a complex64 RBM");
+    else
+        YQ_CHECK_ARG(q->dtype == YQ_C128, "construct: FP64 precision needs a complex128 RBM");
+    rbm_prepare(q);
+    const int ns = S->ns;
+    const size_t P = q->P;
+    sr->ns = ns;
+    sr->mode = sr->mode_req == YQ_SR_AUTO ? (size_t(ns) < P ? YQ_SR_T : YQ_SR_S) : sr->mode_req;
+    if (sr->precision == YQ_PREC_MIXED) sr->mode = YQ_SR_T;  // tensor-core path is built for the dual form
+    sr->dim = sr->mode == YQ_SR_T ? ns : int(P);
+    sr->dim_pad = ((sr->dim + NB - 1) / NB) * NB;
+    const size_t cs = q->csize();
+    sr->eloc.ensure(size_t(ns) * sizeof(c128));
+    sr->tanhs.ensure(size_t(ns) * q->m * cs);
+    sr->O.ensure(size_t(ns) * P * cs);
+    sr->oloc.ensure(P * sizeof(c128));
+    sr->grad.ensure(P * sizeof(c128));
+    sr->v.ensure(P * sizeof(c128));
+    sr->work_p.ensure(P * sizeof(c128));
+    const size_t vec = size_t(std::max(ns, sr->dim_pad));
+    sr->y.ensure(vec * sizeof(c128));
+    sr->rhs.ensure(vec * sizeof(c128));
+    sr->work_s.ensure(vec * sizeof(c128));
+    sr->s1.ensure(vec * sizeof(c128));
+    sr->s2.ensure(vec * sizeof(c128));
+    sr->s3.ensure(vec * sizeof(c128));
+    sr->s4.ensure(vec * sizeof(c128));
+    sr->stats.ensure(64 * sizeof(double));
+    if (sr->precision == YQ_PREC_MIXED) {
+        const size_t kpad = gram_tc_kpad(P);
+        const size_t rows = gram_tc_rows(ns);
+        sr->xh.ensure(rows * kpad * 2);
+        sr->xl.ensure(rows * kpad * 2);
+        sr->yh.ensure(rows * kpad * 2);
+        sr->yl.ensure(rows * kpad * 2);
+    }
+    if (q->dtype == YQ_C64)
+        construct_t<float>(sr);
+    else
+        construct_t<double>(sr);
+    sr->constructed = true;
+    sr->solved = false;
+}
+
+// Form the shifted SR matrix (S or T) into G (lower, padded).
+template <typename R>
+static void form_matrix_t(yq_sr_s* sr, double shift) {
+    cudaStream_t st = sr->q->ctx->stream;
+    const size_t P = sr->q->P;
+    const int ns = sr->ns;
+    sr->G.ensure(size_t(sr->dim_pad) * sr->dim_pad * sizeof(c128));
+    sr->Linv.ensure(size_t(sr->dim_pad / NB) * NB * NB * sizeof(c128));
+    c128* G = sr->G.as<c128>();
+    if (sr->dim_pad != sr->dim) {
+        pad_identity_kernel<<<148 * 8, 256, 0, st>>>(G, sr->dim, sr->dim_pad);
+        YQ_LAUNCH_CHECK();
+    }
+    if (sr->mode == YQ_SR_T) {
+        if (sr->precision == YQ_PREC_MIXED)
+            gram_tc_run(sr->xh.as<uint16_t>(), sr->xl.as<uint16_t>(), sr->yh.as<uint16_t>(), sr->yl.as<uint16_t>(),
+                        ns, P, G, size_t(sr->dim_pad), 1.0 / ns, shift, sr->q->ctx->status.as<int>(), st);
+        else
+            gram_fp64<R>(sr->O.as<cplx<R>>(), P, 0, ns, int(P), G, size_t(sr->dim_pad), 1.0 / ns, 0, shift, st);
+    } else {
+        gram_fp64<R>(sr->O.as<cplx<R>>(), P, 1, int(P), ns, G, size_t(sr->dim_pad), 1.0 / ns, 0, shift, st);
+    }
+}
+
+static void form_matrix(yq_sr_s* sr, double shift) {
+    if (sr->q->dtype == YQ_C64)
+        form_matrix_t<float>(sr, shift);
+    else
+        form_matrix_t<double>(sr, shift);
+}
+
+// y <- O~^H x * alpha  (P-vector out), x: ns-vector
+template <typename R>
+static void op_ohy(yq_sr_s* sr, const c128* x, double alpha, c128* out, const c128* addv, double beta) {
+    cudaStream_t st = sr->q->ctx->stream;
+    const size_t P = sr->q->P;
+    const int ns = sr->ns;
+    const int nsplit = std::max(1, std::min(16, int(4 * 148 / std::max(1u, cdiv_u(P, 256)))));
+    const int chunk = (ns + nsplit - 1) / nsplit;
+    dim3 g(cdiv_u(P, 256), nsplit);
+    ohy_partial_kernel<R><<<g, 256, 0, st>>>(P, ns, chunk, sr->O.as<cplx<R>>(), x, sr->part.as<c128>());
+    YQ_LAUNCH_CHECK();
+    reduce_parts_kernel<<<cdiv_u(P, 256), 256, 0, st>>>(P, nsplit, alpha, sr->part.as<c128>(), addv, beta, out);
+    YQ_LAUNCH_CHECK();
+}
+template <typename R>
+static void op_ox(yq_sr_s* sr, const c128* x, double alpha, c128* out) {
+    ox_kernel<R><<<sr->ns, 256, 0, sr->q->ctx->stream>>>(sr->q->P, sr->ns, sr->O.as<cplx<R>>(), x, alpha, out);
+    YQ_LAUNCH_CHECK();
+}
+
+// apply(x) = O~^H (O~ x) / Ns + shift x  (SRMat.hpp:170-189)
+template <typename R>
+static void sr_apply(yq_sr_s* sr, const c128* x, double shift, c128* out) {
+    op_ox<R>(sr, x, 1.0 / sr->ns, sr->work_s.as<c128>());
+    op_ohy<R>(sr, sr->work_s.as<c128>(), 1.0, out, x, shift);
+}
+
+// ---------------------------------------------------------------------------
+// Device-side vector helpers for CG (host-driven loop, FP64).
+__global__ void dotc_kernel(size_t n, const c128* __restrict__ a, const c128* __restrict__ b, double* __restrict__ out) {
+    __shared__ c128 red[8];
+    c128 acc = mk(0., 0.);
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        acc = acc + conj(a[i]) * b[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
+        acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        c128 r = red[0];
+        for (int w = 1; w < int(blockDim.x >> 5); ++w) r = r + red[w];
+        out[2 * blockIdx.x] = r.re;
+        out[2 * blockIdx.x + 1] = r.im;
+    }
+}
+__global__ void axpy_kernel(size_t n, c128 alpha, const c128* __restrict__ x, c128* __restrict__ y) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        y[i] = y[i] + alpha * x[i];
+}
+__global__ void xpby_kernel(size_t n, const c128* __restrict__ x, double beta, c128* __restrict__ y) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        y[i] = x[i] + beta * y[i];
+}
+
+static c128 dotc(yq_sr_s* sr, size_t n, const c128* a, const c128* b) {
+    cudaStream_t st = sr->q->ctx->stream;
+    const int blocks = 128;
+    double* buf = sr->q->ctx->scratch.as<double>();
+    dotc_kernel<<<blocks, 256, 0, st>>>(n, a, b, buf);
+    YQ_LAUNCH_CHECK();
+    double h[2 * blocks];
+    YQ_CUDA(cudaMemcpyAsync(h, buf, sizeof(h), cudaMemcpyDeviceToHost, st));
+    YQ_CUDA(cudaStreamSynchronize(st));
+    c128 r = mk(0., 0.);
+    for (int i = 0; i < blocks; ++i) r = r + mk(h[2 * i], h[2 * i + 1]);
+    return r;
+}
+
+// Eigen::ConjugateGradient<..., Lower|Upper, IdentityPreconditioner> semantics.
+template <typename R>
+static void solve_cg_t(yq_sr_s* sr, double shift, double tol, int* iters, double* relres) {
+    cudaStream_t st = sr->q->ctx->stream;
+    const size_t P = sr->q->P;
+    DevBuf rb, pb, tb;
+    rb.ensure(P * sizeof(c128));
+    pb.ensure(P * sizeof(c128));
+    tb.ensure(P * sizeof(c128));
+    c128 *x = sr->v.as<c128>(), *r = rb.as<c128>(), *p = pb.as<c128>(), *tmp = tb.as<c128>();
+    YQ_CUDA(cudaMemsetAsync(x, 0, P * sizeof(c128), st));
+    YQ_CUDA(cudaMemcpyAsync(r, sr->grad.as<c128>(), P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+    const unsigned g = std::min(148u * 8, cdiv_u(P, 256));
+    double rhsNorm2 = dotc(sr, P, r, r).re;
+    int it = 0;
+    double res2 = rhsNorm2;
+    if (rhsNorm2 > 0.) {
+        const double threshold = tol * tol * rhsNorm2;
+        YQ_CUDA(cudaMemcpyAsync(p, r, P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+        double absNew = dotc(sr, P, r, p).re;
+        const int maxit = int(2 * P);
+        while (it < maxit) {
+            sr_apply<R>(sr, p, shift, tmp);
+            c128 pt = dotc(sr, P, p, tmp);
+            c128 alpha = cdiv(mk(absNew, 0.0), pt);
+            axpy_kernel<<<g, 256, 0, st>>>(P, alpha, p, x);
+            axpy_kernel<<<g, 256, 0, st>>>(P, mk(-alpha.re, -alpha.im), tmp, r);
+            YQ_LAUNCH_CHECK();
+            res2 = dotc(sr, P, r, r).re;
+            if (res2 < threshold) break;
+            double absOld = absNew;
+            absNew = res2;
+            xpby_kernel<<<g, 256, 0, st>>>(P, r, absNew / absOld, p);
+            YQ_LAUNCH_CHECK();
+            ++it;
+        }
+    }
+    if (iters) *iters = it;
+    if (relres) *relres = rhsNorm2 > 0. ? std::sqrt(res2 / rhsNorm2) : 0.;
+}
+
+__global__ void residual_kernel(size_t n, const c128* __restrict__ b, const c128* __restrict__ ax, c128* __restrict__ r) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        r[i] = b[i] - ax[i];
+}
+
+template <typename R>
+static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps) {
+    yq_ctx_s* ctx = sr->q->ctx;
+    cudaStream_t st = ctx->stream;
+    const size_t P = sr->q->P;
+    const int ns = sr->ns;
+    ctx->stage_begin(ST_GRAM);
+    form_matrix_t<R>(sr, shift);
+    ctx->stage_end(ST_GRAM);
+    ctx->stage_begin(ST_SOLVE);
+    cholesky(sr);
+    const size_t dp = size_t(sr->dim_pad);
+    if (sr->mode == YQ_SR_T) {
+        // y = (T + shift)^{-1} (E - <E>) / Ns ; v = O~^H y   (push-through identity)
+        c128* b = sr->rhs.as<c128>();
+        YQ_CUDA(cudaMemcpyAsync(b, sr->y.as<c128>(), dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+        c128* sol = sr->s1.as<c128>();
+        c128* tmp = sr->s2.as<c128>();
+        chol_solve(sr, b, tmp, sol);
+        // iterative refinement against the exact operator (T y = O~ (O~^H y) / Ns + shift y, FP64 sums)
+        for (int k = 0; k < ir_steps; ++k) {
+            c128* ty = sr->s3.as<c128>();
+            c128* r = sr->rhs.as<c128>();
+            c128* dy = sr->s4.as<c128>();
+            YQ_CUDA(cudaMemsetAsync(ty, 0, dp * sizeof(c128), st));
+            op_ohy<R>(sr, sol, 1.0, sr->work_p.as<c128>(), nullptr, 0.0);
+            op_ox<R>(sr, sr->work_p.as<c128>(), 1.0 / ns, ty);
+            axpy_kernel<<<cdiv_u(ns, 256), 256, 0, st>>>(size_t(ns), mk(shift, 0.0), sol, ty);
+            residual_kernel<<<cdiv_u(dp, 256), 256, 0, st>>>(dp, sr->y.as<c128>(), ty, r);
+            YQ_LAUNCH_CHECK();
+            chol_solve(sr, r, tmp, dy);
+            axpy_kernel<<<cdiv_u(dp, 256), 256, 0, st>>>(dp, mk(1.0, 0.0), dy, sol);
+            YQ_LAUNCH_CHECK();
+        }
+        op_ohy<R>(sr, sol, 1.0, sr->v.as<c128>(), nullptr, 0.0);
+    } else {
+        c128* b = sr->rhs.as<c128>();
+        YQ_CUDA(cudaMemsetAsync(b, 0, dp * sizeof(c128), st));
+        YQ_CUDA(cudaMemcpyAsync(b, sr->grad.as<c128>(), P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+        chol_solve(sr, b, sr->s2.as<c128>(), sr->s1.as<c128>());
+        YQ_CUDA(cudaMemcpyAsync(sr->v.as<c128>(), sr->s1.p, P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+    }
+    ctx->stage_end(ST_SOLVE);
+}
+
+void sr_solve(yq_sr_s* sr, double shift, int solver, double cg_tol, int ir_steps, int* iters, double* relres) {
+    if (!sr->constructed) throw Error(YQ_E_STATE, "solve: call construct first");
+    YQ_CHECK_ARG(shift >= 0.0, "solve: shift must be >= 0");
+    if (solver == YQ_SOLVE_CG) {
+        sr->q->ctx->stage_begin(ST_SOLVE);
+        if (sr->q->dtype == YQ_C64)
+            solve_cg_t<float>(sr, shift, cg_tol, iters, relres);
+        else
+            solve_cg_t<double>(sr, shift, cg_tol, iters, relres);
+        sr->q->ctx->stage_end(ST_SOLVE);
+    } else {
+        if (sr->q->dtype == YQ_C64)
+            solve_llt_t<float>(sr, shift, ir_steps);
+        else
+            solve_llt_t<double>(sr, shift, ir_steps);
+        if (iters) *iters = 0;
+        if (relres) *relres = 0.;
+    }
+    sr->solved = true;
+}
+
+void sr_form_matrix_public(yq_sr_s* sr, double shift) { form_matrix(sr, shift); }
+
+void sr_update_params(yq_sr_s* sr, double lr) {
+    if (!sr->solved) throw Error(YQ_E_STATE, "update: call solve first");
+    yq_ctx_s* ctx = sr->q->ctx;
+    cudaStream_t st = ctx->stream;
+    ctx->stage_begin(ST_UPDATE);
+    const int blocks = 148;
+    update_kernel<<<blocks, 256, 0, st>>>(sr->q->P, lr, sr->v.as<c128>(), sr->q->p64.as<c128>(),
+                                          ctx->scratch.as<double>());
+    finish_norm_kernel<<<1, 1, 0, st>>>(blocks, ctx->scratch.as<double>(), sr->stats.as<double>(),
+                                        ctx->status.as<int>());
+    YQ_LAUNCH_CHECK();
+    sr->q->version++;
+    ctx->stage_end(ST_UPDATE);
+}
+
+}  // namespace yq
