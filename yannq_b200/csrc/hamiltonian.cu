@@ -86,6 +86,7 @@ struct ElocArgs {
     const int8_t* sigma;
     const cplx<R>* theta;
     const cplx<R>* tauT;
+    const cplx<R>* W;
     const c128* Lk;
     const c128* a;  // visible bias (FP64) or null
     c128* out;
@@ -96,13 +97,18 @@ template <typename R>
 __global__ void __launch_bounds__(256) eloc_kernel(ElocArgs<R> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R>* t = reinterpret_cast<cplx<R>*>(smem_raw);
-    int8_t* s = reinterpret_cast<int8_t*>(smem_raw + sizeof(cplx<R>) * A.m);
+    cplx<R>* th = t + A.m;
+    int8_t* s = reinterpret_cast<int8_t*>(smem_raw + 2 * sizeof(cplx<R>) * A.m);
     __shared__ c128 red[8];
     const int n = A.H.n, m = A.m;
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int smp = blockIdx.x; smp < A.ns; smp += gridDim.x) {
         for (int i = tid; i < n; i += nt) s[i] = A.sigma[size_t(smp) * n + i];
-        for (int j = tid; j < m; j += nt) t[j] = ctanh(A.theta[size_t(smp) * m + j]);
+        for (int j = tid; j < m; j += nt) {
+            cplx<R> v = A.theta[size_t(smp) * m + j];
+            th[j] = v;
+            t[j] = ctanh(v);
+        }
         __syncthreads();
         c128 acc = mk(0., 0.);
         for (int i = tid; i < n; i += nt) {
@@ -113,10 +119,10 @@ __global__ void __launch_bounds__(256) eloc_kernel(ElocArgs<R> A) {
             if (c == 0.0) continue;  // zero coefficient: the reference multiplies the ratio by 0
             c128 val;
             if (kb < 0) {
-                ScaledProd<R> P = prod1<R>(ka, R(s[ka]), n, m, t, 1, A.tauT);
+                ScaledProd<R> P = prod1<R>(ka, R(s[ka]), n, m, t, th, 1, A.tauT, A.W);
                 val = value_scaled(base1(A.Lk, A.a, ka, double(s[ka])), P);
             } else {
-                ScaledProd<R> P = prod2<R>(ka, R(s[ka]), kb, R(s[kb]), n, m, t, 1, A.tauT);
+                ScaledProd<R> P = prod2<R>(ka, R(s[ka]), kb, R(s[kb]), n, m, t, th, 1, A.tauT, A.W);
                 val = value_scaled(base1(A.Lk, A.a, ka, double(s[ka])) + base1(A.Lk, A.a, kb, double(s[kb])), P);
             }
             acc = acc + c * val;
@@ -148,6 +154,7 @@ static void eloc_t(yq_ham_s* H, yq_rbm_s* q, int ns, const int8_t* d_sigma, cons
     A.sigma = d_sigma;
     A.theta = reinterpret_cast<const cplx<R>*>(d_theta);
     A.tauT = q->tauT.as<cplx<R>>();
+    A.W = q->W.as<cplx<R>>();
     A.Lk = q->Lk.as<c128>();
     A.a = q->use_bias ? q->p64.as<c128>() + size_t(q->n) * q->m : nullptr;
     A.out = d_out;
@@ -155,7 +162,7 @@ static void eloc_t(yq_ham_s* H, yq_rbm_s* q, int ns, const int8_t* d_sigma, cons
     int threads = ((H->n + 31) / 32) * 32;
     if (threads > 256) threads = 256;
     if (threads < 64) threads = 64;
-    size_t smem = sizeof(cplx<R>) * q->m + A.nstride;
+    size_t smem = 2 * sizeof(cplx<R>) * q->m + A.nstride;
     if (smem > 48 * 1024)
         YQ_CUDA(cudaFuncSetAttribute(eloc_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int blocks = ns < 148 * 16 ? ns : 148 * 16;

@@ -46,15 +46,72 @@ struct RenormChunk<float> {
     static constexpr int mask = 3;
 };
 
-// prod_j (1 - s_k t_j tau_jk) with tau given transposed (tauT[j * n + k]), t with stride ts.
+// Cancellation guard.  1 - s t tau loses relative accuracy when |t tau| ~ 1 and
+// the difference is small (both tanh near +-1): the relative error grows as
+// |t tau| / |d|.  Below |d| < |t tau| / 256 the factor is re-evaluated in the
+// reference's well-conditioned logcosh form,
+//   d = cosh(theta - x) / (cosh(theta) cosh(x)),   x = 2 s W,
+// and for two flips d = cosh(theta - x - y) / (cosh(theta) cosh(x) cosh(y)).
+// Threshold on |d|^2 / |t tau|^2: relative error amplification <= 256 in FP64
+// (~6e-14), <= 16 in FP32 (~1e-6).
 template <typename R>
-__device__ __forceinline__ ScaledProd<R> prod1(int k, R sk, int n, int m, const cplx<R>* t, int ts,
-                                              const cplx<R>* tauT) {
+struct Cancel {
+    static constexpr double thr2 = 1.0 / 65536.0;
+};
+template <>
+struct Cancel<float> {
+    static constexpr double thr2 = 1.0 / 256.0;
+};
+
+template <typename R>
+__device__ __noinline__ cplx<R> exact_factor1(cplx<R> th, R sk, cplx<R> w) {
+    c128 t = cast<double>(th);
+    c128 x = (2.0 * double(sk)) * cast<double>(w);
+    c128 l = clogcosh(t - x) - clogcosh(t) - clogcosh(x);
+    return cast<R>(cexp(l));
+}
+template <typename R>
+__device__ __noinline__ cplx<R> exact_factor2(cplx<R> th, R sk, cplx<R> wk, R sl, cplx<R> wl) {
+    c128 t = cast<double>(th);
+    c128 x = (2.0 * double(sk)) * cast<double>(wk);
+    c128 y = (2.0 * double(sl)) * cast<double>(wl);
+    c128 l = clogcosh(t - x - y) - clogcosh(t) - clogcosh(x) - clogcosh(y);
+    return cast<R>(cexp(l));
+}
+
+// One-flip factor for hidden unit j.
+template <typename R>
+__device__ __forceinline__ cplx<R> factor1(cplx<R> tj, cplx<R> tau, R sk, cplx<R> thj, const cplx<R>* wkj,
+                                           bool& exact) {
+    cplx<R> tt = tj * tau;
+    cplx<R> d = mk(R(1) - sk * tt.re, -sk * tt.im);
+    exact = norm2(d) < R(Cancel<R>::thr2) * norm2(tt);
+    if (exact) d = exact_factor1(thj, sk, *wkj);
+    return d;
+}
+// Two-flip factor for hidden unit j (tx = s_k tau_jk, ty = s_l tau_jl).
+template <typename R>
+__device__ __forceinline__ cplx<R> factor2(cplx<R> tj, cplx<R> tx, cplx<R> ty, R sk, R sl, cplx<R> thj,
+                                           const cplx<R>* wkj, const cplx<R>* wlj, bool& exact) {
+    cplx<R> a = tx * ty, b = tj * (tx + ty);
+    cplx<R> d = one<R>() + a - b;
+    R big = fmax(R(1), fmax(norm2(a), norm2(b)));
+    exact = norm2(d) < R(Cancel<R>::thr2) * big;
+    if (exact) d = exact_factor2(thj, sk, *wkj, sl, *wlj);
+    return d;
+}
+
+// prod_j (1 - s_k t_j tau_jk) with tau given transposed (tauT[j * n + k]); t and theta
+// with stride ts; W column-major (m x n).
+template <typename R>
+__device__ __forceinline__ ScaledProd<R> prod1(int k, R sk, int n, int m, const cplx<R>* t, const cplx<R>* th,
+                                              int ts, const cplx<R>* tauT, const cplx<R>* W) {
     ScaledProd<R> P;
     P.init();
     for (int j = 0; j < m; ++j) {
-        cplx<R> tt = t[size_t(j) * ts] * tauT[size_t(j) * n + k];
-        cplx<R> d = mk(R(1) - sk * tt.re, -sk * tt.im);
+        bool ex;
+        cplx<R> d = factor1<R>(t[size_t(j) * ts], tauT[size_t(j) * n + k], sk, th[size_t(j) * ts],
+                               W + size_t(k) * m + j, ex);
         P.p = P.p * d;
         renorm_if(P, j, RenormChunk<R>::mask);
     }
@@ -63,15 +120,16 @@ __device__ __forceinline__ ScaledProd<R> prod1(int k, R sk, int n, int m, const 
 }
 
 template <typename R>
-__device__ __forceinline__ ScaledProd<R> prod2(int k, R sk, int l, R sl, int n, int m, const cplx<R>* t, int ts,
-                                              const cplx<R>* tauT) {
+__device__ __forceinline__ ScaledProd<R> prod2(int k, R sk, int l, R sl, int n, int m, const cplx<R>* t,
+                                              const cplx<R>* th, int ts, const cplx<R>* tauT, const cplx<R>* W) {
     ScaledProd<R> P;
     P.init();
     for (int j = 0; j < m; ++j) {
         cplx<R> tx = sk * tauT[size_t(j) * n + k];
         cplx<R> ty = sl * tauT[size_t(j) * n + l];
-        cplx<R> tj = t[size_t(j) * ts];
-        cplx<R> d = one<R>() + tx * ty - tj * (tx + ty);
+        bool ex;
+        cplx<R> d = factor2<R>(t[size_t(j) * ts], tx, ty, sk, sl, th[size_t(j) * ts], W + size_t(k) * m + j,
+                               W + size_t(l) * m + j, ex);
         P.p = P.p * d;
         renorm_if(P, j, RenormChunk<R>::mask);
     }

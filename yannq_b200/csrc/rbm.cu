@@ -145,22 +145,26 @@ void rbm_log_psi(yq_rbm_s* q, int ns, const int8_t* d_sigma, c128* d_out) {
 template <typename R>
 __global__ void log_ratio_kernel(int n, int m, int ns, const int8_t* __restrict__ sigma, const c128* __restrict__ theta,
                                  int nflip, const int* __restrict__ flips, const cplx<R>* __restrict__ tauT,
-                                 const c128* __restrict__ Lk, const c128* __restrict__ a, cplx<R>* __restrict__ tws,
-                                 c128* __restrict__ out) {
+                                 const c128* __restrict__ Lk, const c128* __restrict__ a, const cplx<R>* __restrict__ W,
+                                 cplx<R>* __restrict__ tws, c128* __restrict__ out) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= ns) return;
-    cplx<R>* t = tws + size_t(s) * m;
-    for (int j = 0; j < m; ++j) t[j] = cast<R>(ctanh(theta[size_t(s) * m + j]));
+    cplx<R>* t = tws + size_t(s) * 2 * m;
+    cplx<R>* th = t + m;
+    for (int j = 0; j < m; ++j) {
+        t[j] = cast<R>(ctanh(theta[size_t(s) * m + j]));
+        th[j] = cast<R>(theta[size_t(s) * m + j]);
+    }
     const int8_t* sg = sigma + size_t(s) * n;
     int k = flips[size_t(s) * nflip];
     R sk = R(sg[k]);
     if (nflip == 1) {
-        ScaledProd<R> P = prod1<R>(k, sk, n, m, t, 1, tauT);
+        ScaledProd<R> P = prod1<R>(k, sk, n, m, t, th, 1, tauT, W);
         out[s] = base1(Lk, a, k, double(sk)) + log_scaled(P);
     } else {
         int l = flips[size_t(s) * nflip + 1];
         R sl = R(sg[l]);
-        ScaledProd<R> P = prod2<R>(k, sk, l, sl, n, m, t, 1, tauT);
+        ScaledProd<R> P = prod2<R>(k, sk, l, sl, n, m, t, th, 1, tauT, W);
         out[s] = base1(Lk, a, k, double(sk)) + base1(Lk, a, l, double(sl)) + log_scaled(P);
     }
 }
@@ -170,16 +174,16 @@ void rbm_log_ratio(yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_the
     if (ns <= 0) return;
     rbm_prepare(q);
     DevBuf tws;
-    tws.ensure(size_t(ns) * q->m * q->csize());
+    tws.ensure(size_t(ns) * 2 * q->m * q->csize());
     const c128* a = q->use_bias ? q->p64.as<c128>() + size_t(q->n) * q->m : nullptr;
     if (q->dtype == YQ_C64)
         log_ratio_kernel<float><<<cdiv_u(ns, 64), 64, 0, q->ctx->stream>>>(
             q->n, q->m, ns, d_sigma, reinterpret_cast<const c128*>(d_theta), nflip, d_flips, q->tauT.as<c64>(),
-            q->Lk.as<c128>(), a, tws.as<c64>(), d_out);
+            q->Lk.as<c128>(), a, q->W.as<c64>(), tws.as<c64>(), d_out);
     else
         log_ratio_kernel<double><<<cdiv_u(ns, 64), 64, 0, q->ctx->stream>>>(
             q->n, q->m, ns, d_sigma, reinterpret_cast<const c128*>(d_theta), nflip, d_flips, q->tauT.as<c128>(),
-            q->Lk.as<c128>(), a, tws.as<c128>(), d_out);
+            q->Lk.as<c128>(), a, q->W.as<c128>(), tws.as<c128>(), d_out);
     YQ_LAUNCH_CHECK();
     YQ_CUDA(cudaStreamSynchronize(q->ctx->stream));
 }

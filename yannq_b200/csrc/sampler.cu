@@ -168,13 +168,21 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
             if (MOVE == YQ_MOVE_LOCAL) {
                 const R sk = R(s[k]);
                 const cplx<R>* tk = A.tau + size_t(k) * m;
+                const cplx<R>* wk = A.W + size_t(k) * m;
                 cplx<R> tv[JPL], d[JPL];
+                unsigned exact = 0u;  // bit r: factor r re-evaluated in logcosh form (ratio.cuh)
 #pragma unroll
                 for (int r = 0; r < JPL; ++r) {
                     int j = lane + 32 * r;
-                    tv[r] = (j < m) ? tk[j] : mk(R(0), R(0));
-                    cplx<R> tt = t[r] * tv[r];
-                    d[r] = mk(R(1) - sk * tt.re, -sk * tt.im);
+                    if (j < m) {
+                        tv[r] = tk[j];
+                        bool ex;
+                        d[r] = factor1<R>(t[r], tv[r], sk, th[r], wk + j, ex);
+                        exact |= unsigned(ex) << r;
+                    } else {
+                        tv[r] = mk(R(0), R(0));
+                        d[r] = one<R>();
+                    }
                 }
                 R ls = R(0);
                 cplx<R> pr = mk(R(1), R(0));
@@ -192,14 +200,13 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 const R logr = R(0.5) * ls + R(base);
                 // LocalSweeper.hpp:45-47: p = min(1, exp(beta * 2 * Re logRatio)); accept if u < p
                 if (u < exp(two * logr)) {
-                    const cplx<R>* wk = A.W + size_t(k) * m;
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
                         int j = lane + 32 * r;
                         if (j < m) {
                             cplx<R> w = wk[j];
                             th[r] = th[r] - (two * sk) * w;
-                            t[r] = cdiv(t[r] - sk * tv[r], d[r]);
+                            t[r] = ((exact >> r) & 1u) ? ctanh(th[r]) : cdiv(t[r] - sk * tv[r], d[r]);
                         }
                     }
                     __syncwarp();
@@ -214,15 +221,24 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 const R sk = R(sk8), sl = R(sl8);
                 const cplx<R>* tk = A.tau + size_t(k) * m;
                 const cplx<R>* tl = A.tau + size_t(l) * m;
+                const cplx<R>* wk = A.W + size_t(k) * m;
+                const cplx<R>* wl = A.W + size_t(l) * m;
                 cplx<R> tx[JPL], ty[JPL], d[JPL];
+                unsigned exact = 0u;
 #pragma unroll
                 for (int r = 0; r < JPL; ++r) {
                     int j = lane + 32 * r;
-                    cplx<R> a = (j < m) ? tk[j] : mk(R(0), R(0));
-                    cplx<R> b = (j < m) ? tl[j] : mk(R(0), R(0));
-                    tx[r] = sk * a;
-                    ty[r] = sl * b;
-                    d[r] = one<R>() + tx[r] * ty[r] - t[r] * (tx[r] + ty[r]);
+                    if (j < m) {
+                        tx[r] = sk * tk[j];
+                        ty[r] = sl * tl[j];
+                        bool ex;
+                        d[r] = factor2<R>(t[r], tx[r], ty[r], sk, sl, th[r], wk + j, wl + j, ex);
+                        exact |= unsigned(ex) << r;
+                    } else {
+                        tx[r] = mk(R(0), R(0));
+                        ty[r] = mk(R(0), R(0));
+                        d[r] = one<R>();
+                    }
                 }
                 R ls = R(0);
                 cplx<R> pr = mk(R(1), R(0));
@@ -241,8 +257,6 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                             2.0 * double(sl) * A.p64[size_t(n) * m + l].re;
                 const R logr = R(0.5) * ls + R(base);
                 if (u < exp(two * logr)) {
-                    const cplx<R>* wk = A.W + size_t(k) * m;
-                    const cplx<R>* wl = A.W + size_t(l) * m;
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
                         int j = lane + 32 * r;
@@ -252,7 +266,8 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                             cplx<R> dd = mk(-(two * sk) * a.re - (two * sl) * b.re, -(two * sk) * a.im - (two * sl) * b.im);
                             th[r] = th[r] + dd;
                             cplx<R> sxy = tx[r] + ty[r];
-                            t[r] = cdiv(t[r] * (one<R>() + tx[r] * ty[r]) - sxy, d[r]);
+                            t[r] = ((exact >> r) & 1u) ? ctanh(th[r])
+                                                       : cdiv(t[r] * (one<R>() + tx[r] * ty[r]) - sxy, d[r]);
                         }
                     }
                     __syncwarp();
