@@ -72,6 +72,10 @@ int yq_ctx_synchronize(yq_ctx ctx);
  * 6 total, 7 mean + F.  (The reference times sampling and solving with
  * std::chrono: Runners/RunRBM.hpp:169-214.) */
 int yq_ctx_stage_ms(yq_ctx ctx, int stage, float* ms);
+/* Micro-benchmarked device roofs (no reference counterpart): out[0] FP64 SIMT
+ * TFLOP/s, out[1] FP32 SIMT TFLOP/s, out[2] FP64 tensor-core (DMMA) TFLOP/s,
+ * out[3] complex128 logcosh evaluations per second in units of 1e9. */
+int yq_measure_peaks(yq_ctx ctx, double* out);
 
 /* ---- RBM machine (Machines/RBM.hpp) ---------------------------------------- */
 /* RBM<T>(n, m, useBias) -- Machines/RBM.hpp:48-53; dtype YQ_C64 or YQ_C128. */

@@ -53,6 +53,7 @@ SIGNATURES = {
     "yq_ctx_destroy": [_vp],
     "yq_ctx_synchronize": [_vp],
     "yq_ctx_stage_ms": [_vp, _i, _vp],
+    "yq_measure_peaks": [_vp, _vp],
     "yq_rbm_create": [_vp, _i, _i, _i, _i, _vp],
     "yq_rbm_destroy": [_vp],
     "yq_rbm_dim": [_vp, _vp],
@@ -173,6 +174,12 @@ class Context:
         v = C.c_float()
         check(lib().yq_ctx_stage_ms(self.h, STAGES.get(stage, stage), C.byref(v)))
         return v.value
+
+    def measure_peaks(self):
+        out = np.zeros(4)
+        check(lib().yq_measure_peaks(self.h, _p(out)))
+        return {"fp64_simt_tflops": out[0], "fp32_simt_tflops": out[1], "fp64_dmma_tflops": out[2],
+                "logcosh_c128_geval_s": out[3]}
 
 
 class RBM:

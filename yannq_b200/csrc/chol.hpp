@@ -1,0 +1,21 @@
+// Blocked FP64 Cholesky of the shifted SR matrix and the triangular solves
+// (the Eigen::LLT of GroundState/SRMat.hpp:231-237 and Runners/RunRBM.hpp:196-201).
+#pragma once
+#include "common.cuh"
+
+namespace yq {
+
+constexpr int CHOL_NB = 64;
+
+// In-place lower Cholesky of the Hermitian matrix G (row-major, n x n, n a multiple
+// of CHOL_NB, lower triangle used).  Linv / LinvH receive, per diagonal block, the
+// inverse of L_kk and its conjugate transpose (n / CHOL_NB blocks of 64 x 64).
+// A non-positive pivot sets DS_NOT_PD in *status (the factorisation continues with
+// a unit pivot so that every launch stays well defined).
+void chol_factor(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* status, cudaStream_t st);
+
+// out = (L L^H)^{-1} b.  b is overwritten (forward sweep), work holds L^{-1} b.
+void chol_solve(const c128* G, int n, size_t ld, const c128* Linv, const c128* LinvH, c128* b, c128* work,
+                c128* out, cudaStream_t st);
+
+}  // namespace yq

@@ -84,7 +84,7 @@ struct yq_sr_s {
     yq::DevBuf stats;   // double[8]: E, var, mean.re, mean.im, |v|, acc...
     // dense SR matrix and Cholesky factor (lower, row-major, dim_pad x dim_pad)
     int dim = 0, dim_pad = 0;
-    yq::DevBuf G, Linv;
+    yq::DevBuf G, Linv, LinvH;
     // mixed precision operands (BF16 hi/lo planes of [Re|Im] and [Im|-Re])
     yq::DevBuf xh, xl, yh, yl;
     double host_stats[8] = {};

@@ -7,12 +7,14 @@
 #include <cmath>
 #include <vector>
 
+#include "chol.hpp"
+#include "gemm64.cuh"
 #include "gram_tc.hpp"
 #include "internal.hpp"
 
 namespace yq {
 
-static constexpr int NB = 64;  // Cholesky block size
+static constexpr int NB = CHOL_NB;  // Cholesky block size
 
 // ---------------------------------------------------------------------------
 template <typename R>
@@ -208,290 +210,12 @@ __global__ void centred_rhs_kernel(int ns, int ns_pad, const c128* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// FP64 complex Gram matrix, lower tiles only:  C(r, c) = alpha sum_k Z(r, k) conj(Z(c, k))
-// (+ C if accumulate) (+ shift on the diagonal).  Z(r, k) = Z[r ld + k] (kmode 0, rows
-// K-contiguous: T-mode and the Cholesky trailing update) or conj(Z[k ld + r])
-// (kmode 1: S = O~^H O~ from row-major O~).  64 x 64 tiles, 4 x 4 per thread.
-template <typename R, int KMODE>
-__global__ void __launch_bounds__(256) gram_fp64_kernel(const cplx<R>* __restrict__ Z, size_t ldz, int nrows, int K,
-                                                        c128* __restrict__ C, size_t ldc, double alpha,
-                                                        int accumulate, double shift) {
-    __shared__ c128 As[16][64 + 1];
-    __shared__ c128 Bs[16][64 + 1];
-    // lower-triangular tile index -> (bi, bj), bi >= bj
-    const long long tix = blockIdx.x;
-    long long bi = (long long)((sqrt(8.0 * double(tix) + 1.0) - 1.0) * 0.5);
-    while (bi * (bi + 1) / 2 > tix) --bi;
-    while ((bi + 1) * (bi + 2) / 2 <= tix) ++bi;
-    const long long bj = tix - bi * (bi + 1) / 2;
-    const int r0 = int(bi) * 64, c0 = int(bj) * 64;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    c128 acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = mk(0., 0.);
-
-    for (int k0 = 0; k0 < K; k0 += 16) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int e = tid + 256 * q;
-            int row, kk;
-            if (KMODE == 0) {
-                row = e >> 4;
-                kk = e & 15;
-            } else {
-                kk = e >> 6;
-                row = e & 63;
-            }
-            const int k = k0 + kk;
-            c128 va = mk(0., 0.), vb = mk(0., 0.);
-            if (k < K) {
-                const int ra = r0 + row, rb = c0 + row;
-                if (KMODE == 0) {
-                    if (ra < nrows) va = cast<double>(Z[size_t(ra) * ldz + k]);
-                    if (rb < nrows) vb = cast<double>(Z[size_t(rb) * ldz + k]);
-                } else {
-                    if (ra < nrows) va = conj(cast<double>(Z[size_t(k) * ldz + ra]));
-                    if (rb < nrows) vb = conj(cast<double>(Z[size_t(k) * ldz + rb]));
-                }
-            }
-            As[kk][row] = va;
-            Bs[kk][row] = vb;
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int kk = 0; kk < 16; ++kk) {
-            c128 a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    // a * conj(b)
-                    acc[i][j].re += a[i].re * b[j].re + a[i].im * b[j].im;
-                    acc[i][j].im += a[i].im * b[j].re - a[i].re * b[j].im;
-                }
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int r = r0 + ty + 16 * i, c = c0 + tx + 16 * j;
-            if (r < nrows && c < nrows && r >= c) {
-                c128 v = alpha * acc[i][j];
-                c128* dst = C + size_t(r) * ldc + c;
-                if (accumulate) v = v + *dst;
-                if (r == c) v.re += shift;
-                *dst = v;
-            }
-        }
-}
-
-template <typename R>
-static void gram_fp64(const cplx<R>* Z, size_t ldz, int kmode, int nrows, int K, c128* C, size_t ldc, double alpha,
-                      int accumulate, double shift, cudaStream_t st) {
-    if (nrows <= 0) return;
-    const long long nt = (nrows + 63) / 64;
-    const long long tiles = nt * (nt + 1) / 2;
-    if (kmode == 0)
-        gram_fp64_kernel<R, 0><<<unsigned(tiles), 256, 0, st>>>(Z, ldz, nrows, K, C, ldc, alpha, accumulate, shift);
-    else
-        gram_fp64_kernel<R, 1><<<unsigned(tiles), 256, 0, st>>>(Z, ldz, nrows, K, C, ldc, alpha, accumulate, shift);
-    YQ_LAUNCH_CHECK();
-}
-
 // Padding of the SR matrix to a multiple of NB: zero off-diagonal, unit diagonal.
 __global__ void pad_identity_kernel(c128* G, int dim, int dim_pad) {
     size_t total = size_t(dim_pad) * dim_pad;
     for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < total; q += size_t(gridDim.x) * blockDim.x) {
         int r = int(q / dim_pad), c = int(q % dim_pad);
         if (r >= dim || c >= dim) G[q] = mk(r == c ? 1.0 : 0.0, 0.0);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Blocked right-looking Cholesky (lower, row-major, in place), NB = 64.
-// Diagonal block: unblocked factorisation in shared memory + the inverse of
-// L_kk (stored in Linv for the panel TRSM and the triangular solves).
-__global__ void __launch_bounds__(256) potrf_diag_kernel(c128* __restrict__ G, size_t ld, int k0,
-                                                         c128* __restrict__ Linv, int* __restrict__ status) {
-    extern __shared__ c128 sm[];
-    c128* A = sm;             // [64][64]
-    c128* X = sm + NB * NB;   // [64][64] inverse
-    const int tid = threadIdx.x;
-    for (int e = tid; e < NB * NB; e += blockDim.x) {
-        int r = e / NB, c = e % NB;
-        A[e] = (c <= r) ? G[size_t(k0 + r) * ld + k0 + c] : mk(0., 0.);
-        X[e] = mk(0., 0.);
-    }
-    __syncthreads();
-    for (int c = 0; c < NB; ++c) {
-        if (tid == 0) {
-            double d = A[c * NB + c].re;
-            if (!(d > 0.0)) {
-                atomicOr(status, DS_NOT_PD);
-                d = 1.0;
-            }
-            A[c * NB + c] = mk(sqrt(d), 0.0);
-        }
-        __syncthreads();
-        const double inv = 1.0 / A[c * NB + c].re;
-        for (int r = c + 1 + tid; r < NB; r += blockDim.x) A[r * NB + c] = inv * A[r * NB + c];
-        __syncthreads();
-        const int w = NB - c - 1;
-        for (int e = tid; e < w * w; e += blockDim.x) {
-            int r = c + 1 + e / w, q = c + 1 + e % w;
-            if (q <= r) A[r * NB + q] = A[r * NB + q] - A[r * NB + c] * conj(A[q * NB + c]);
-        }
-        __syncthreads();
-    }
-    // X = L^{-1} by forward substitution, one column per thread
-    if (tid < NB) {
-        const int col = tid;
-        for (int r = col; r < NB; ++r) {
-            c128 acc = mk(r == col ? 1.0 : 0.0, 0.0);
-            for (int q = col; q < r; ++q) acc = acc - A[r * NB + q] * X[q * NB + col];
-            X[r * NB + col] = (1.0 / A[r * NB + r].re) * acc;
-        }
-    }
-    __syncthreads();
-    for (int e = tid; e < NB * NB; e += blockDim.x) {
-        int r = e / NB, c = e % NB;
-        if (c <= r) G[size_t(k0 + r) * ld + k0 + c] = A[e];
-        Linv[e] = X[e];
-    }
-}
-
-// Panel: L[r, k0:k0+64] = A[r, k0:k0+64] L_kk^{-H} for rows r >= k0 + 64.
-__global__ void __launch_bounds__(256) trsm_panel_kernel(c128* __restrict__ G, size_t ld, int k0, int dim_pad,
-                                                         const c128* __restrict__ Linv) {
-    extern __shared__ c128 sm[];
-    c128* X = sm;             // [64][64]
-    c128* Ar = sm + NB * NB;  // [32][64]
-    const int tid = threadIdx.x;
-    const int rbase = k0 + NB + blockIdx.x * 32;
-    for (int e = tid; e < NB * NB; e += blockDim.x) X[e] = Linv[e];
-    for (int e = tid; e < 32 * NB; e += blockDim.x) {
-        int rr = e / NB, c = e % NB;
-        int r = rbase + rr;
-        Ar[e] = (r < dim_pad) ? G[size_t(r) * ld + k0 + c] : mk(0., 0.);
-    }
-    __syncthreads();
-    // thread -> (row rr = tid / 8, columns c = (tid % 8) + 8 q)
-    const int rr = tid >> 3, cg = tid & 7;
-    const int r = rbase + rr;
-    if (r >= dim_pad) return;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int c = cg + 8 * q;
-        c128 acc = mk(0., 0.);
-        for (int qq = 0; qq <= c; ++qq) acc = acc + Ar[rr * NB + qq] * conj(X[c * NB + qq]);
-        G[size_t(r) * ld + k0 + c] = acc;
-    }
-}
-
-// Forward step kb of L x = y: x_kb = Linv_kb y_kb; y_r -= L[r, kb block] x_kb for r beyond the block.
-__global__ void __launch_bounds__(256) trsv_fwd_kernel(const c128* __restrict__ G, size_t ld, int k0, int dim_pad,
-                                                       const c128* __restrict__ Linv, c128* __restrict__ y,
-                                                       c128* __restrict__ x) {
-    __shared__ c128 yb[NB], xb[NB];
-    const int tid = threadIdx.x;
-    if (tid < NB) yb[tid] = y[k0 + tid];
-    __syncthreads();
-    if (tid < NB) {
-        c128 acc = mk(0., 0.);
-        for (int q = 0; q <= tid; ++q) acc = acc + Linv[tid * NB + q] * yb[q];
-        xb[tid] = acc;
-        if (blockIdx.x == 0) x[k0 + tid] = acc;
-    }
-    __syncthreads();
-    const int r = k0 + NB + blockIdx.x * blockDim.x + tid;
-    if (r < dim_pad) {
-        c128 acc = mk(0., 0.);
-        const c128* row = G + size_t(r) * ld + k0;
-        for (int q = 0; q < NB; ++q) acc = acc + row[q] * xb[q];
-        y[r] = y[r] - acc;
-    }
-}
-
-// Backward step kb of L^H z = x: z_kb = Linv_kb^H x_kb; x_r -= sum_q conj(L[k0+q, r]) z_kb[q] for r < k0.
-__global__ void __launch_bounds__(256) trsv_bwd_kernel(const c128* __restrict__ G, size_t ld, int k0,
-                                                       const c128* __restrict__ Linv, c128* __restrict__ xv,
-                                                       c128* __restrict__ z) {
-    __shared__ c128 xb[NB], zb[NB];
-    const int tid = threadIdx.x;
-    if (tid < NB) xb[tid] = xv[k0 + tid];
-    __syncthreads();
-    if (tid < NB) {
-        c128 acc = mk(0., 0.);
-        for (int q = tid; q < NB; ++q) acc = acc + conj(Linv[q * NB + tid]) * xb[q];
-        zb[tid] = acc;
-        if (blockIdx.x == 0) z[k0 + tid] = acc;
-    }
-    __syncthreads();
-    const int r = blockIdx.x * blockDim.x + tid;
-    if (r < k0) {
-        c128 acc = mk(0., 0.);
-        for (int q = 0; q < NB; ++q) acc = acc + conj(G[size_t(k0 + q) * ld + r]) * zb[q];
-        xv[r] = xv[r] - acc;
-    }
-}
-
-static void cholesky(yq_sr_s* sr) {
-    cudaStream_t st = sr->q->ctx->stream;
-    int* status = sr->q->ctx->status.as<int>();
-    const int n = sr->dim_pad;
-    const size_t ld = size_t(n);
-    c128* G = sr->G.as<c128>();
-    const int nb = n / NB;
-    static bool attr = false;
-    if (!attr) {
-        YQ_CUDA(cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(2 * NB * NB * sizeof(c128))));
-        YQ_CUDA(cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int((NB * NB + 32 * NB) * sizeof(c128))));
-        attr = true;
-    }
-    for (int kb = 0; kb < nb; ++kb) {
-        const int k0 = kb * NB;
-        c128* Li = sr->Linv.as<c128>() + size_t(kb) * NB * NB;
-        potrf_diag_kernel<<<1, 256, 2 * NB * NB * sizeof(c128), st>>>(G, ld, k0, Li, status);
-        YQ_LAUNCH_CHECK();
-        const int rest = n - k0 - NB;
-        if (rest <= 0) break;
-        trsm_panel_kernel<<<cdiv_u(rest, 32), 256, (NB * NB + 32 * NB) * sizeof(c128), st>>>(G, ld, k0, n, Li);
-        YQ_LAUNCH_CHECK();
-        gram_fp64<double>(G + size_t(k0 + NB) * ld + k0, ld, 0, rest, NB, G + size_t(k0 + NB) * ld + k0 + NB, ld,
-                          -1.0, 1, 0.0, st);
-    }
-}
-
-// b (dim_pad) -> (L L^H)^{-1} b, using work as scratch; result in out.
-static void chol_solve(yq_sr_s* sr, c128* b, c128* work, c128* out) {
-    cudaStream_t st = sr->q->ctx->stream;
-    const int n = sr->dim_pad;
-    const size_t ld = size_t(n);
-    const c128* G = sr->G.as<c128>();
-    const int nb = n / NB;
-    for (int kb = 0; kb < nb; ++kb) {
-        const int k0 = kb * NB;
-        const int rest = n - k0 - NB;
-        trsv_fwd_kernel<<<std::max(1u, cdiv_u(std::max(rest, 0), 256)), 256, 0, st>>>(
-            G, ld, k0, n, sr->Linv.as<c128>() + size_t(kb) * NB * NB, b, work);
-        YQ_LAUNCH_CHECK();
-    }
-    for (int kb = nb - 1; kb >= 0; --kb) {
-        const int k0 = kb * NB;
-        trsv_bwd_kernel<<<std::max(1u, cdiv_u(k0, 256)), 256, 0, st>>>(G, ld, k0,
-                                                                      sr->Linv.as<c128>() + size_t(kb) * NB * NB,
-                                                                      work, out);
-        YQ_LAUNCH_CHECK();
     }
 }
 
@@ -648,6 +372,7 @@ static void form_matrix_t(yq_sr_s* sr, double shift) {
     const int ns = sr->ns;
     sr->G.ensure(size_t(sr->dim_pad) * sr->dim_pad * sizeof(c128));
     sr->Linv.ensure(size_t(sr->dim_pad / NB) * NB * NB * sizeof(c128));
+    sr->LinvH.ensure(size_t(sr->dim_pad / NB) * NB * NB * sizeof(c128));
     c128* G = sr->G.as<c128>();
     if (sr->dim_pad != sr->dim) {
         pad_identity_kernel<<<148 * 8, 256, 0, st>>>(G, sr->dim, sr->dim_pad);
@@ -798,15 +523,19 @@ static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps) {
     form_matrix_t<R>(sr, shift);
     ctx->stage_end(ST_GRAM);
     ctx->stage_begin(ST_SOLVE);
-    cholesky(sr);
+    chol_factor(sr->G.as<c128>(), sr->dim_pad, size_t(sr->dim_pad), sr->Linv.as<c128>(), sr->LinvH.as<c128>(),
+                sr->q->ctx->status.as<int>(), st);
     const size_t dp = size_t(sr->dim_pad);
+    const c128* G = sr->G.as<c128>();
+    const c128* Li = sr->Linv.as<c128>();
+    const c128* LiH = sr->LinvH.as<c128>();
     if (sr->mode == YQ_SR_T) {
         // y = (T + shift)^{-1} (E - <E>) / Ns ; v = O~^H y   (push-through identity)
         c128* b = sr->rhs.as<c128>();
         YQ_CUDA(cudaMemcpyAsync(b, sr->y.as<c128>(), dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
         c128* sol = sr->s1.as<c128>();
         c128* tmp = sr->s2.as<c128>();
-        chol_solve(sr, b, tmp, sol);
+        chol_solve(G, sr->dim_pad, dp, Li, LiH, b, tmp, sol, st);
         // iterative refinement against the exact operator (T y = O~ (O~^H y) / Ns + shift y, FP64 sums)
         for (int k = 0; k < ir_steps; ++k) {
             c128* ty = sr->s3.as<c128>();
@@ -818,7 +547,7 @@ static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps) {
             axpy_kernel<<<cdiv_u(ns, 256), 256, 0, st>>>(size_t(ns), mk(shift, 0.0), sol, ty);
             residual_kernel<<<cdiv_u(dp, 256), 256, 0, st>>>(dp, sr->y.as<c128>(), ty, r);
             YQ_LAUNCH_CHECK();
-            chol_solve(sr, r, tmp, dy);
+            chol_solve(G, sr->dim_pad, dp, Li, LiH, r, tmp, dy, st);
             axpy_kernel<<<cdiv_u(dp, 256), 256, 0, st>>>(dp, mk(1.0, 0.0), dy, sol);
             YQ_LAUNCH_CHECK();
         }
@@ -827,7 +556,7 @@ static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps) {
         c128* b = sr->rhs.as<c128>();
         YQ_CUDA(cudaMemsetAsync(b, 0, dp * sizeof(c128), st));
         YQ_CUDA(cudaMemcpyAsync(b, sr->grad.as<c128>(), P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
-        chol_solve(sr, b, sr->s2.as<c128>(), sr->s1.as<c128>());
+        chol_solve(G, sr->dim_pad, dp, Li, LiH, b, sr->s2.as<c128>(), sr->s1.as<c128>(), st);
         YQ_CUDA(cudaMemcpyAsync(sr->v.as<c128>(), sr->s1.p, P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
     }
     ctx->stage_end(ST_SOLVE);
