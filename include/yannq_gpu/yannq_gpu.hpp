@@ -1,0 +1,379 @@
+// yannq_gpu.hpp -- header-only C++ adapters over the C ABI of libyannq_b200.
+//
+// They keep the names and call pattern of yannq's template API so that a driver
+// written against Yannq/Machines, Yannq/Samplers, Yannq/Hamiltonians,
+// Yannq/GroundState and Yannq/Runners switches to the B200 backend by changing
+// types, not code:
+//
+//   yannq::RBM<T>                      -> yannq::gpu::RBM<T>          (Machines/RBM.hpp)
+//   TFIsing / XXZ                      -> yannq::gpu::TFIsing / XXZ   (Hamiltonians/*.hpp)
+//   LocalSweeper / SwapSweeper         -> same names in yannq::gpu    (Samplers/*Sweeper.hpp)
+//   SamplerMT<Machine, State, Sweeper> -> yannq::gpu::SamplerMT<Machine, Sweeper>
+//   SRMat<Machine, Hamiltonian>        -> yannq::gpu::SRMat<Machine, Hamiltonian>
+//   RunRBM<T>                          -> yannq::gpu::RunRBM<T>        (Runners/RunRBM.hpp)
+//
+// Parameters, samples and the SR solution stay on the device; vectors cross the
+// boundary as std::vector<std::complex<double>> in the reference's layout
+// [W column-major (m x n) | a | b].  Errors of the C ABI become yannq::gpu::Error.
+#pragma once
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../yannq_b200.h"
+
+namespace yannq {
+namespace gpu {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+inline void check(int code) {
+    if (code != YQ_OK) {
+        char buf[1024];
+        yq_last_error(buf, sizeof(buf));
+        if (code == YQ_E_ARG) throw std::invalid_argument(buf);
+        throw Error(code, buf);
+    }
+}
+
+using cd = std::complex<double>;
+
+// One device and its stream (no reference counterpart: the reference is host-only).
+class Context {
+    yq_ctx h_ = nullptr;
+
+public:
+    explicit Context(int device = 0) { check(yq_ctx_create(device, &h_)); }
+    ~Context() { yq_ctx_destroy(h_); }
+    Context(const Context&) = delete;
+    Context& operator=(const Context&) = delete;
+    yq_ctx handle() const { return h_; }
+    void synchronize() const { check(yq_ctx_synchronize(h_)); }
+    // device milliseconds of the last call's stage: "sample", "eloc", "O", "gram", "solve", "update", "total"
+    float stageMs(int stage) const {
+        float ms = 0.f;
+        check(yq_ctx_stage_ms(h_, stage, &ms));
+        return ms;
+    }
+};
+
+// Machines/RBM.hpp: RBM<T>(n, m, useBias) with T = std::complex<double> (FP64 path)
+// or std::complex<float> (mixed-precision path).
+template <typename T>
+class RBM {
+    static_assert(std::is_same<T, std::complex<double>>::value || std::is_same<T, std::complex<float>>::value,
+                  "yannq::gpu::RBM supports complex<double> and complex<float>");
+    yq_rbm h_ = nullptr;
+    uint32_t n_, m_;
+    bool useBias_;
+    size_t dim_ = 0;
+
+public:
+    using Scalar = T;
+    using RealScalar = typename T::value_type;
+    using Vector = std::vector<cd>;
+
+    RBM(Context& ctx, uint32_t n, uint32_t m, bool useBias = true) : n_(n), m_(m), useBias_(useBias) {
+        check(yq_rbm_create(ctx.handle(), int(n), int(m), useBias ? 1 : 0,
+                            std::is_same<T, std::complex<double>>::value ? YQ_C128 : YQ_C64, &h_));
+        check(yq_rbm_dim(h_, &dim_));
+    }
+    ~RBM() { yq_rbm_destroy(h_); }
+    RBM(const RBM&) = delete;
+    RBM& operator=(const RBM&) = delete;
+
+    yq_rbm handle() const { return h_; }
+    uint32_t getN() const { return n_; }
+    uint32_t getM() const { return m_; }
+    uint32_t getDim() const { return uint32_t(dim_); }
+    bool useBias() const { return useBias_; }
+
+    // RBM.hpp:271-291
+    Vector getParams() const {
+        Vector p(dim_);
+        check(yq_rbm_get_params(h_, reinterpret_cast<double*>(p.data())));
+        return p;
+    }
+    void setParams(const Vector& p) {
+        if (p.size() != dim_) throw std::invalid_argument("setParams: size != getDim()");
+        check(yq_rbm_set_params(h_, reinterpret_cast<const double*>(p.data())));
+    }
+    // RBM.hpp:261-269
+    void updateParams(const Vector& d) {
+        if (d.size() != dim_) throw std::invalid_argument("updateParams: size != getDim()");
+        check(yq_rbm_update_params(h_, reinterpret_cast<const double*>(d.data())));
+    }
+    // RBM.hpp:325-349 (Philox-seeded normal draws in the reference's order)
+    void initializeRandom(uint64_t seed, double sigma = 1e-3) { check(yq_rbm_init_random(h_, seed, sigma)); }
+
+    // logCoeff over configurations (ns x n, entries +-1), RBM.hpp:367-378
+    std::vector<cd> logCoeff(const std::vector<int8_t>& sigma) const {
+        const int ns = int(sigma.size() / n_);
+        std::vector<cd> out(ns);
+        check(yq_rbm_log_psi(h_, ns, sigma.data(), reinterpret_cast<double*>(out.data())));
+        return out;
+    }
+    // calcTheta over configurations, RBM.hpp:137-141
+    std::vector<cd> calcTheta(const std::vector<int8_t>& sigma) const {
+        const int ns = int(sigma.size() / n_);
+        std::vector<cd> out(size_t(ns) * m_);
+        check(yq_rbm_theta(h_, ns, sigma.data(), reinterpret_cast<double*>(out.data())));
+        return out;
+    }
+    // logDeriv over (sigma, theta) samples, RBM.hpp:390-406 (row per sample)
+    std::vector<cd> logDeriv(const std::vector<int8_t>& sigma, const std::vector<cd>& theta) const {
+        const int ns = int(sigma.size() / n_);
+        std::vector<cd> out(size_t(ns) * dim_);
+        check(yq_rbm_log_deriv(h_, ns, sigma.data(), reinterpret_cast<const double*>(theta.data()),
+                               reinterpret_cast<double*>(out.data())));
+        return out;
+    }
+};
+
+// Hamiltonians (duck-typed in the reference; here descriptors of device kernels)
+class Hamiltonian {
+    yq_ham h_ = nullptr;
+    int n_;
+
+protected:
+    Hamiltonian(Context& ctx, int kind, int n, int lx, int ly, double J, double h, bool sign) : n_(n) {
+        check(yq_ham_create(ctx.handle(), kind, n, lx, ly, J, h, sign ? 1 : 0, &h_));
+    }
+
+public:
+    virtual ~Hamiltonian() { yq_ham_destroy(h_); }
+    Hamiltonian(const Hamiltonian&) = delete;
+    Hamiltonian& operator=(const Hamiltonian&) = delete;
+    yq_ham handle() const { return h_; }
+    int size() const { return n_; }
+};
+// Hamiltonians/TFIsing.hpp: E_loc = sum_i J s_i s_{i+1} + h ratio(i)
+struct TFIsing : Hamiltonian {
+    TFIsing(Context& ctx, int n, double J, double h) : Hamiltonian(ctx, YQ_HAM_TFI, n, 0, 0, J, h, false) {}
+};
+// Hamiltonians/XXZ.hpp
+struct XXZ : Hamiltonian {
+    XXZ(Context& ctx, int n, double J, double Delta, bool signRule = false)
+        : Hamiltonian(ctx, YQ_HAM_XXZ, n, 0, 0, J, Delta, signRule) {}
+};
+// periodic lx x ly square lattice (no reference counterpart)
+struct TFIsing2D : Hamiltonian {
+    TFIsing2D(Context& ctx, int lx, int ly, double J, double h)
+        : Hamiltonian(ctx, YQ_HAM_TFI2D, lx * ly, lx, ly, J, h, false) {}
+};
+
+// Samplers/LocalSweeper.hpp, Samplers/SwapSweeper.hpp (+ neighbour-pair variant)
+struct LocalSweeper {
+    static constexpr int move = YQ_MOVE_LOCAL;
+    uint32_t n;
+    explicit LocalSweeper(uint32_t n_) : n(n_) {}
+};
+struct SwapSweeper {
+    static constexpr int move = YQ_MOVE_EXCHANGE_ANY;
+    uint32_t n;
+    explicit SwapSweeper(uint32_t n_) : n(n_) {}
+};
+struct SwapSweeperNN {
+    static constexpr int move = YQ_MOVE_EXCHANGE_NN;
+    uint32_t n;
+    explicit SwapSweeperNN(uint32_t n_) : n(n_) {}
+};
+
+// Samples of the last sample() call; they stay on the device.
+struct SampleSet {
+    yq_sampler sampler;
+    int ns;
+    std::size_t size() const { return std::size_t(ns); }
+};
+
+// Samplers/SamplerMT.hpp with nTmps = 1 (parallel tempering is not built).
+template <class Machine, class Sweeper>
+class SamplerMT {
+    yq_sampler h_ = nullptr;
+    uint64_t seed_ = 0;
+    uint32_t epoch_ = 0;
+    bool reinit_ = true;
+
+public:
+    SamplerMT(const Machine& qs, uint32_t nTmps, uint32_t nChainsPer, const Sweeper& sw, int nup = -1) {
+        if (nTmps != 1) throw std::invalid_argument("SamplerMT: only nTmps = 1 is built (no parallel tempering)");
+        if (sw.n != qs.getN()) throw std::invalid_argument("SamplerMT: sweeper size differs from the machine");
+        check(yq_sampler_create(qs.handle(), int(nChainsPer), Sweeper::move, nup, 0, &h_));
+    }
+    ~SamplerMT() { yq_sampler_destroy(h_); }
+    SamplerMT(const SamplerMT&) = delete;
+    SamplerMT& operator=(const SamplerMT&) = delete;
+    yq_sampler handle() const { return h_; }
+
+    // SamplerMT.hpp:72-79 (seeded instead of std::random_device)
+    void initializeRandomEngine(uint64_t seed = 0) { seed_ = seed; }
+    // SamplerMT.hpp:103-110: fresh random chains at the next sample() call
+    void randomize() { reinit_ = true; }
+    // keep the chains across calls (persistent Markov chains)
+    void keepChains() { reinit_ = false; }
+    // SamplerMT.hpp:180-204
+    SampleSet sample(uint32_t nSweeps, uint32_t nDiscard) {
+        check(yq_sample(h_, int(nSweeps), int(nDiscard), seed_, epoch_++, reinit_ ? 1 : 0));
+        int ns = 0;
+        check(yq_sampler_num_samples(h_, &ns));
+        return SampleSet{h_, ns};
+    }
+    void setEpoch(uint32_t e) { epoch_ = e; }
+    bool reinit() const { return reinit_; }
+    uint64_t seed() const { return seed_; }
+    uint32_t epoch() const { return epoch_; }
+};
+
+// GroundState/SRMat.hpp
+template <class Machine, class Ham>
+class SRMat {
+    yq_sr h_ = nullptr;
+    const Machine& qs_;
+
+public:
+    template <class Sampler>
+    SRMat(const Machine& qs, const Ham& ham, const Sampler& sampler, int mode = YQ_SR_AUTO)
+        : qs_(qs) {
+        const int prec = std::is_same<typename Machine::Scalar, std::complex<float>>::value ? YQ_PREC_MIXED
+                                                                                            : YQ_PREC_FP64;
+        check(yq_sr_create(qs.handle(), ham.handle(), sampler.handle(), prec == YQ_PREC_MIXED ? YQ_SR_T : mode, prec,
+                           &h_));
+    }
+    ~SRMat() { yq_sr_destroy(h_); }
+    SRMat(const SRMat&) = delete;
+    SRMat& operator=(const SRMat&) = delete;
+    yq_sr handle() const { return h_; }
+
+    // SRMat.hpp:89-103 (the sample set must come from the bound sampler)
+    void constructFromSamples(const SampleSet&) { check(yq_sr_construct(h_)); }
+    // SRMat.hpp:151-159
+    double eloc() const {
+        double e, v;
+        check(yq_sr_energy(h_, &e, &v));
+        return e;
+    }
+    double elocVar() const {
+        double e, v;
+        check(yq_sr_energy(h_, &e, &v));
+        return v;
+    }
+    std::vector<cd> energyGrad() const { return get(2, qs_.getDim()); }
+    std::vector<cd> oloc() const { return get(1, qs_.getDim()); }
+    // SRMat.hpp:231-237
+    std::vector<cd> solveExact(double shift) {
+        std::vector<cd> v(qs_.getDim());
+        check(yq_sr_solve(h_, shift, YQ_SOLVE_LLT, 0.0, reinterpret_cast<double*>(v.data()), nullptr, nullptr));
+        return v;
+    }
+    // SRMat.hpp:197-208
+    std::vector<cd> solveCG(double shift, double tol = 1e-4, int* iters = nullptr, double* relres = nullptr) {
+        std::vector<cd> v(qs_.getDim());
+        check(yq_sr_solve(h_, shift, YQ_SOLVE_CG, tol, reinterpret_cast<double*>(v.data()), iters, relres));
+        return v;
+    }
+    // SRMat.hpp:142-149 (lower triangle of S or of the dual T, without shift)
+    std::vector<cd> corrMat(int* dim) {
+        check(yq_sr_matrix(h_, dim, nullptr));
+        std::vector<cd> out(size_t(*dim) * size_t(*dim));
+        check(yq_sr_matrix(h_, dim, reinterpret_cast<double*>(out.data())));
+        return out;
+    }
+
+private:
+    std::vector<cd> get(int which, size_t n) const {
+        std::vector<cd> out(n);
+        check(yq_sr_get(h_, which, reinterpret_cast<double*>(out.data())));
+        return out;
+    }
+};
+
+// Optimizers/SGD.hpp: update = -max(alpha / t^p, 1e-4) v
+struct SGD {
+    double alpha = 0.05, p = 0.0;
+    int t = 0;
+    double eta() {
+        ++t;
+        return std::max(alpha / std::pow(double(t), p), 1e-4);
+    }
+};
+
+// Runners/RunRBM.hpp:123-222: the epoch loop on the device.
+template <typename T>
+class RunRBM {
+    Context& ctx_;
+    RBM<T> qs_;
+    double lambdaIni_ = 1e-3, lambdaDecay_ = 1.0, lambdaMin_ = 1e-4;
+    int maxIter_ = 2000;
+    bool useCG_ = false;
+    double cgTol_ = 1e-4;
+    double gradClip_ = 0.0;
+    SGD opt_;
+    bool initialized_ = false;
+
+public:
+    RunRBM(Context& ctx, unsigned N, unsigned alpha, bool useBias) : ctx_(ctx), qs_(ctx, N, alpha * N, useBias) {}
+    RBM<T>& getQs() { return qs_; }
+    void initializeRandom(uint64_t seed, double wIni = 1e-3) {
+        qs_.initializeRandom(seed, wIni);
+        initialized_ = true;
+    }
+    void setLambda(double ini, double decay = 1.0, double mn = 0.0) {
+        lambdaIni_ = ini;
+        lambdaDecay_ = decay;
+        lambdaMin_ = mn;
+    }
+    void setIterParams(int maxIter, int /*saveWfPer*/) { maxIter_ = maxIter; }
+    void setOptimizer(const SGD& opt) { opt_ = opt; }
+    void setSolverParams(bool useCG, double cgTol = 1e-4) {
+        useCG_ = useCG;
+        cgTol_ = cgTol;
+    }
+    void setGradClip(double clip) { gradClip_ = clip; }
+
+    // callback(ll, currE, nv, cgErr, smp_ms, slv_ms) as RunRBM.hpp:219
+    template <class Sampler, class Ham, class Callback>
+    void run(Sampler& sampler, Callback&& callback, Ham& ham, int nSweeps, int nSweepsDiscard = -1,
+             uint64_t seed = 0) {
+        if (!initialized_) initializeRandom(seed, 1e-3);
+        if (nSweepsDiscard < 0) nSweepsDiscard = int(0.1 * nSweeps);
+        SRMat<RBM<T>, Ham> srm(qs_, ham, sampler);
+        sampler.initializeRandomEngine(seed);
+        for (int ll = 0; ll <= maxIter_; ++ll) {
+            const double lambda = std::max(lambdaIni_ * std::pow(lambdaDecay_, ll), lambdaMin_);
+            const double eta = opt_.eta();
+            if (gradClip_ == 0.0) {
+                yq_iter_params p{nSweeps, nSweepsDiscard, sampler.reinit() ? 1 : 0, seed, uint32_t(ll), lambda, eta,
+                                 useCG_ ? YQ_SOLVE_CG : YQ_SOLVE_LLT, cgTol_,
+                                 std::is_same<T, std::complex<float>>::value ? 2 : 0};
+                yq_iter_result r;
+                check(yq_vmc_iteration(srm.handle(), &p, &r));
+                callback(ll, r.energy, r.update_norm, r.cg_err, ctx_.stageMs(0), ctx_.stageMs(4));
+            } else {
+                sampler.setEpoch(uint32_t(ll));
+                SampleSet sr = sampler.sample(uint32_t(nSweeps), uint32_t(nSweepsDiscard));
+                srm.constructFromSamples(sr);
+                std::vector<cd> v = useCG_ ? srm.solveCG(lambda, cgTol_) : srm.solveExact(lambda);
+                double nv = 0.0;
+                for (auto& x : v) nv += std::norm(x);
+                nv = std::sqrt(nv);
+                const double scale = nv > gradClip_ ? gradClip_ / nv : 1.0;  // RunRBM.hpp:205-209
+                for (auto& x : v) x *= -eta * scale;
+                qs_.updateParams(v);
+                callback(ll, srm.eloc(), nv, 0.0, ctx_.stageMs(0), ctx_.stageMs(4));
+            }
+        }
+    }
+};
+
+}  // namespace gpu
+}  // namespace yannq
