@@ -104,6 +104,22 @@ int yq_rbm_log_ratio(yq_rbm q, int ns, const int8_t* sigma, const double* theta,
 /* logDeriv over a batch -- Machines/RBM.hpp:390-406 / constructDelta
  * (GroundState/utils.hpp:12-51): out ns x getDim() complex, row per sample. */
 int yq_rbm_log_deriv(yq_rbm q, int ns, const int8_t* sigma, const double* theta, double* out);
+/* Column mean of the log-derivative rows (the oloc vector of the SR step) from
+ * samples already on the device, for callers that cannot let the library allocate
+ * device memory (for example a host framework that has reserved the device for
+ * its own allocator, or a service loop where allocation latency and its implicit
+ * synchronisation are not acceptable).  No counterpart in the reference.
+ * d_sigma: ns x n int8 (+-1); d_theta: ns x m in the RBM's compute type (complex64
+ * or complex128, the layout yq_sampler_get_samples returns on the host);
+ * d_oloc: getDim() complex128 output.  All three are device pointers owned by the
+ * caller; the call is asynchronous on the context's stream.
+ * Allocates nothing: its partial sums live in a fixed 4 MiB array compiled into
+ * the library (held by every GPU that loads it), so it rejects machines with
+ * (n + 1) (m + 1) > 262144.  Every call shares that array: calls that overlap on
+ * the GPU race and must be serialised by the caller.  The first call on a device
+ * looks up the array's device address; make that first call before any stream
+ * capture. */
+int yq_rbm_oloc_noalloc(yq_rbm q, int ns, const int8_t* d_sigma, const void* d_theta, double* d_oloc);
 
 /* ---- Hamiltonians (Hamiltonians/TFIsing.hpp, Hamiltonians/XXZ.hpp) -------- */
 /* kind YQ_HAM_TFI: TFIsing(n, J, h); YQ_HAM_XXZ: XXZ(n, J, Delta = h, signRule);

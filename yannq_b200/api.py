@@ -65,6 +65,7 @@ SIGNATURES = {
     "yq_rbm_log_psi": [_vp, _i, _vp, _vp],
     "yq_rbm_log_ratio": [_vp, _i, _vp, _vp, _i, _vp, _vp],
     "yq_rbm_log_deriv": [_vp, _i, _vp, _vp, _vp],
+    "yq_rbm_oloc_noalloc": [_vp, _i, _vp, _vp, _vp],
     "yq_ham_create": [_vp, _i, _i, _i, _i, _d, _d, _i, _vp],
     "yq_ham_destroy": [_vp],
     "yq_ham_enumerate": [_vp, _i, _vp, _vp, _vp, _vp, _vp],

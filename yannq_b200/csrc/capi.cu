@@ -8,6 +8,7 @@
 
 namespace yq {
 std::atomic<unsigned long long> g_launches{0};
+void record_error(const std::string& msg);
 }
 
 using namespace yq;
@@ -31,6 +32,13 @@ int guard(F&& f) {
         return YQ_E_ARG;
     }
 }
+
+}  // namespace
+
+// Lets entry points defined in other files report their failure to yq_last_error().
+void yq::record_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
 
 void need(const void* p, const char* what) {
     if (!p) throw Error(YQ_E_ARG, std::string("null argument: ") + what);
