@@ -238,6 +238,63 @@ def cpu_sample(steps=1, warmup=0):
     return 1.0 / statistics.mean(times), cores, sample
 
 
+def suite(api, ctx, hbm_gbs):
+    """Secondary workloads, reported beside the headline.
+
+    xxz64: 1D XXZ chain N = 64, Delta = 1, periodic, Sz = 0, RBM alpha = 4 (P = 16,704),
+    4096 chains x 32 recorded sweeps (+32 thermalisation) of anti-aligned neighbour
+    exchanges -> 131,072 samples; times the sampler, E_loc and the O writer (HBM write
+    bound: Ns P x 8 / 16 bytes) in complex64 and complex128.
+    ff40: FeedForward Conv1D(1->12, K 5) -> LnCosh -> FC(480->16) -> LnCosh -> Sum on
+    N = 40 spins (P = 7,740), forward + adjoint at batch 4096 / 16384 / 65536 with
+    activations stored vs recomputed; O write bandwidth, TFI E_loc at h = 1.
+    """
+    out = {}
+    n, m, chains, sweeps = 64, 256, 4096, 32
+    for name, dt, prec in (("c64", api.C64, api.PREC_MIXED), ("c128", api.C128, api.PREC_FP64)):
+        q = api.RBM(ctx, n, m, True, dt)
+        q.init_random(W["seed"], 0.01)
+        H = api.Hamiltonian.xxz(ctx, n, 1.0, 1.0, False)
+        S = api.Sampler(q, chains, api.MOVE_EXCHANGE_NN, n // 2)
+        sr = api.SR(q, H, S, api.SR_S, prec)
+        S.sample(sweeps, 32, W["seed"], 0, True)
+        S.sample(sweeps, 32, W["seed"], 1, True)
+        t_s = ctx.stage_ms("sample")
+        sr.construct()
+        sr.construct()
+        t_e, t_o = ctx.stage_ms("eloc"), ctx.stage_ms("O")
+        ns = chains * sweeps
+        bytes_o = ns * q.dim * (8 if dt == api.C64 else 16)
+        out[f"xxz64_{name}"] = {"samples": ns, "P": q.dim, "sample_ms": t_s, "samples_per_s": ns / (t_s * 1e-3),
+                                "proposals_per_s": chains * (sweeps + 32) * n / (t_s * 1e-3), "eloc_ms": t_e,
+                                "O_ms": t_o, "O_GBps": bytes_o / (t_o * 1e-3) / 1e9,
+                                "O_frac_of_hbm": bytes_o / (t_o * 1e-3) / 1e9 / hbm_gbs}
+        for x in (sr, S, H, q):
+            x.close()
+    f = api.FeedForward(ctx, 40, 12, 5, 16)
+    f.init_random(W["seed"])
+    ff = {}
+    for batch in (4096, 16384, 65536):
+        f.random_batch(batch, W["seed"])
+        row = {}
+        for mode, budget in (("store", 1 << 62), ("recompute", 0)):
+            f.forward(budget, copy=False)
+            f.adjoint(copy=False)
+            f.forward(budget, copy=False)
+            tf = ctx.stage_ms(8)
+            f.adjoint(copy=False)
+            ta = ctx.stage_ms(9)
+            row[mode] = {"forward_ms": tf, "adjoint_ms": ta,
+                         "O_GBps": batch * f.dim * 4 / (ta * 1e-3) / 1e9}
+        f.eloc_tfi(-1.0, -1.0, copy=False)
+        f.eloc_tfi(-1.0, -1.0, copy=False)
+        row["eloc_ms"] = ctx.stage_ms(10)
+        ff[str(batch)] = row
+    f.close()
+    out["ff40"] = ff
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -246,6 +303,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-suite", action="store_true", help="skip the secondary workloads")
     args = ap.parse_args()
     ws, rank, lrank, pg = _dist()
     warmup = max(3, args.warmup)
@@ -311,6 +369,8 @@ def main():
                               "stages_ms": f["stages_ms"], "energy_per_site": f["energy_per_site"],
                               "gpu_launches": f["launches"]}
         line["mixed_over_fp64"] = f["ms_per_step"] / head["ms_per_step"]
+    if not args.no_suite:
+        line["suite"] = suite(api, ctx, peaks.get("hbm_gbs", 6553.9))
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, cores, sample = cpu_sample(steps=1, warmup=0)
         line["cpu_baseline"] = {"value": v, "unit": "iters/s", "cores": cores, "kind": "port", "sample": sample}

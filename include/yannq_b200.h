@@ -184,6 +184,35 @@ int yq_sr_solve(yq_sr sr, double shift, int solver, double cg_tol, double* v, in
  * (S or T, including the shift), lower triangle, dim x dim complex row-major. */
 int yq_sr_matrix(yq_sr sr, int* dim, double* out);
 
+/* ---- FeedForward machine (Machines/FeedForward.hpp) ------------------------ */
+/* FeedForward with addLayer<Conv1D>(1, channels, kernel, stride 1, no bias),
+ * LnCosh, addLayer<FullyConnected>(L * channels, fc_out, no bias), LnCosh and a
+ * Sum output (fc_out x Mean({fc_out, 1}, 0), layers/Mean.hpp:92-125), FP32
+ * parameters [conv kernel (kernel x channels, column-major) | fc weight
+ * ((L channels) x fc_out, column-major)] (FeedForward.hpp:76-127). */
+typedef struct yq_ff_s* yq_ff;
+int yq_ff_create(yq_ctx ctx, int L, int channels, int kernel, int fc_out, yq_ff* out);
+int yq_ff_destroy(yq_ff f);
+int yq_ff_dim(yq_ff f, size_t* dim);
+int yq_ff_set_params(yq_ff f, const double* params);
+int yq_ff_get_params(yq_ff f, double* params);
+/* initializeRandom(re, Xavier) -- FeedForward.hpp:42-73, Philox-seeded normals. */
+int yq_ff_init_random(yq_ff f, uint64_t seed);
+/* The batch of configurations the next calls act on (batch x L int8 from the host,
+ * or drawn on the device). */
+int yq_ff_set_batch(yq_ff f, int batch, const int8_t* sigma);
+int yq_ff_random_batch(yq_ff f, int batch, uint64_t seed);
+/* forward / makeData -- FeedForward.hpp:152-184: log psi of the batch (host copy if
+ * logpsi != null).  Activations are kept for the adjoint when batch x (L channels +
+ * fc_out) floats fit act_budget_bytes; otherwise the adjoint recomputes them. */
+int yq_ff_forward(yq_ff f, size_t act_budget_bytes, double* logpsi);
+/* backward -- FeedForward.hpp:186-205 with dout = 1: the log-derivative rows
+ * (batch x getDim(), host copy as doubles if O != null). */
+int yq_ff_adjoint(yq_ff f, double* O);
+/* TFIsing(L, J, h)'s local energy of the batch (Hamiltonians/TFIsing.hpp:28-39)
+ * with psi-ratios from single-flip updates of the activations. */
+int yq_ff_eloc_tfi(yq_ff f, double J, double h, double* eloc);
+
 /* ---- one VMC iteration (Runners/RunRBM.hpp:151-221) ----------------------- */
 typedef struct {
     int n_sweeps;          /* recorded sweeps (samples = n_chains * n_sweeps)       */

@@ -88,6 +88,17 @@ SIGNATURES = {
     "yq_sr_solve": [_vp, _d, _i, _d, _vp, _vp, _vp],
     "yq_sr_matrix": [_vp, _vp, _vp],
     "yq_vmc_iteration": [_vp, _vp, _vp],
+    "yq_ff_create": [_vp, _i, _i, _i, _i, _vp],
+    "yq_ff_destroy": [_vp],
+    "yq_ff_dim": [_vp, _vp],
+    "yq_ff_set_params": [_vp, _vp],
+    "yq_ff_get_params": [_vp, _vp],
+    "yq_ff_init_random": [_vp, _u64],
+    "yq_ff_set_batch": [_vp, _i, _vp],
+    "yq_ff_random_batch": [_vp, _i, _u64],
+    "yq_ff_forward": [_vp, _sz, _vp],
+    "yq_ff_adjoint": [_vp, _vp],
+    "yq_ff_eloc_tfi": [_vp, _d, _d, _vp],
 }
 
 _lib = None
@@ -379,3 +390,57 @@ class SR:
         r = IterResult()
         check(lib().yq_vmc_iteration(self.h, C.byref(p), C.byref(r)))
         return r
+
+
+class FeedForward:
+    """Conv1D(1 -> channels, kernel, periodic) -> LnCosh -> FC(L channels -> fc_out) -> LnCosh -> Sum, FP32."""
+
+    def __init__(self, ctx, L, channels, kernel, fc_out):
+        self.ctx, self.L = ctx, L
+        h = C.c_void_p()
+        check(lib().yq_ff_create(ctx.h, L, channels, kernel, fc_out, C.byref(h)))
+        self.h = h
+        d = C.c_size_t()
+        check(lib().yq_ff_dim(h, C.byref(d)))
+        self.dim = d.value
+        self.batch = 0
+
+    def close(self):
+        if self.h:
+            check(lib().yq_ff_destroy(self.h))
+            self.h = None
+
+    def set_params(self, p):
+        check(lib().yq_ff_set_params(self.h, _p(np.ascontiguousarray(p, dtype=np.float64))))
+
+    def get_params(self):
+        out = np.zeros(self.dim)
+        check(lib().yq_ff_get_params(self.h, _p(out)))
+        return out
+
+    def init_random(self, seed):
+        check(lib().yq_ff_init_random(self.h, seed))
+
+    def set_batch(self, sigma):
+        s = _s8(sigma).reshape(-1, self.L)
+        self.batch = s.shape[0]
+        check(lib().yq_ff_set_batch(self.h, self.batch, _p(s)))
+
+    def random_batch(self, batch, seed):
+        self.batch = batch
+        check(lib().yq_ff_random_batch(self.h, batch, seed))
+
+    def forward(self, act_budget_bytes=1 << 62, copy=True):
+        out = np.zeros(self.batch) if copy else None
+        check(lib().yq_ff_forward(self.h, act_budget_bytes, _p(out)))
+        return out
+
+    def adjoint(self, copy=True):
+        out = np.zeros((self.batch, self.dim)) if copy else None
+        check(lib().yq_ff_adjoint(self.h, _p(out)))
+        return out
+
+    def eloc_tfi(self, J, h, copy=True):
+        out = np.zeros(self.batch, np.complex128) if copy else None
+        check(lib().yq_ff_eloc_tfi(self.h, J, h, _p(out)))
+        return out

@@ -629,8 +629,6 @@ int yq_sr_create(yq_rbm q, yq_ham H, yq_sampler S, int mode, int precision, yq_s
             throw Error(YQ_E_ARG, "sr: mixed precision needs a complex64 RBM");
         if (precision == YQ_PREC_FP64 && q->dtype != YQ_C128)
             throw Error(YQ_E_ARG, "sr: FP64 precision needs a complex128 RBM");
-        if (precision == YQ_PREC_MIXED && mode == YQ_SR_S)
-            throw Error(YQ_E_UNSUPPORTED, "sr: the mixed-precision path is built for the T (sample-space) form");
         auto* sr = new yq_sr_s();
         sr->q = q;
         sr->H = H;

@@ -10,7 +10,7 @@
 namespace yq {
 
 enum Stage { ST_SAMPLE = 0, ST_ELOC = 1, ST_O = 2, ST_GRAM = 3, ST_SOLVE = 4, ST_UPDATE = 5, ST_TOTAL = 6, ST_MEAN = 7,
-             ST_COUNT = 8 };
+             ST_FF_FORWARD = 8, ST_FF_ADJOINT = 9, ST_FF_ELOC = 10, ST_COUNT = 11 };
 
 // Device-side status word bits (set by kernels, read once per call by the host).
 enum : int { DS_NONFINITE = 1, DS_NOT_PD = 2, DS_TIMEOUT = 4 };
@@ -63,6 +63,22 @@ struct yq_sampler_s {
     yq::DevBuf acc;      // n_chains u64
     int ns = 0;
     uint64_t proposals = 0;  // per chain, last call
+};
+
+// FeedForward machine Conv1D(1 -> C, kernel K, periodic, no bias) -> LnCosh ->
+// FullyConnected(L C -> F, no bias) -> LnCosh -> Sum, FP32 parameters.
+struct yq_ff_s {
+    yq_ctx_s* ctx = nullptr;
+    int L = 0, C = 0, K = 0, F = 0;
+    size_t P = 0;                 // K C + L C F
+    yq::DevBuf params;            // float [conv kernel (K x C col-major) | fc weight ((L C) x F col-major)]
+    int batch = 0;
+    yq::DevBuf sigma;             // batch x L int8
+    yq::DevBuf logpsi;            // batch double
+    yq::DevBuf acts;              // batch x (L C + F) float, when stored
+    bool acts_valid = false;
+    yq::DevBuf O;                 // batch x P float
+    yq::DevBuf eloc;              // batch c128
 };
 
 struct yq_sr_s {

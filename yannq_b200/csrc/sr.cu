@@ -328,7 +328,7 @@ void sr_construct(yq_sr_s* sr) {
     const size_t P = q->P;
     sr->ns = ns;
     sr->mode = sr->mode_req == YQ_SR_AUTO ? (size_t(ns) < P ? YQ_SR_T : YQ_SR_S) : sr->mode_req;
-    if (sr->precision == YQ_PREC_MIXED) sr->mode = YQ_SR_T;  // tensor-core path is built for the dual form
+    // mixed precision: T-form on the tensor cores; S-form (Ns >= P) with FP32 O~ and FP64 sums
     sr->dim = sr->mode == YQ_SR_T ? ns : int(P);
     sr->dim_pad = ((sr->dim + NB - 1) / NB) * NB;
     const size_t cs = q->csize();
@@ -348,7 +348,7 @@ void sr_construct(yq_sr_s* sr) {
     sr->s3.ensure(vec * sizeof(c128));
     sr->s4.ensure(vec * sizeof(c128));
     sr->stats.ensure(64 * sizeof(double));
-    if (sr->precision == YQ_PREC_MIXED) {
+    if (sr->precision == YQ_PREC_MIXED && sr->mode == YQ_SR_T) {
         const size_t kpad = gram_tc_kpad(P);
         const size_t rows = gram_tc_rows(ns);
         sr->xh.ensure(rows * kpad * 2);
