@@ -18,4 +18,14 @@ void chol_factor(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* status
 void chol_solve(const c128* G, int n, size_t ld, const c128* Linv, const c128* LinvH, c128* b, c128* work,
                 c128* out, cudaStream_t st);
 
+// Persistent tile variants (chol_tile.cu): one cooperative launch each for the
+// factorisation and for each sweep of the solve.  `scratch` holds the tile
+// flags, the work counter and the tile order (chol_tile_scratch_bytes(n) bytes).
+size_t chol_tile_scratch_bytes(int n);
+void chol_factor_tiled(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* status, void* scratch,
+                       int sm_count, cudaStream_t st);
+// out = (L L^H)^{-1} b; b is overwritten with the solution as well.
+void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c128* LinvH, c128* b, c128* out,
+                      int* status, void* scratch, int sm_count, cudaStream_t st);
+
 }  // namespace yq

@@ -1,0 +1,491 @@
+// Persistent tile Cholesky and triangular solves (FP64, complex, lower, in place).
+//
+// One cooperative launch with one CTA per SM factors the whole matrix.  Tiles of
+// 64 x 64 are numbered column by column (diagonal tile first in each column) and
+// handed out in that order by an atomic counter; tile (i, j) computes
+//   F = A_ij - sum_{k<j} L_ik L_jk^H          (DMMA m8n8k4, operands staged by cp.async)
+//   i == j:  L_jj = chol(F) in shared memory, plus L_jj^{-1} and L_jj^{-H}
+//   i >  j:  L_ij = F L_jj^{-H}
+// and publishes a flag.  A tile waits only on tiles with smaller numbers (left
+// columns, or the diagonal of its own column), which were handed out earlier to
+// co-resident CTAs, so the schedule cannot deadlock.  Every wait is bounded: a
+// timeout sets DS_TIMEOUT and an abort word that makes every CTA stop.
+//
+// The solves use the same scheme with 64-row blocks: the forward sweep of block
+// row r accumulates L[r, k] x_k as each x_k is published, then applies
+// L_rr^{-1}; the backward sweep runs the block rows in reverse with L^H.
+#include <algorithm>
+#include <vector>
+
+#include "chol.hpp"
+#include "internal.hpp"
+
+namespace yq {
+
+namespace {
+constexpr int TB = 64;        // tile size
+constexpr int KC = 16;        // K chunk of the staged operands
+constexpr int SLS = 20;       // staged row stride (complex)
+constexpr int FLS = TB + 1;   // factor-tile row stride (complex)
+constexpr size_t SM_STAGE = size_t(4) * TB * SLS * sizeof(c128);   // 2 stages x {A, B}
+constexpr size_t SM_FACTOR = size_t(3) * TB * FLS * sizeof(c128);  // F, X, T
+constexpr size_t SM_TILE = SM_FACTOR > SM_STAGE ? SM_FACTOR : SM_STAGE;
+
+__device__ __forceinline__ void cpa16(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+struct Sync {
+    int* status;
+    int* abort_word;
+    unsigned cap;
+};
+
+// Thread 0 waits for *flag != 0 (bounded), then the CTA synchronises.  Returns
+// false when this or another CTA gave up.
+__device__ bool wait_flag(const int* flag, const Sync& S, int* s_ok) {
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned it = 0;
+        while (ld_acquire(flag) == 0) {
+            if (ld_acquire(S.abort_word) != 0 || ++it > S.cap) {
+                ok = 0;
+                break;
+            }
+            __nanosleep(64);
+        }
+        if (!ok && it > S.cap) {
+            atomicOr(S.status, DS_TIMEOUT);
+            atomicExch(S.abort_word, 1);
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// Publishes a flag after every thread's global writes of the tile.
+__device__ void publish(int* flag) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(flag, 1);
+}
+
+// c (4 x 4 sub-tiles of the warp's 32 x 32 block) += A B^H over K = 4 * nk,
+// A and B read from shared memory rows (row stride lda / ldb complex).
+__device__ __forceinline__ void warp_mma(const c128* A, int lda, const c128* B, int ldb, int nk, int wm, int wn, int fr,
+                                         int fk, double (&cre)[4][4][2], double (&cim)[4][4][2]) {
+    for (int ks = 0; ks < nk; ++ks) {
+        const int k = ks * 4 + fk;
+        double ar[4], ai[4], br[4], bi[4], bn[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const c128 v = A[(wm * 32 + i * 8 + fr) * lda + k];
+            ar[i] = v.re;
+            ai[i] = v.im;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const c128 v = B[(wn * 32 + j * 8 + fr) * ldb + k];
+            br[j] = v.re;
+            bi[j] = v.im;
+            bn[j] = -v.im;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                dmma(cre[i][j], ar[i], br[j]);
+                dmma(cre[i][j], ai[i], bi[j]);
+                dmma(cim[i][j], ai[i], br[j]);
+                dmma(cim[i][j], ar[i], bn[j]);
+            }
+    }
+}
+
+// Unblocked factorisation of the 64 x 64 tile F (lower part) in shared memory and
+// its inverse X = L^{-1} by the blocked recursion X21 = -X22 (L21 X11).
+__device__ bool factor_tile(c128* F, c128* X, c128* T, int* status) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    bool ok = true;
+    for (int e = tid; e < TB * TB; e += nt) {
+        const int r = e / TB, c = e % TB;
+        if (c > r) F[r * FLS + c] = mk(0., 0.);
+        X[r * FLS + c] = mk(0., 0.);
+    }
+    __syncthreads();
+    for (int c = 0; c < TB; ++c) {
+        if (tid == 0) {
+            double d = F[c * FLS + c].re;
+            if (!(d > 0.0)) {
+                atomicOr(status, DS_NOT_PD);
+                d = 1.0;
+            }
+            F[c * FLS + c] = mk(sqrt(d), 0.0);
+        }
+        __syncthreads();
+        const double inv = 1.0 / F[c * FLS + c].re;
+        for (int r = c + 1 + tid; r < TB; r += nt) F[r * FLS + c] = inv * F[r * FLS + c];
+        __syncthreads();
+        const int w = TB - c - 1;
+        const int tri = w * (w + 1) / 2;
+        for (int e = tid; e < tri; e += nt) {
+            int r = int((sqrtf(8.0f * float(e) + 1.0f) - 1.0f) * 0.5f);
+            while (r * (r + 1) / 2 > e) --r;
+            while ((r + 1) * (r + 2) / 2 <= e) ++r;
+            const int q = e - r * (r + 1) / 2;
+            const int rr = c + 1 + r, qq = c + 1 + q;
+            F[rr * FLS + qq] = F[rr * FLS + qq] - F[rr * FLS + c] * conj(F[qq * FLS + c]);
+        }
+        __syncthreads();
+    }
+    if (tid < TB) {
+        const int o = (tid >> 3) * 8, col = tid & 7;
+        for (int r = col; r < 8; ++r) {
+            c128 acc = mk(r == col ? 1.0 : 0.0, 0.0);
+            for (int q = col; q < r; ++q) acc = acc - F[(o + r) * FLS + o + q] * X[(o + q) * FLS + o + col];
+            X[(o + r) * FLS + o + col] = (1.0 / F[(o + r) * FLS + o + r].re) * acc;
+        }
+    }
+    __syncthreads();
+    for (int s = 8; s < TB; s *= 2) {
+        const int cnt = (TB / (2 * s)) * s * s;
+        for (int e = tid; e < cnt; e += nt) {
+            const int p = e / (s * s), i = (e / s) % s, j = e % s, o = 2 * s * p;
+            c128 acc = mk(0., 0.);
+            for (int q = j; q < s; ++q) acc = acc + F[(o + s + i) * FLS + o + q] * X[(o + q) * FLS + o + j];
+            T[(o + i) * FLS + o + j] = acc;
+        }
+        __syncthreads();
+        for (int e = tid; e < cnt; e += nt) {
+            const int p = e / (s * s), i = (e / s) % s, j = e % s, o = 2 * s * p;
+            c128 acc = mk(0., 0.);
+            for (int q = 0; q <= i; ++q) acc = acc + X[(o + s + i) * FLS + o + s + q] * T[(o + q) * FLS + o + j];
+            X[(o + s + i) * FLS + o + j] = mk(-acc.re, -acc.im);
+        }
+        __syncthreads();
+    }
+    return ok;
+}
+
+struct TileArgs {
+    c128* G;
+    size_t ld;
+    int nt;
+    c128* Linv;
+    c128* LinvH;
+    const int2* items;
+    int nitems;
+    int* counter;
+    int* flags;  // nt x nt
+    Sync S;
+};
+
+__global__ void __launch_bounds__(128, 1) chol_tile_kernel(TileArgs a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    typedef c128 Stage[TB][SLS];
+    Stage* As = reinterpret_cast<Stage*>(sm);
+    Stage* Bs = reinterpret_cast<Stage*>(sm + 2 * sizeof(Stage));
+    c128* F = reinterpret_cast<c128*>(sm);
+    c128* X = F + TB * FLS;
+    c128* T = X + TB * FLS;
+    __shared__ int s_item, s_ok;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int wm = warp >> 1, wn = warp & 1, fr = lane >> 2, fk = lane & 3;
+    for (;;) {
+        if (tid == 0) s_item = ld_acquire(a.S.abort_word) ? a.nitems : atomicAdd(a.counter, 1);
+        __syncthreads();
+        const int w = s_item;
+        __syncthreads();
+        if (w >= a.nitems) break;
+        const int i = a.items[w].x, j = a.items[w].y;
+        double cre[4][4][2], cim[4][4][2];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) cre[p][q][0] = cre[p][q][1] = cim[p][q][0] = cim[p][q][1] = 0.0;
+        // ---- F = A_ij - sum_k L_ik L_jk^H
+        const int nchunk = 4 * j;
+        bool ok = true;
+        auto load = [&](int buf, int c) {
+            const int kb = c >> 2, k0 = kb * TB + (c & 3) * KC;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int e = tid + 128 * q, row = e >> 4, kk = e & 15;
+                cpa16(&As[buf][row][kk], a.G + size_t(i * TB + row) * a.ld + k0 + kk);
+                cpa16(&Bs[buf][row][kk], a.G + size_t(j * TB + row) * a.ld + k0 + kk);
+            }
+            cpa_commit();
+        };
+        if (nchunk > 0) {
+            ok = wait_flag(&a.flags[i * a.nt + 0], a.S, &s_ok) && wait_flag(&a.flags[j * a.nt + 0], a.S, &s_ok);
+            if (ok) load(0, 0);
+        }
+        for (int c = 0; ok && c < nchunk; ++c) {
+            const int buf = c & 1;
+            if (c + 1 < nchunk) {
+                if (((c + 1) & 3) == 0) {
+                    const int kb = (c + 1) >> 2;
+                    ok = wait_flag(&a.flags[i * a.nt + kb], a.S, &s_ok) &&
+                         wait_flag(&a.flags[j * a.nt + kb], a.S, &s_ok);
+                    if (!ok) break;
+                }
+                load(buf ^ 1, c + 1);
+                cpa_wait_one();
+            } else {
+                cpa_wait_all();
+            }
+            __syncthreads();
+            warp_mma(&As[buf][0][0], SLS, &Bs[buf][0][0], SLS, KC / 4, wm, wn, fr, fk, cre, cim);
+            __syncthreads();
+        }
+        cpa_wait_all();
+        __syncthreads();
+        if (!ok) break;
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int r = wm * 32 + p * 8 + fr, c = wn * 32 + q * 8 + 2 * fk + h;
+                    const c128 g = a.G[size_t(i * TB + r) * a.ld + j * TB + c];
+                    F[r * FLS + c] = mk(g.re - cre[p][q][h], g.im - cim[p][q][h]);
+                }
+        __syncthreads();
+        if (i == j) {
+            factor_tile(F, X, T, a.S.status);
+            c128* Li = a.Linv + size_t(j) * TB * TB;
+            c128* LiH = a.LinvH + size_t(j) * TB * TB;
+            for (int e = tid; e < TB * TB; e += blockDim.x) {
+                const int r = e / TB, c = e % TB;
+                if (c <= r) a.G[size_t(j * TB + r) * a.ld + j * TB + c] = F[r * FLS + c];
+                Li[e] = X[r * FLS + c];
+                LiH[e] = conj(X[c * FLS + r]);
+            }
+            publish(&a.flags[j * a.nt + j]);
+        } else {
+            if (!wait_flag(&a.flags[j * a.nt + j], a.S, &s_ok)) break;
+            // X <- L_jj^{-1} (rows r, K-contiguous): L_ij = F (L_jj^{-1})^H
+            const c128* Li = a.Linv + size_t(j) * TB * TB;
+            for (int e = tid; e < TB * TB; e += blockDim.x) {
+                const int r = e / TB, c = e % TB;
+                cpa16(&X[r * FLS + c], Li + e);
+            }
+            cpa_commit();
+            cpa_wait_all();
+            __syncthreads();
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) cre[p][q][0] = cre[p][q][1] = cim[p][q][0] = cim[p][q][1] = 0.0;
+            warp_mma(F, FLS, X, FLS, TB / 4, wm, wn, fr, fk, cre, cim);
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int r = wm * 32 + p * 8 + fr, c = wn * 32 + q * 8 + 2 * fk + h;
+                        a.G[size_t(i * TB + r) * a.ld + j * TB + c] = mk(cre[p][q][h], cim[p][q][h]);
+                    }
+            publish(&a.flags[i * a.nt + j]);
+        }
+    }
+    cpa_wait_all();
+}
+
+// ---------------------------------------------------------------------------
+struct SolveArgs {
+    const c128* G;
+    size_t ld;
+    int nt;
+    const c128* Linv;
+    const c128* LinvH;
+    c128* b;    // in: right-hand side; forward result written here per block
+    int* flags; // nt
+    Sync S;
+};
+
+__device__ __forceinline__ c128 wsum(c128 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.re += __shfl_xor_sync(0xffffffffu, v.re, o);
+        v.im += __shfl_xor_sync(0xffffffffu, v.im, o);
+    }
+    return v;
+}
+
+// Forward: x_r = L_rr^{-1} (b_r - sum_{k<r} L_rk x_k), block rows in increasing order.
+__global__ void __launch_bounds__(128) chol_fwd_tile_kernel(SolveArgs a) {
+    __shared__ c128 acc[TB], xk[TB];
+    __shared__ int s_ok;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int r = blockIdx.x; r < a.nt; r += gridDim.x) {
+        if (tid < TB) acc[tid] = a.b[r * TB + tid];
+        __syncthreads();
+        bool ok = true;
+        for (int k = 0; k < r; ++k) {
+            if (!wait_flag(&a.flags[k], a.S, &s_ok)) {
+                ok = false;
+                break;
+            }
+            if (tid < TB) xk[tid] = a.b[k * TB + tid];
+            __syncthreads();
+            // 4 warps x 16 rows; lanes over the 64 columns
+            for (int q = 0; q < TB / 4; ++q) {
+                const int row = warp * (TB / 4) + q;
+                const c128* Lr = a.G + size_t(r * TB + row) * a.ld + k * TB;
+                c128 v = wsum(Lr[lane] * xk[lane] + Lr[lane + 32] * xk[lane + 32]);
+                if (lane == 0) acc[row] = acc[row] - v;
+            }
+            __syncthreads();
+        }
+        if (!ok) return;
+        const c128* Li = a.Linv + size_t(r) * TB * TB;
+        c128 out[TB / 4];
+        for (int q = 0; q < TB / 4; ++q) {
+            const int row = warp * (TB / 4) + q;
+            out[q] = wsum(Li[row * TB + lane] * acc[lane] + Li[row * TB + lane + 32] * acc[lane + 32]);
+        }
+        __syncthreads();
+        if (lane == 0)
+            for (int q = 0; q < TB / 4; ++q) a.b[r * TB + warp * (TB / 4) + q] = out[q];
+        publish(&a.flags[r]);
+    }
+}
+
+// Backward: z_r = L_rr^{-H} (x_r - sum_{k>r} L_kr^H z_k), block rows in decreasing order.
+__global__ void __launch_bounds__(128) chol_bwd_tile_kernel(SolveArgs a) {
+    __shared__ c128 acc[TB], zk[TB];
+    __shared__ c128 part[2][TB];
+    __shared__ int s_ok;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int t = blockIdx.x; t < a.nt; t += gridDim.x) {
+        const int r = a.nt - 1 - t;
+        if (tid < TB) acc[tid] = a.b[r * TB + tid];
+        __syncthreads();
+        bool ok = true;
+        for (int k = a.nt - 1; k > r; --k) {
+            if (!wait_flag(&a.flags[k], a.S, &s_ok)) {
+                ok = false;
+                break;
+            }
+            if (tid < TB) zk[tid] = a.b[k * TB + tid];
+            __syncthreads();
+            // acc[c] -= sum_row conj(L[k*64 + row][r*64 + c]) z_k[row]; thread (half, c)
+            const int c = tid & (TB - 1), half = tid >> 6;
+            c128 v = mk(0., 0.);
+            for (int row = half * 32; row < half * 32 + 32; ++row)
+                v = v + conj(a.G[size_t(k * TB + row) * a.ld + r * TB + c]) * zk[row];
+            part[half][c] = v;
+            __syncthreads();
+            if (tid < TB) acc[tid] = acc[tid] - part[0][tid] - part[1][tid];
+            __syncthreads();
+        }
+        if (!ok) return;
+        const c128* LiH = a.LinvH + size_t(r) * TB * TB;
+        c128 out[TB / 4];
+        for (int q = 0; q < TB / 4; ++q) {
+            const int row = warp * (TB / 4) + q;
+            out[q] = wsum(LiH[row * TB + lane] * acc[lane] + LiH[row * TB + lane + 32] * acc[lane + 32]);
+        }
+        __syncthreads();
+        if (lane == 0)
+            for (int q = 0; q < TB / 4; ++q) a.b[r * TB + warp * (TB / 4) + q] = out[q];
+        publish(&a.flags[r]);
+    }
+}
+
+int coresident_blocks(const void* fn, int threads, size_t smem, int sm_count) {
+    int per_sm = 0;
+    YQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+    if (per_sm < 1) throw Error(YQ_E_UNSUPPORTED, "persistent Cholesky: kernel does not fit on an SM");
+    return per_sm * sm_count;
+}
+}  // namespace
+
+// Scratch: [counter, abort, pad..., flags nt*nt, solve flags 2*nt], then the item list.
+size_t chol_tile_scratch_bytes(int n) {
+    const size_t nt = size_t(n) / TB;
+    return (16 + nt * nt + 2 * nt) * sizeof(int) + nt * (nt + 1) / 2 * sizeof(int2) + 256;
+}
+
+void chol_factor_tiled(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* status, void* scratch,
+                       int sm_count, cudaStream_t st) {
+    YQ_CHECK_ARG(n % TB == 0 && n > 0, "cholesky: dimension must be a positive multiple of 64");
+    const int nt = n / TB;
+    int* words = static_cast<int*>(scratch);
+    int* flags = words + 16;
+    int2* items = reinterpret_cast<int2*>((reinterpret_cast<uintptr_t>(flags + size_t(nt) * nt + 2 * nt) + 15) &
+                                          ~uintptr_t(15));
+    // column-major tile order, diagonal first
+    static thread_local std::vector<int2> host_items;
+    static thread_local int host_nt = -1;
+    const int nitems = nt * (nt + 1) / 2;
+    if (host_nt != nt) {
+        host_items.clear();
+        for (int j = 0; j < nt; ++j)
+            for (int i = j; i < nt; ++i) host_items.push_back(make_int2(i, j));
+        host_nt = nt;
+    }
+    YQ_CUDA(cudaMemsetAsync(words, 0, (16 + size_t(nt) * nt) * sizeof(int), st));
+    YQ_CUDA(cudaMemcpyAsync(items, host_items.data(), size_t(nitems) * sizeof(int2), cudaMemcpyHostToDevice, st));
+    static bool attr = false;
+    if (!attr) {
+        YQ_CUDA(cudaFuncSetAttribute(chol_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SM_TILE)));
+        attr = true;
+    }
+    TileArgs a{G, ld, nt, Linv, LinvH, items, nitems, words + 0, flags, Sync{status, words + 1, 1u << 24}};
+    const int grid = std::min(coresident_blocks(reinterpret_cast<const void*>(chol_tile_kernel), 128, SM_TILE, sm_count),
+                              std::max(1, nitems));
+    void* args[] = {&a};
+    YQ_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(chol_tile_kernel), dim3(grid), dim3(128), args,
+                                        SM_TILE, st));
+    YQ_LAUNCH_CHECK();
+}
+
+void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c128* LinvH, c128* b, c128* out,
+                      int* status, void* scratch, int sm_count, cudaStream_t st) {
+    const int nt = n / TB;
+    int* words = static_cast<int*>(scratch);
+    int* sflags = words + 16 + size_t(nt) * nt;
+    YQ_CUDA(cudaMemsetAsync(sflags, 0, 2 * size_t(nt) * sizeof(int), st));
+    YQ_CUDA(cudaMemsetAsync(words + 2, 0, sizeof(int), st));  // abort word of the solves
+    const int grid_f = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_fwd_tile_kernel), 128, 0,
+                                                      sm_count));
+    const int grid_b = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_bwd_tile_kernel), 128, 0,
+                                                      sm_count));
+    SolveArgs fa{G, ld, nt, Linv, LinvH, b, sflags, Sync{status, words + 2, 1u << 24}};
+    void* fargs[] = {&fa};
+    YQ_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(chol_fwd_tile_kernel), dim3(grid_f), dim3(128),
+                                        fargs, 0, st));
+    YQ_LAUNCH_CHECK();
+    SolveArgs ba{G, ld, nt, Linv, LinvH, b, sflags + nt, Sync{status, words + 2, 1u << 24}};
+    void* bargs[] = {&ba};
+    YQ_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(chol_bwd_tile_kernel), dim3(grid_b), dim3(128),
+                                        bargs, 0, st));
+    YQ_LAUNCH_CHECK();
+    if (out != b) YQ_CUDA(cudaMemcpyAsync(out, b, size_t(n) * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+}
+
+}  // namespace yq

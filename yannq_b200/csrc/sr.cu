@@ -523,12 +523,31 @@ static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps) {
     form_matrix_t<R>(sr, shift);
     ctx->stage_end(ST_GRAM);
     ctx->stage_begin(ST_SOLVE);
-    chol_factor(sr->G.as<c128>(), sr->dim_pad, size_t(sr->dim_pad), sr->Linv.as<c128>(), sr->LinvH.as<c128>(),
-                sr->q->ctx->status.as<int>(), st);
+    // Persistent tile Cholesky by default; YQ_CHOLESKY=recursive selects the
+    // recursive launch-per-step variant (kept for comparison).
+    static const bool recursive = [] {
+        const char* e = std::getenv("YQ_CHOLESKY");
+        return e && std::string(e) == "recursive";
+    }();
+    sr->chol_work.ensure(chol_tile_scratch_bytes(sr->dim_pad));
+    if (recursive)
+        chol_factor(sr->G.as<c128>(), sr->dim_pad, size_t(sr->dim_pad), sr->Linv.as<c128>(), sr->LinvH.as<c128>(),
+                    ctx->status.as<int>(), st);
+    else
+        chol_factor_tiled(sr->G.as<c128>(), sr->dim_pad, size_t(sr->dim_pad), sr->Linv.as<c128>(),
+                          sr->LinvH.as<c128>(), ctx->status.as<int>(), sr->chol_work.p, ctx->sm_count, st);
     const size_t dp = size_t(sr->dim_pad);
     const c128* G = sr->G.as<c128>();
     const c128* Li = sr->Linv.as<c128>();
     const c128* LiH = sr->LinvH.as<c128>();
+    auto chol_solve = [&](const c128* G_, int n_, size_t ld_, const c128* Li_, const c128* LiH_, c128* b_, c128* tmp_,
+                          c128* out_, cudaStream_t st_) {
+        if (recursive)
+            yq::chol_solve(G_, n_, ld_, Li_, LiH_, b_, tmp_, out_, st_);
+        else
+            chol_solve_tiled(G_, n_, ld_, Li_, LiH_, b_, out_, ctx->status.as<int>(), sr->chol_work.p, ctx->sm_count,
+                             st_);
+    };
     if (sr->mode == YQ_SR_T) {
         // y = (T + shift)^{-1} (E - <E>) / Ns ; v = O~^H y   (push-through identity)
         c128* b = sr->rhs.as<c128>();
