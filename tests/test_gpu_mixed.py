@@ -102,3 +102,20 @@ def test_mixed_full_size_properties(ctx, orc):
     assert np.all(np.isfinite(vm))
     assert abs(em - ef) / abs(ef) < 1e-5
     assert np.linalg.norm(vm - vf) / np.linalg.norm(vf) < 1e-3
+
+
+@pytest.mark.parametrize("chains,sweeps", [(100, 12), (64, 9)])
+def test_mixed_panel_cholesky_matches_fp64(ctx, orc, chains, sweeps):
+    """T larger than one 512-wide Cholesky panel: the tensor-core trailing updates
+    (ragged 704- and 192-row trailing blocks for Ns = 1200, identity padding up to
+    a multiple of 64) followed by refinement reproduce the FP64 oracle solve."""
+    from yannq_b200 import api
+
+    n, m = 36, 72
+    p, s, th, q, H, S, sr = _case(api, ctx, orc, n, m, chains, sweeps, seed=11, sd=0.05)
+    ref = orc.sr_step(orc.Ham.tfi(n, -1.0, -1.0), m, p, s, th, 1e-3, orc.SR_T, orc.SOLVE_LLT)
+    v, _, _ = sr.solve(1e-3, api.SOLVE_LLT)
+    err = np.max(np.abs(v - ref["v"])) / np.max(np.abs(ref["v"]))
+    assert err < TOL_V, err
+    for x in (sr, S, H, q):
+        x.close()

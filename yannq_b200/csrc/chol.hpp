@@ -24,6 +24,15 @@ void chol_solve(const c128* G, int n, size_t ld, const c128* Linv, const c128* L
 size_t chol_tile_scratch_bytes(int n);
 void chol_factor_tiled(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* status, void* scratch,
                        int sm_count, cudaStream_t st);
+// Panel form for matrices whose accuracy is that of the BF16x3 products: the
+// persistent FP64 tile kernel factors each CHOL_PANEL-wide block column (tiles
+// updated only by the columns of their own panel), and the trailing matrix is
+// updated once per panel on the tensor cores (C -= L21 L21^H, BF16x3, FP32
+// accumulation).  `planes` holds chol_panel_planes_bytes(n) bytes of split operands.
+constexpr int CHOL_PANEL = 512;
+size_t chol_panel_planes_bytes(int n);
+void chol_factor_panels(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* status, void* scratch,
+                        void* planes, int sm_count, cudaStream_t st);
 // out = (L L^H)^{-1} b; b is overwritten with the solution as well.
 void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c128* LinvH, c128* b, c128* out,
                       int* status, void* scratch, int sm_count, cudaStream_t st);

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "chol.hpp"
+#include "gram_tc.hpp"
 #include "internal.hpp"
 
 namespace yq {
@@ -122,75 +123,99 @@ __device__ __forceinline__ void warp_mma(const c128* A, int lda, const c128* B, 
     }
 }
 
-// Unblocked factorisation of the 64 x 64 tile F (lower part) in shared memory and
-// its inverse X = L^{-1} by the blocked recursion X21 = -X22 (L21 X11).
-__device__ bool factor_tile(c128* F, c128* X, c128* T, int* status) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    bool ok = true;
-    for (int e = tid; e < TB * TB; e += nt) {
+// Factorisation of the 64 x 64 tile F (lower part) in shared memory and its
+// inverse X = L^{-1}, fused into one right-looking sweep with one barrier per
+// step.  The 128 threads form a 16 x 8 grid; thread (tr, tq) owns the elements
+// (tr + 16 a, tq + 8 b), a < 4, b < 8, of F and of X, so every step gives each
+// thread up to 32 independent updates.  Step c, with d = F_cc:
+//   L[:, c] = F[:, c] / sqrt(d)                      (written to T)
+//   F_rq -= F_rc conj(F_qc) / d       for c < q <= r (trailing Schur complement)
+//   R_rq -= F_rc R_cq / d             for q <= c < r (row elimination of R = I)
+// and row c of R becomes row c of X = L^{-1} after scaling by 1 / sqrt(d), which
+// is done one step later (step c reads R_c*, nothing reads it afterwards).  Every
+// write goes to an element that no thread reads in the same step.  On exit F
+// holds L (upper part zero).  Needs blockDim.x == 128.
+__device__ void factor_tile(c128* F, c128* X, c128* T, int* status) {
+    const int tid = threadIdx.x;
+    const int tr = tid & 15, tq = tid >> 4;
+    for (int e = tid; e < TB * TB; e += 128) {
         const int r = e / TB, c = e % TB;
-        if (c > r) F[r * FLS + c] = mk(0., 0.);
-        X[r * FLS + c] = mk(0., 0.);
+        X[r * FLS + c] = mk(r == c ? 1.0 : 0.0, 0.0);
+        T[r * FLS + c] = mk(0., 0.);
     }
     __syncthreads();
+    double is_prev = 1.0;
     for (int c = 0; c < TB; ++c) {
-        if (tid == 0) {
-            double d = F[c * FLS + c].re;
-            if (!(d > 0.0)) {
-                atomicOr(status, DS_NOT_PD);
-                d = 1.0;
+        double d = F[c * FLS + c].re;
+        if (!(d > 0.0)) {
+            if (tid == 0) atomicOr(status, DS_NOT_PD);
+            d = 1.0;  // unit pivot keeps the launch well defined
+        }
+        const double is = rsqrt(d), id = is * is;
+        c128 fc[4], fq[8], xq[8];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) fc[a] = F[(tr + 16 * a) * FLS + c];
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const int q = tq + 8 * b;
+            fq[b] = F[q * FLS + c];
+            xq[b] = X[c * FLS + q];
+        }
+        if (tq == (c & 7)) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int r = tr + 16 * a;
+                if (r == c) T[r * FLS + c] = mk(d * is, 0.0);
+                else if (r > c) T[r * FLS + c] = is * fc[a];
             }
-            F[c * FLS + c] = mk(sqrt(d), 0.0);
         }
-        __syncthreads();
-        const double inv = 1.0 / F[c * FLS + c].re;
-        for (int r = c + 1 + tid; r < TB; r += nt) F[r * FLS + c] = inv * F[r * FLS + c];
-        __syncthreads();
-        const int w = TB - c - 1;
-        const int tri = w * (w + 1) / 2;
-        for (int e = tid; e < tri; e += nt) {
-            int r = int((sqrtf(8.0f * float(e) + 1.0f) - 1.0f) * 0.5f);
-            while (r * (r + 1) / 2 > e) --r;
-            while ((r + 1) * (r + 2) / 2 <= e) ++r;
-            const int q = e - r * (r + 1) / 2;
-            const int rr = c + 1 + r, qq = c + 1 + q;
-            F[rr * FLS + qq] = F[rr * FLS + qq] - F[rr * FLS + c] * conj(F[qq * FLS + c]);
+        if (c > 0 && tr == ((c - 1) & 15)) {
+            const int r = c - 1;  // = tr + 16 ((c - 1) >> 4)
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                const int q = tq + 8 * b;
+                if (q <= r) X[r * FLS + q] = is_prev * X[r * FLS + q];
+            }
         }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int r = tr + 16 * a;
+            if (r > c) {
+                const c128 g = id * fc[a];
+#pragma unroll
+                for (int b = 0; b < 8; ++b) {
+                    const int q = tq + 8 * b;
+                    if (q > c) {
+                        if (q <= r) F[r * FLS + q] = F[r * FLS + q] - g * conj(fq[b]);
+                    } else {
+                        X[r * FLS + q] = X[r * FLS + q] - g * xq[b];
+                    }
+                }
+            }
+        }
+        is_prev = is;
         __syncthreads();
     }
-    if (tid < TB) {
-        const int o = (tid >> 3) * 8, col = tid & 7;
-        for (int r = col; r < 8; ++r) {
-            c128 acc = mk(r == col ? 1.0 : 0.0, 0.0);
-            for (int q = col; q < r; ++q) acc = acc - F[(o + r) * FLS + o + q] * X[(o + q) * FLS + o + col];
-            X[(o + r) * FLS + o + col] = (1.0 / F[(o + r) * FLS + o + r].re) * acc;
+    if (tr == ((TB - 1) & 15)) {
+        const int r = TB - 1;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const int q = tq + 8 * b;
+            X[r * FLS + q] = is_prev * X[r * FLS + q];
         }
+    }
+    for (int e = tid; e < TB * TB; e += 128) {
+        const int r = e / TB, c = e % TB;
+        F[r * FLS + c] = T[r * FLS + c];
     }
     __syncthreads();
-    for (int s = 8; s < TB; s *= 2) {
-        const int cnt = (TB / (2 * s)) * s * s;
-        for (int e = tid; e < cnt; e += nt) {
-            const int p = e / (s * s), i = (e / s) % s, j = e % s, o = 2 * s * p;
-            c128 acc = mk(0., 0.);
-            for (int q = j; q < s; ++q) acc = acc + F[(o + s + i) * FLS + o + q] * X[(o + q) * FLS + o + j];
-            T[(o + i) * FLS + o + j] = acc;
-        }
-        __syncthreads();
-        for (int e = tid; e < cnt; e += nt) {
-            const int p = e / (s * s), i = (e / s) % s, j = e % s, o = 2 * s * p;
-            c128 acc = mk(0., 0.);
-            for (int q = 0; q <= i; ++q) acc = acc + X[(o + s + i) * FLS + o + s + q] * T[(o + q) * FLS + o + j];
-            X[(o + s + i) * FLS + o + j] = mk(-acc.re, -acc.im);
-        }
-        __syncthreads();
-    }
-    return ok;
 }
 
 struct TileArgs {
     c128* G;
     size_t ld;
     int nt;
+    int kbeg;  // first tile column that contributes to the updates (0: the whole factorisation)
     c128* Linv;
     c128* LinvH;
     const int2* items;
@@ -224,10 +249,10 @@ __global__ void __launch_bounds__(128, 1) chol_tile_kernel(TileArgs a) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) cre[p][q][0] = cre[p][q][1] = cim[p][q][0] = cim[p][q][1] = 0.0;
         // ---- F = A_ij - sum_k L_ik L_jk^H
-        const int nchunk = 4 * j;
+        const int nchunk = 4 * (j - a.kbeg);
         bool ok = true;
         auto load = [&](int buf, int c) {
-            const int kb = c >> 2, k0 = kb * TB + (c & 3) * KC;
+            const int kb = a.kbeg + (c >> 2), k0 = kb * TB + (c & 3) * KC;
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
                 const int e = tid + 128 * q, row = e >> 4, kk = e & 15;
@@ -237,14 +262,15 @@ __global__ void __launch_bounds__(128, 1) chol_tile_kernel(TileArgs a) {
             cpa_commit();
         };
         if (nchunk > 0) {
-            ok = wait_flag(&a.flags[i * a.nt + 0], a.S, &s_ok) && wait_flag(&a.flags[j * a.nt + 0], a.S, &s_ok);
+            ok = wait_flag(&a.flags[i * a.nt + a.kbeg], a.S, &s_ok) &&
+                 wait_flag(&a.flags[j * a.nt + a.kbeg], a.S, &s_ok);
             if (ok) load(0, 0);
         }
         for (int c = 0; ok && c < nchunk; ++c) {
             const int buf = c & 1;
             if (c + 1 < nchunk) {
                 if (((c + 1) & 3) == 0) {
-                    const int kb = (c + 1) >> 2;
+                    const int kb = a.kbeg + ((c + 1) >> 2);
                     ok = wait_flag(&a.flags[i * a.nt + kb], a.S, &s_ok) &&
                          wait_flag(&a.flags[j * a.nt + kb], a.S, &s_ok);
                     if (!ok) break;
@@ -424,51 +450,112 @@ int coresident_blocks(const void* fn, int threads, size_t smem, int sm_count) {
 }
 }  // namespace
 
-// Scratch: [counter, abort, pad..., flags nt*nt, solve flags 2*nt], then the item list.
+// Scratch layout (ints): [0] tile counter of the full factorisation, [1] abort word
+// of the factorisation, [2] abort word of the solves, [16 .. 16 + nt) tile counters
+// of the panels, then the tile flags (nt x nt), the solve flags (2 nt), and the
+// 16-byte aligned tile list.
+struct Scratch {
+    int* words;
+    int* panel_counters;
+    int* flags;
+    int* sflags;
+    int2* items;
+    Scratch(void* p, int nt) {
+        words = static_cast<int*>(p);
+        panel_counters = words + 16;
+        flags = panel_counters + nt;
+        sflags = flags + size_t(nt) * nt;
+        items = reinterpret_cast<int2*>((reinterpret_cast<uintptr_t>(sflags + 2 * size_t(nt)) + 15) & ~uintptr_t(15));
+    }
+};
+
 size_t chol_tile_scratch_bytes(int n) {
     const size_t nt = size_t(n) / TB;
-    return (16 + nt * nt + 2 * nt) * sizeof(int) + nt * (nt + 1) / 2 * sizeof(int2) + 256;
+    return (16 + nt + nt * nt + 2 * nt) * sizeof(int) + nt * (nt + 1) / 2 * sizeof(int2) + 256;
+}
+
+// Column-major tile order, diagonal first: column j starts at j nt - j (j - 1) / 2.
+__global__ void tile_items_kernel(int nt, int2* items) {
+    const int j = blockIdx.x;
+    const size_t off = size_t(j) * nt - size_t(j) * (j - 1) / 2;
+    for (int i = j + threadIdx.x; i < nt; i += blockDim.x) items[off + (i - j)] = make_int2(i, j);
+}
+static void write_items(const Scratch& sc, int nt, cudaStream_t st) {
+    tile_items_kernel<<<nt, 128, 0, st>>>(nt, sc.items);
+    YQ_LAUNCH_CHECK();
+}
+
+static int tile_grid() {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        YQ_CUDA(cudaFuncSetAttribute(chol_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SM_TILE)));
+        YQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chol_tile_kernel, 128, SM_TILE));
+        if (per_sm < 1) throw Error(YQ_E_UNSUPPORTED, "persistent Cholesky: kernel does not fit on an SM");
+    }
+    return per_sm;
+}
+
+static void launch_tiles(const TileArgs& a, int nitems, int sm_count, cudaStream_t st) {
+    const int grid = std::min(tile_grid() * sm_count, std::max(1, nitems));
+    TileArgs copy = a;
+    void* args[] = {&copy};
+    YQ_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(chol_tile_kernel), dim3(grid), dim3(128), args,
+                                        SM_TILE, st));
+    YQ_LAUNCH_CHECK();
 }
 
 void chol_factor_tiled(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* status, void* scratch,
                        int sm_count, cudaStream_t st) {
     YQ_CHECK_ARG(n % TB == 0 && n > 0, "cholesky: dimension must be a positive multiple of 64");
     const int nt = n / TB;
-    int* words = static_cast<int*>(scratch);
-    int* flags = words + 16;
-    int2* items = reinterpret_cast<int2*>((reinterpret_cast<uintptr_t>(flags + size_t(nt) * nt + 2 * nt) + 15) &
-                                          ~uintptr_t(15));
-    // column-major tile order, diagonal first
-    static thread_local std::vector<int2> host_items;
-    static thread_local int host_nt = -1;
+    Scratch sc(scratch, nt);
+    write_items(sc, nt, st);
+    YQ_CUDA(cudaMemsetAsync(sc.words, 0, reinterpret_cast<char*>(sc.sflags) - reinterpret_cast<char*>(sc.words), st));
     const int nitems = nt * (nt + 1) / 2;
-    if (host_nt != nt) {
-        host_items.clear();
-        for (int j = 0; j < nt; ++j)
-            for (int i = j; i < nt; ++i) host_items.push_back(make_int2(i, j));
-        host_nt = nt;
+    TileArgs a{G, ld, nt, 0, Linv, LinvH, sc.items, nitems, sc.words + 0, sc.flags, Sync{status, sc.words + 1, 1u << 24}};
+    launch_tiles(a, nitems, sm_count, st);
+}
+
+size_t chol_panel_planes_bytes(int n) {
+    const size_t rows = ((size_t(n) + TC_BM - 1) / TC_BM) * TC_BM;
+    return 4 * rows * size_t(2 * CHOL_PANEL) * sizeof(uint16_t);
+}
+
+void chol_factor_panels(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* status, void* scratch,
+                        void* planes, int sm_count, cudaStream_t st) {
+    YQ_CHECK_ARG(n % TB == 0 && n > 0, "cholesky: dimension must be a positive multiple of 64");
+    const int nt = n / TB, pw = CHOL_PANEL / TB;
+    Scratch sc(scratch, nt);
+    write_items(sc, nt, st);
+    YQ_CUDA(cudaMemsetAsync(sc.words, 0, reinterpret_cast<char*>(sc.sflags) - reinterpret_cast<char*>(sc.words), st));
+    const size_t plane_elems = chol_panel_planes_bytes(n) / (4 * sizeof(uint16_t));
+    uint16_t* xh = static_cast<uint16_t*>(planes);
+    uint16_t *xl = xh + plane_elems, *yh = xl + plane_elems, *yl = yh + plane_elems;
+    int first = 0;  // index of the panel's first tile in the column-major list
+    for (int j0 = 0, p = 0; j0 < nt; j0 += pw, ++p) {
+        const int j1 = std::min(nt, j0 + pw);
+        int count = 0;
+        for (int j = j0; j < j1; ++j) count += nt - j;
+        TileArgs a{G, ld, nt, j0, Linv, LinvH, sc.items + first, count, sc.panel_counters + p, sc.flags,
+                   Sync{status, sc.words + 1, 1u << 24}};
+        launch_tiles(a, count, sm_count, st);
+        first += count;
+        if (j1 == nt) break;
+        // trailing update  G[r0:, r0:] -= L21 L21^H  on the tensor cores
+        const int r0 = j1 * TB, n2 = n - r0, w = (j1 - j0) * TB;
+        const size_t rows_pad = ((size_t(n2) + TC_BM - 1) / TC_BM) * TC_BM;
+        herk_tc_split_block(G, ld, r0, j0 * TB, n2, w, rows_pad, xh, xl, yh, yl, st);
+        herk_tc_run(xh, xl, yh, yl, n2, rows_pad, size_t(2 * w), G + size_t(r0) * ld + r0, ld, -1.0, 0.0, true, status,
+                    st);
     }
-    YQ_CUDA(cudaMemsetAsync(words, 0, (16 + size_t(nt) * nt) * sizeof(int), st));
-    YQ_CUDA(cudaMemcpyAsync(items, host_items.data(), size_t(nitems) * sizeof(int2), cudaMemcpyHostToDevice, st));
-    static bool attr = false;
-    if (!attr) {
-        YQ_CUDA(cudaFuncSetAttribute(chol_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SM_TILE)));
-        attr = true;
-    }
-    TileArgs a{G, ld, nt, Linv, LinvH, items, nitems, words + 0, flags, Sync{status, words + 1, 1u << 24}};
-    const int grid = std::min(coresident_blocks(reinterpret_cast<const void*>(chol_tile_kernel), 128, SM_TILE, sm_count),
-                              std::max(1, nitems));
-    void* args[] = {&a};
-    YQ_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(chol_tile_kernel), dim3(grid), dim3(128), args,
-                                        SM_TILE, st));
-    YQ_LAUNCH_CHECK();
 }
 
 void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c128* LinvH, c128* b, c128* out,
                       int* status, void* scratch, int sm_count, cudaStream_t st) {
     const int nt = n / TB;
-    int* words = static_cast<int*>(scratch);
-    int* sflags = words + 16 + size_t(nt) * nt;
+    Scratch sc(scratch, nt);
+    int* words = sc.words;
+    int* sflags = sc.sflags;
     YQ_CUDA(cudaMemsetAsync(sflags, 0, 2 * size_t(nt) * sizeof(int), st));
     YQ_CUDA(cudaMemsetAsync(words + 2, 0, sizeof(int), st));  // abort word of the solves
     const int grid_f = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_fwd_tile_kernel), 128, 0,

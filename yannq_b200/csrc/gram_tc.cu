@@ -1,13 +1,16 @@
-// tcgen05 Gram kernel of the mixed-precision SR path (see gram_tc.hpp).
+// tcgen05 Hermitian rank-k kernel of the mixed-precision SR path (see gram_tc.hpp).
 //
-// One CTA per 128 x 256 output tile of the lower triangle of T (T_re tiles read
-// A rows from X, T_im tiles from Y; B rows always from X).  Warp roles:
-//   warp 0       TMA producer: 4-stage ring of {A 128x64, B 256x64} BF16 tiles,
-//                128-byte swizzle, completion counted on "full" mbarriers;
-//   warp 1       TMEM allocator and single-thread MMA issuer: 4 x
+// One CTA per 128 x 256 complex output tile of the lower triangle.  Both parts
+// of the tile are accumulated by the same CTA: TMEM columns 0..255 hold Re = X X^T
+// and columns 256..511 hold Im = Y X^T, so each staged B tile feeds two MMAs and
+// the epilogue writes whole complex numbers.  Warp roles:
+//   warp 0       TMA producer: 3-stage ring of {X 128x64, Y 128x64, B 256x64} BF16
+//                tiles, 128-byte swizzle, completion counted on "full" mbarriers;
+//   warp 1       TMEM allocator and single-thread MMA issuer: 2 x 4
 //                tcgen05.mma.cta_group::1.kind::f16 (M128 N256 K16) per stage,
 //                tcgen05.commit releases the stage ("empty") and finally "done";
-//   warps 2..5   epilogue: tcgen05.ld 32x32b.x32 from TMEM, scale, FP64 store.
+//   warps 2..5   epilogue: tcgen05.ld 32x32b.x32 from TMEM, scale, FP64 store
+//                (or read-add-store for the trailing updates of the Cholesky).
 // K runs over three segments (hi.hi, hi.lo, lo.hi) of the split operands.
 // Every mbarrier wait is bounded: on timeout the kernel sets DS_TIMEOUT in the
 // status word, the other roles stop at their next wait, and TMEM is released.
@@ -70,23 +73,59 @@ void gram_tc_prepare_operands(const c64* O, int ns, size_t P, uint16_t* xh, uint
     YQ_LAUNCH_CHECK();
 }
 
+// Block split of a complex FP64 panel (the L21 of the Cholesky), K = 2 w.
+__global__ void split_block_kernel(const c128* __restrict__ G, size_t ld, int r0, int c0, int n, int w,
+                                   size_t rows_pad, uint16_t* __restrict__ xh, uint16_t* __restrict__ xl,
+                                   uint16_t* __restrict__ yh, uint16_t* __restrict__ yl) {
+    const size_t kp = size_t(2 * w);
+    const size_t total = rows_pad * kp;
+    for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < total; q += size_t(gridDim.x) * blockDim.x) {
+        const size_t row = q / kp;
+        const int k = int(q - row * kp);
+        float xv = 0.f, yv = 0.f;
+        if (row < size_t(n)) {
+            const int c = k < w ? k : k - w;
+            const c128 v = G[(size_t(r0) + row) * ld + size_t(c0) + c];
+            xv = float(k < w ? v.re : v.im);
+            yv = float(k < w ? v.im : -v.re);
+        }
+        uint16_t a, b;
+        split_bf16(xv, a, b);
+        xh[q] = a;
+        xl[q] = b;
+        split_bf16(yv, a, b);
+        yh[q] = a;
+        yl[q] = b;
+    }
+}
+
+void herk_tc_split_block(const c128* G, size_t ld, int r0, int c0, int n, int w, size_t rows_pad, uint16_t* xh,
+                         uint16_t* xl, uint16_t* yh, uint16_t* yl, cudaStream_t st) {
+    YQ_CHECK_ARG(w > 0 && w % 32 == 0 && rows_pad % TC_BM == 0 && size_t(n) <= rows_pad, "herk split: block shape");
+    const size_t total = rows_pad * size_t(2 * w);
+    split_block_kernel<<<std::max(1u, std::min(148u * 16, cdiv_u(total, 256))), 256, 0, st>>>(G, ld, r0, c0, n, w,
+                                                                                              rows_pad, xh, xl, yh, yl);
+    YQ_LAUNCH_CHECK();
+}
+
 // ---------------------------------------------------------------------------
-constexpr int TC_STAGES = 4;
-constexpr int TC_BNW = 256;                        // output columns per tile
-constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;      // 16 KiB
-constexpr int TC_B_BYTES = TC_BNW * TC_BK * 2;     // 32 KiB
-constexpr int TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;
-constexpr int TC_TMEM_COLS = 256;
+constexpr int TC_STAGES = 3;
+constexpr int TC_BNW = 256;                                   // output columns per tile
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;                 // 16 KiB (X or Y rows)
+constexpr int TC_B_BYTES = TC_BNW * TC_BK * 2;                // 32 KiB
+constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + TC_B_BYTES;   // 64 KiB
+constexpr int TC_TMEM_COLS = 512;                             // Re: 0..255, Im: 256..511
 constexpr int TC_THREADS = 192;
 constexpr size_t TC_SMEM = size_t(TC_STAGES) * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 
 struct TcParams {
-    int ns, nt;            // samples, 128-row tiles per half
-    int tiles_per_half;
+    int n;                 // output rows (= columns) that are written
+    int nt;                // 128-row tiles
     int kb_per_seg;        // kpad / 64
-    c128* G;
-    size_t ldg;
+    c128* C;
+    size_t ldc;
     double alpha, shift;
+    int accumulate;
     int* status;
     unsigned wait_cap;
 };
@@ -168,9 +207,9 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
         : "r"(taddr))
 
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    gram_tc_kernel(const __grid_constant__ CUtensorMap mXhA, const __grid_constant__ CUtensorMap mXlA,
-                   const __grid_constant__ CUtensorMap mYhA, const __grid_constant__ CUtensorMap mYlA,
-                   const __grid_constant__ CUtensorMap mXhB, const __grid_constant__ CUtensorMap mXlB, TcParams p) {
+    herk_tc_kernel(const __grid_constant__ CUtensorMap mXh, const __grid_constant__ CUtensorMap mXl,
+                   const __grid_constant__ CUtensorMap mYh, const __grid_constant__ CUtensorMap mYl,
+                   const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, TcParams p) {
     extern __shared__ uint8_t smem_raw[];
     // 1024-byte aligned stage buffers, barriers after them
     const uint32_t raw = smem_u32(smem_raw);
@@ -185,16 +224,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    // tile of this CTA
+    // tile of this CTA: 128-row block bi, 256-column block bj <= bi / 2
     int t = blockIdx.x;
-    const int half = t >= p.tiles_per_half ? 1 : 0;
-    if (half) t -= p.tiles_per_half;
     int bi = 0;
     while (bi < p.nt && t >= (bi >> 1) + 1) {
         t -= (bi >> 1) + 1;
         ++bi;
     }
-    const int bj = t;  // 256-column tile, bj <= bi / 2
+    const int bj = t;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; ++s) {
@@ -229,11 +266,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 mbar_expect_tx(fb, TC_STAGE_BYTES);
                 const int seg = kb / p.kb_per_seg;
                 const int kx = (kb - seg * p.kb_per_seg) * TC_BK;
-                const CUtensorMap* ma = half ? (seg == 2 ? &mYlA : &mYhA) : (seg == 2 ? &mXlA : &mXhA);
-                const CUtensorMap* mb = (seg == 1) ? &mXlB : &mXhB;
-                const uint32_t sa = smem_u32(gbase + size_t(stage) * TC_STAGE_BYTES);
-                tma_load_2d(sa, ma, kx, bi * TC_BM, fb);
-                tma_load_2d(sa + TC_A_BYTES, mb, kx, bj * TC_BNW, fb);
+                const uint32_t sx = smem_u32(gbase + size_t(stage) * TC_STAGE_BYTES);
+                tma_load_2d(sx, seg == 2 ? &mXl : &mXh, kx, bi * TC_BM, fb);
+                tma_load_2d(sx + TC_A_BYTES, seg == 2 ? &mYl : &mYh, kx, bi * TC_BM, fb);
+                tma_load_2d(sx + 2 * TC_A_BYTES, seg == 1 ? &mBl : &mBh, kx, bj * TC_BNW, fb);
             }
         }
     } else if (warp == 1) {
@@ -242,39 +278,89 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const int stage = kb % TC_STAGES, round = kb / TC_STAGES;
                 if (!mbar_wait(smem_u32(&full[stage]), uint32_t(round & 1), abort_flag, p.wait_cap, p.status)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t sa = smem_u32(gbase + size_t(stage) * TC_STAGE_BYTES);
-                const uint32_t sb = sa + TC_A_BYTES;
+                const uint32_t sx = smem_u32(gbase + size_t(stage) * TC_STAGE_BYTES);
+                const uint32_t sy = sx + TC_A_BYTES, sb = sx + 2 * TC_A_BYTES;
 #pragma unroll
-                for (int k = 0; k < TC_BK / 16; ++k)
-                    umma_bf16(tmem, sw128_desc(sa + k * 32), sw128_desc(sb + k * 32), (kb | k) != 0 ? 1u : 0u);
+                for (int k = 0; k < TC_BK / 16; ++k) {
+                    const uint32_t acc = (kb | k) != 0 ? 1u : 0u;
+                    const uint64_t db = sw128_desc(sb + k * 32);
+                    umma_bf16(tmem, sw128_desc(sx + k * 32), db, acc);
+                    umma_bf16(tmem + TC_BNW, sw128_desc(sy + k * 32), db, acc);
+                }
                 umma_commit(smem_u32(&empty[stage]));
             }
             umma_commit(smem_u32(done));  // tracks every MMA issued above
         }
         __syncwarp();
     } else {
-        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows rbase .. rbase + 31).
+        // Each 32 x 32 chunk is transposed through shared memory (the stage ring is
+        // idle once "done" has fired) so that a warp reads and writes 512 contiguous
+        // bytes of one row per instruction.
+        const int lg = warp & 3;
+        const int rbase = bi * TC_BM + lg * 32;
+        const int cbase = bj * TC_BNW;
+        if (p.accumulate) {
+            // bring this warp's rows of C into L2 while the main loop runs: one
+            // 128-byte line per lane, a row segment (256 x 16 B) per instruction
+            for (int rr = 0; rr < 32; ++rr) {
+                const int r = rbase + rr;
+                if (r < p.n && cbase + 8 * lane <= r)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(p.C + size_t(r) * p.ldc + cbase + 8 * lane));
+            }
+        }
         const bool ok = mbar_wait(smem_u32(done), 0u, abort_flag, p.wait_cap, p.status);
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int lg = warp & 3;
-        const int r = bi * TC_BM + lg * 32 + lane;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // stage ring reused by generic stores
+        constexpr int SLD = 33;  // staged row stride (float2), conflict-light in both directions
+        float2* stg = reinterpret_cast<float2*>(gbase) + (warp - 2) * (32 * SLD);
 #pragma unroll 1
         for (int chunk = 0; chunk < TC_BNW / 32; ++chunk) {
-            uint32_t v[32];
+            uint32_t vr[32], vi[32];
             const uint32_t taddr = tmem + (uint32_t(lg * 32) << 16) + uint32_t(chunk * 32);
-            YQ_TMEM_LD_X32(taddr, v);
+            YQ_TMEM_LD_X32(taddr, vr);
+            YQ_TMEM_LD_X32(taddr + TC_BNW, vi);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (!ok || r >= p.ns) continue;
-            double* grow = reinterpret_cast<double*>(p.G + size_t(r) * p.ldg) + half;
+            const int c0 = cbase + chunk * 32;
+            if (!ok || rbase >= p.n || c0 > rbase + 31) continue;  // warp-uniform
 #pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                const int c = bj * TC_BNW + chunk * 32 + i;
-                if (c < p.ns && c <= r) {
-                    double val = p.alpha * double(__uint_as_float(v[i]));
-                    if (!half && c == r) val += p.shift;
-                    grow[2 * size_t(c)] = val;
+            for (int i = 0; i < 32; ++i) stg[lane * SLD + i] = make_float2(__uint_as_float(vr[i]), __uint_as_float(vi[i]));
+            __syncwarp();
+            const int c = c0 + lane;
+            if (p.accumulate) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    double2 o[16];
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const int r = rbase + 16 * h + k;
+                        o[k] = (r < p.n && c <= r) ? reinterpret_cast<const double2*>(p.C + size_t(r) * p.ldc)[c]
+                                                   : make_double2(0.0, 0.0);
+                    }
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const int rr = 16 * h + k, r = rbase + rr;
+                        if (r < p.n && c <= r) {
+                            const float2 v = stg[rr * SLD + lane];
+                            o[k].x += p.alpha * double(v.x);
+                            o[k].y += p.alpha * double(v.y);
+                            reinterpret_cast<double2*>(p.C + size_t(r) * p.ldc)[c] = o[k];
+                        }
+                    }
+                }
+            } else {
+#pragma unroll 4
+                for (int rr = 0; rr < 32; ++rr) {
+                    const int r = rbase + rr;
+                    if (r < p.n && c <= r) {
+                        const float2 v = stg[rr * SLD + lane];
+                        double re = p.alpha * double(v.x);
+                        if (c == r) re += p.shift;
+                        reinterpret_cast<double2*>(p.C + size_t(r) * p.ldc)[c] = make_double2(re, p.alpha * double(v.y));
+                    }
                 }
             }
+            __syncwarp();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -314,36 +400,43 @@ static CUtensorMap make_map(const uint16_t* base, size_t rows, size_t kpad, uint
     return m;
 }
 
-void gram_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int ns, size_t P,
-                 c128* G, size_t ldg, double alpha, double shift, int* d_status, cudaStream_t st) {
-    const size_t kpad = gram_tc_kpad(P), rows = gram_tc_rows(ns);
-    YQ_CHECK_ARG(kpad % TC_BK == 0 && rows % TC_BM == 0, "gram_tc: operand padding");
+void herk_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int n,
+                 size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
+                 int* d_status, cudaStream_t st) {
+    YQ_CHECK_ARG(n > 0 && kpad % TC_BK == 0 && kpad > 0 && rows_pad % TC_BM == 0 && size_t(n) <= rows_pad,
+                 "herk_tc: operand padding");
     YQ_CHECK_ARG(reinterpret_cast<uintptr_t>(xh) % 16 == 0 && reinterpret_cast<uintptr_t>(xl) % 16 == 0 &&
                      reinterpret_cast<uintptr_t>(yh) % 16 == 0 && reinterpret_cast<uintptr_t>(yl) % 16 == 0,
-                 "gram_tc: operand base addresses must be 16-byte aligned");
-    CUtensorMap mXhA = make_map(xh, rows, kpad, TC_BM), mXlA = make_map(xl, rows, kpad, TC_BM);
-    CUtensorMap mYhA = make_map(yh, rows, kpad, TC_BM), mYlA = make_map(yl, rows, kpad, TC_BM);
-    CUtensorMap mXhB = make_map(xh, rows, kpad, TC_BNW), mXlB = make_map(xl, rows, kpad, TC_BNW);
+                 "herk_tc: operand base addresses must be 16-byte aligned");
+    YQ_CHECK_ARG(reinterpret_cast<uintptr_t>(C) % 16 == 0, "herk_tc: output must be 16-byte aligned");
+    CUtensorMap mXh = make_map(xh, rows_pad, kpad, TC_BM), mXl = make_map(xl, rows_pad, kpad, TC_BM);
+    CUtensorMap mYh = make_map(yh, rows_pad, kpad, TC_BM), mYl = make_map(yl, rows_pad, kpad, TC_BM);
+    CUtensorMap mBh = make_map(xh, rows_pad, kpad, TC_BNW), mBl = make_map(xl, rows_pad, kpad, TC_BNW);
     TcParams p;
-    p.ns = ns;
-    p.nt = int(rows / TC_BM);
-    int tph = 0;
-    for (int b = 0; b < p.nt; ++b) tph += (b >> 1) + 1;
-    p.tiles_per_half = tph;
+    p.n = n;
+    p.nt = int((size_t(n) + TC_BM - 1) / TC_BM);
+    int tiles = 0;
+    for (int b = 0; b < p.nt; ++b) tiles += (b >> 1) + 1;
     p.kb_per_seg = int(kpad / TC_BK);
-    p.G = G;
-    p.ldg = ldg;
+    p.C = C;
+    p.ldc = ldc;
     p.alpha = alpha;
     p.shift = shift;
+    p.accumulate = accumulate ? 1 : 0;
     p.status = d_status;
     p.wait_cap = 1u << 24;
     static bool attr = false;
     if (!attr) {
-        YQ_CUDA(cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TC_SMEM)));
+        YQ_CUDA(cudaFuncSetAttribute(herk_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TC_SMEM)));
         attr = true;
     }
-    gram_tc_kernel<<<2 * tph, TC_THREADS, TC_SMEM, st>>>(mXhA, mXlA, mYhA, mYlA, mXhB, mXlB, p);
+    herk_tc_kernel<<<tiles, TC_THREADS, TC_SMEM, st>>>(mXh, mXl, mYh, mYl, mBh, mBl, p);
     YQ_LAUNCH_CHECK();
+}
+
+void gram_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int ns, size_t P,
+                 c128* G, size_t ldg, double alpha, double shift, int* d_status, cudaStream_t st) {
+    herk_tc_run(xh, xl, yh, yl, ns, gram_tc_rows(ns), gram_tc_kpad(P), G, ldg, alpha, shift, false, d_status, st);
 }
 
 }  // namespace yq

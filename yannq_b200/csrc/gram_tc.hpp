@@ -1,8 +1,11 @@
-// Tensor-core (tcgen05) Gram matrix of the mixed-precision SR path:
-//   T = O~ O~^H / Ns + shift I   from complex64 O~ (Ns x P, row-major),
-// as one real GEMM  [X; Y] X^T  with X = [Re O~ | Im O~], Y = [Im O~ | -Re O~]
-// (T_re = X X^T, T_im = Y X^T), each operand split into BF16 hi + lo parts and
-// the three products hi.hi + hi.lo + lo.hi accumulated in FP32 in TMEM.
+// Tensor-core (tcgen05) Hermitian rank-k kernels of the mixed-precision SR path.
+//
+// For a complex matrix A (rows x K) the product A A^H is one real GEMM pair
+//   Re(A A^H) = X X^T,  Im(A A^H) = Y X^T,   X = [Re A | Im A],  Y = [Im A | -Re A],
+// with every operand split into BF16 hi + lo parts and the three products
+// hi.hi + hi.lo + lo.hi accumulated in FP32 in TMEM.  The same kernel forms the
+// Gram matrix T = O~ O~^H / Ns + shift I and applies the trailing updates
+// C -= L21 L21^H of the panel Cholesky.
 #pragma once
 #include <cstddef>
 #include <cstdint>
@@ -12,7 +15,6 @@
 namespace yq {
 
 constexpr int TC_BM = 128;  // rows of a tile (TMEM lanes)
-constexpr int TC_BN = 128;  // columns of a tile (TMEM columns, FP32)
 constexpr int TC_BK = 64;   // K per stage: 64 BF16 = one 128-byte swizzle atom row
 
 // K extent (2P) padded to the stage depth, and the padded row count of the operands.
@@ -27,5 +29,17 @@ void gram_tc_prepare_operands(const c64* O, int ns, size_t P, uint16_t* xh, uint
 // G[r, c] (r >= c, r, c < ns) = alpha * T_(r,c) + shift * [r == c], complex FP64, row stride ldg.
 void gram_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int ns, size_t P,
                  c128* G, size_t ldg, double alpha, double shift, int* d_status, cudaStream_t st);
+
+// General form over planes of `rows_pad` rows (a multiple of 128) and `kpad` BF16
+// columns (a multiple of 64):  for r >= c, r, c < n
+//   C[r, c] = (accumulate ? C[r, c] : 0) + alpha (A A^H)_(r,c) + shift [r == c].
+void herk_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int n,
+                 size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
+                 int* d_status, cudaStream_t st);
+
+// Split the complex FP64 block G[r0 .. r0 + n), [c0 .. c0 + w) (row stride ld) into
+// the four planes with K = 2 w; rows n .. rows_pad are written as zeros.
+void herk_tc_split_block(const c128* G, size_t ld, int r0, int c0, int n, int w, size_t rows_pad, uint16_t* xh,
+                         uint16_t* xl, uint16_t* yh, uint16_t* yl, cudaStream_t st);
 
 }  // namespace yq

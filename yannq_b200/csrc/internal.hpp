@@ -101,7 +101,8 @@ struct yq_sr_s {
     // dense SR matrix and Cholesky factor (lower, row-major, dim_pad x dim_pad)
     int dim = 0, dim_pad = 0;
     yq::DevBuf G, Linv, LinvH;
-    yq::DevBuf chol_work;  // persistent Cholesky flags, counter and tile order
+    yq::DevBuf chol_work;    // persistent Cholesky flags, counters and tile order
+    yq::DevBuf chol_planes;  // BF16 split panels of the mixed-precision Cholesky
     // mixed precision operands (BF16 hi/lo planes of [Re|Im] and [Im|-Re])
     yq::DevBuf xh, xl, yh, yl;
     double host_stats[8] = {};

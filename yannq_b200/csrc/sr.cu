@@ -523,19 +523,32 @@ static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps) {
     form_matrix_t<R>(sr, shift);
     ctx->stage_end(ST_GRAM);
     ctx->stage_begin(ST_SOLVE);
-    // Persistent tile Cholesky by default; YQ_CHOLESKY=recursive selects the
-    // recursive launch-per-step variant (kept for comparison).
-    static const bool recursive = [] {
+    // Factorisation: the mixed-precision T-form (whose matrix comes from BF16x3
+    // products) uses the panel form with tensor-core trailing updates; everything
+    // else the persistent FP64 tile kernel.  YQ_CHOLESKY=tiled|recursive overrides
+    // (the recursive launch-per-step variant is kept for comparison).
+    static const int forced = [] {
         const char* e = std::getenv("YQ_CHOLESKY");
-        return e && std::string(e) == "recursive";
+        if (!e) return 0;
+        if (std::string(e) == "recursive") return 1;
+        if (std::string(e) == "tiled") return 2;
+        return 0;
     }();
+    const bool recursive = forced == 1;
+    const bool panels = forced == 0 && sr->precision == YQ_PREC_MIXED && sr->mode == YQ_SR_T;
     sr->chol_work.ensure(chol_tile_scratch_bytes(sr->dim_pad));
-    if (recursive)
+    if (recursive) {
         chol_factor(sr->G.as<c128>(), sr->dim_pad, size_t(sr->dim_pad), sr->Linv.as<c128>(), sr->LinvH.as<c128>(),
                     ctx->status.as<int>(), st);
-    else
+    } else if (panels) {
+        sr->chol_planes.ensure(chol_panel_planes_bytes(sr->dim_pad));
+        chol_factor_panels(sr->G.as<c128>(), sr->dim_pad, size_t(sr->dim_pad), sr->Linv.as<c128>(),
+                           sr->LinvH.as<c128>(), ctx->status.as<int>(), sr->chol_work.p, sr->chol_planes.p,
+                           ctx->sm_count, st);
+    } else {
         chol_factor_tiled(sr->G.as<c128>(), sr->dim_pad, size_t(sr->dim_pad), sr->Linv.as<c128>(),
                           sr->LinvH.as<c128>(), ctx->status.as<int>(), sr->chol_work.p, ctx->sm_count, st);
+    }
     const size_t dp = size_t(sr->dim_pad);
     const c128* G = sr->G.as<c128>();
     const c128* Li = sr->Linv.as<c128>();
