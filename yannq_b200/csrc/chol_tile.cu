@@ -12,8 +12,9 @@
 // timeout sets DS_TIMEOUT and an abort word that makes every CTA stop.
 //
 // The solves use the same scheme with 64-row blocks: the forward sweep of block
-// row r accumulates L[r, k] x_k as each x_k is published, then applies
-// L_rr^{-1}; the backward sweep runs the block rows in reverse with L^H.
+// row r accumulates L[r, k] x_k as each x_k is published (its L tiles streamed
+// into shared memory ahead of the flags), then applies L_rr^{-1}; the backward
+// sweep runs the block rows in reverse with L^H.
 #include <algorithm>
 #include <vector>
 
@@ -352,92 +353,120 @@ struct SolveArgs {
     Sync S;
 };
 
-__device__ __forceinline__ c128 wsum(c128 v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        v.re += __shfl_xor_sync(0xffffffffu, v.re, o);
-        v.im += __shfl_xor_sync(0xffffffffu, v.im, o);
+// Solve sweeps.  One CTA per 64-row block (persistent over blocks r = blockIdx.x,
+// + gridDim.x, ...).  The L tiles a block needs do not depend on the sweep, so they
+// stream into shared memory (cp.async, two buffers) ahead of the flags; only the
+// 64-entry solution block x_k waits for its flag.  The diagonal inverse is staged
+// at the start.  Each chain link is then a shared-memory mat-vec.
+constexpr int SLD = TB + 1;  // staged tile row stride (complex)
+constexpr size_t SM_SOLVE = size_t(3) * TB * SLD * sizeof(c128) + 2 * TB * sizeof(c128);
+
+// Stage the 64 x 64 tile at `src` (row stride ld) into dst[64][SLD].
+__device__ __forceinline__ void stage_tile(c128* dst, const c128* src, size_t ld) {
+    for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
+        const int r = e >> 6, c = e & 63;
+        cpa16(&dst[r * SLD + c], src + size_t(r) * ld + c);
     }
-    return v;
 }
 
 // Forward: x_r = L_rr^{-1} (b_r - sum_{k<r} L_rk x_k), block rows in increasing order.
-__global__ void __launch_bounds__(128) chol_fwd_tile_kernel(SolveArgs a) {
-    __shared__ c128 acc[TB], xk[TB];
+__global__ void __launch_bounds__(128, 1) chol_fwd_tile_kernel(SolveArgs a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    c128* buf = reinterpret_cast<c128*>(sm);   // 2 tiles
+    c128* Li = buf + 2 * TB * SLD;             // diagonal inverse
+    c128* xk = Li + TB * SLD;                  // published block
+    c128* acc = xk + TB;
     __shared__ int s_ok;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, row = tid >> 1, half = tid & 1;
     for (int r = blockIdx.x; r < a.nt; r += gridDim.x) {
+        stage_tile(Li, a.Linv + size_t(r) * TB * TB, TB);
+        cpa_commit();
+        if (r > 0) stage_tile(buf, a.G + size_t(r) * TB * a.ld, a.ld);
+        cpa_commit();
         if (tid < TB) acc[tid] = a.b[r * TB + tid];
-        __syncthreads();
         bool ok = true;
         for (int k = 0; k < r; ++k) {
+            if (k + 1 < r) stage_tile(buf + ((k + 1) & 1) * TB * SLD, a.G + size_t(r) * TB * a.ld + (k + 1) * TB, a.ld);
+            cpa_commit();
             if (!wait_flag(&a.flags[k], a.S, &s_ok)) {
                 ok = false;
                 break;
             }
             if (tid < TB) xk[tid] = a.b[k * TB + tid];
+            cpa_wait_one();  // tile k (and everything before it) has landed
             __syncthreads();
-            // 4 warps x 16 rows; lanes over the 64 columns
-            for (int q = 0; q < TB / 4; ++q) {
-                const int row = warp * (TB / 4) + q;
-                const c128* Lr = a.G + size_t(r * TB + row) * a.ld + k * TB;
-                c128 v = wsum(Lr[lane] * xk[lane] + Lr[lane + 32] * xk[lane + 32]);
-                if (lane == 0) acc[row] = acc[row] - v;
-            }
+            const c128* T = buf + (k & 1) * TB * SLD + row * SLD + half * 32;
+            c128 v = mk(0., 0.);
+#pragma unroll 8
+            for (int c = 0; c < 32; ++c) v = v + T[c] * xk[half * 32 + c];
+            v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
+            v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
             __syncthreads();
+            if (half == 0) acc[row] = acc[row] - v;
         }
-        if (!ok) return;
-        const c128* Li = a.Linv + size_t(r) * TB * TB;
-        c128 out[TB / 4];
-        for (int q = 0; q < TB / 4; ++q) {
-            const int row = warp * (TB / 4) + q;
-            out[q] = wsum(Li[row * TB + lane] * acc[lane] + Li[row * TB + lane + 32] * acc[lane + 32]);
-        }
+        cpa_wait_all();
         __syncthreads();
-        if (lane == 0)
-            for (int q = 0; q < TB / 4; ++q) a.b[r * TB + warp * (TB / 4) + q] = out[q];
+        if (!ok) return;
+        c128 v = mk(0., 0.);
+#pragma unroll 8
+        for (int c = 0; c < 32; ++c) v = v + Li[row * SLD + half * 32 + c] * acc[half * 32 + c];
+        v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
+        v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
+        if (half == 0) a.b[r * TB + row] = v;
         publish(&a.flags[r]);
     }
 }
 
 // Backward: z_r = L_rr^{-H} (x_r - sum_{k>r} L_kr^H z_k), block rows in decreasing order.
-__global__ void __launch_bounds__(128) chol_bwd_tile_kernel(SolveArgs a) {
-    __shared__ c128 acc[TB], zk[TB];
-    __shared__ c128 part[2][TB];
+__global__ void __launch_bounds__(128, 1) chol_bwd_tile_kernel(SolveArgs a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    c128* buf = reinterpret_cast<c128*>(sm);
+    c128* Li = buf + 2 * TB * SLD;
+    c128* zk = Li + TB * SLD;
+    c128* acc = zk + TB;
     __shared__ int s_ok;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, col = tid >> 1, half = tid & 1;
     for (int t = blockIdx.x; t < a.nt; t += gridDim.x) {
         const int r = a.nt - 1 - t;
+        stage_tile(Li, a.LinvH + size_t(r) * TB * TB, TB);
+        cpa_commit();
+        if (r + 1 < a.nt) stage_tile(buf, a.G + size_t(a.nt - 1) * TB * a.ld + r * TB, a.ld);
+        cpa_commit();
         if (tid < TB) acc[tid] = a.b[r * TB + tid];
-        __syncthreads();
         bool ok = true;
-        for (int k = a.nt - 1; k > r; --k) {
+        for (int k = a.nt - 1, i = 0; k > r; --k, ++i) {
+            if (k - 1 > r) stage_tile(buf + ((i + 1) & 1) * TB * SLD, a.G + size_t(k - 1) * TB * a.ld + r * TB, a.ld);
+            cpa_commit();
             if (!wait_flag(&a.flags[k], a.S, &s_ok)) {
                 ok = false;
                 break;
             }
             if (tid < TB) zk[tid] = a.b[k * TB + tid];
+            cpa_wait_one();
             __syncthreads();
-            // acc[c] -= sum_row conj(L[k*64 + row][r*64 + c]) z_k[row]; thread (half, c)
-            const int c = tid & (TB - 1), half = tid >> 6;
+            // acc[col] -= sum_row conj(L[k*64 + row][r*64 + col]) z_k[row]
+            const c128* T = buf + (i & 1) * TB * SLD + col;
             c128 v = mk(0., 0.);
-            for (int row = half * 32; row < half * 32 + 32; ++row)
-                v = v + conj(a.G[size_t(k * TB + row) * a.ld + r * TB + c]) * zk[row];
-            part[half][c] = v;
+#pragma unroll 8
+            for (int q = 0; q < 32; ++q) {
+                const int rr = half * 32 + q;
+                v = v + conj(T[rr * SLD]) * zk[rr];
+            }
+            v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
+            v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
             __syncthreads();
-            if (tid < TB) acc[tid] = acc[tid] - part[0][tid] - part[1][tid];
-            __syncthreads();
+            if (half == 0) acc[col] = acc[col] - v;
         }
-        if (!ok) return;
-        const c128* LiH = a.LinvH + size_t(r) * TB * TB;
-        c128 out[TB / 4];
-        for (int q = 0; q < TB / 4; ++q) {
-            const int row = warp * (TB / 4) + q;
-            out[q] = wsum(LiH[row * TB + lane] * acc[lane] + LiH[row * TB + lane + 32] * acc[lane + 32]);
-        }
+        cpa_wait_all();
         __syncthreads();
-        if (lane == 0)
-            for (int q = 0; q < TB / 4; ++q) a.b[r * TB + warp * (TB / 4) + q] = out[q];
+        if (!ok) return;
+        const int rowo = col;
+        c128 v = mk(0., 0.);
+#pragma unroll 8
+        for (int c = 0; c < 32; ++c) v = v + Li[rowo * SLD + half * 32 + c] * acc[half * 32 + c];
+        v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
+        v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
+        if (half == 0) a.b[r * TB + rowo] = v;
         publish(&a.flags[r]);
     }
 }
@@ -558,19 +587,25 @@ void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c
     int* sflags = sc.sflags;
     YQ_CUDA(cudaMemsetAsync(sflags, 0, 2 * size_t(nt) * sizeof(int), st));
     YQ_CUDA(cudaMemsetAsync(words + 2, 0, sizeof(int), st));  // abort word of the solves
-    const int grid_f = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_fwd_tile_kernel), 128, 0,
-                                                      sm_count));
-    const int grid_b = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_bwd_tile_kernel), 128, 0,
-                                                      sm_count));
+    static bool attr = false;
+    if (!attr) {
+        YQ_CUDA(cudaFuncSetAttribute(chol_fwd_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SM_SOLVE)));
+        YQ_CUDA(cudaFuncSetAttribute(chol_bwd_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SM_SOLVE)));
+        attr = true;
+    }
+    const int grid_f = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_fwd_tile_kernel), 128,
+                                                      SM_SOLVE, sm_count));
+    const int grid_b = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_bwd_tile_kernel), 128,
+                                                      SM_SOLVE, sm_count));
     SolveArgs fa{G, ld, nt, Linv, LinvH, b, sflags, Sync{status, words + 2, 1u << 24}};
     void* fargs[] = {&fa};
     YQ_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(chol_fwd_tile_kernel), dim3(grid_f), dim3(128),
-                                        fargs, 0, st));
+                                        fargs, SM_SOLVE, st));
     YQ_LAUNCH_CHECK();
     SolveArgs ba{G, ld, nt, Linv, LinvH, b, sflags + nt, Sync{status, words + 2, 1u << 24}};
     void* bargs[] = {&ba};
     YQ_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(chol_bwd_tile_kernel), dim3(grid_b), dim3(128),
-                                        bargs, 0, st));
+                                        bargs, SM_SOLVE, st));
     YQ_LAUNCH_CHECK();
     if (out != b) YQ_CUDA(cudaMemcpyAsync(out, b, size_t(n) * sizeof(c128), cudaMemcpyDeviceToDevice, st));
 }

@@ -148,10 +148,23 @@ __global__ void ohy_partial_kernel(size_t P, int ns, int chunk, const cplx<R>* _
     if (p >= P) return;
     const int s0 = split * chunk, s1 = min(ns, s0 + chunk);
     double ar = 0., ai = 0.;
-    for (int s = s0; s < s1; ++s) {
-        cplx<R> o = O[size_t(s) * P + p];
-        c128 y = yv[s];
-        // conj(o) * y
+    int s = s0;
+    // eight independent row loads in flight per thread
+    for (; s + 8 <= s1; s += 8) {
+        cplx<R> o[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) o[u] = O[size_t(s + u) * P + p];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const c128 y = yv[s + u];
+            // conj(o) * y
+            ar += double(o[u].re) * y.re + double(o[u].im) * y.im;
+            ai += double(o[u].re) * y.im - double(o[u].im) * y.re;
+        }
+    }
+    for (; s < s1; ++s) {
+        const cplx<R> o = O[size_t(s) * P + p];
+        const c128 y = yv[s];
         ar += double(o.re) * y.re + double(o.im) * y.im;
         ai += double(o.re) * y.im - double(o.im) * y.re;
     }
@@ -169,7 +182,8 @@ __global__ void reduce_parts_kernel(size_t P, int nsplit, double alpha, const c1
     }
 }
 
-// out_s = alpha * sum_p O~[s, p] x_p  (one block per sample row)
+// out_s = alpha * sum_p O~[s, p] x_p  (one block streams one sample row; four
+// loads of the row in flight per thread)
 template <typename R>
 __global__ void ox_kernel(size_t P, int ns, const cplx<R>* __restrict__ O, const c128* __restrict__ x, double alpha,
                           c128* __restrict__ out) {
@@ -177,9 +191,25 @@ __global__ void ox_kernel(size_t P, int ns, const cplx<R>* __restrict__ O, const
     const int s = blockIdx.x;
     const cplx<R>* row = O + size_t(s) * P;
     double ar = 0., ai = 0.;
-    for (size_t p = threadIdx.x; p < P; p += blockDim.x) {
-        cplx<R> o = row[p];
-        c128 xv = x[p];
+    const size_t step = blockDim.x;
+    size_t p = threadIdx.x;
+    for (; p + 3 * step < P; p += 4 * step) {
+        cplx<R> o[4];
+        c128 xv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            o[u] = row[p + u * step];
+            xv[u] = x[p + u * step];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            ar += double(o[u].re) * xv[u].re - double(o[u].im) * xv[u].im;
+            ai += double(o[u].re) * xv[u].im + double(o[u].im) * xv[u].re;
+        }
+    }
+    for (; p < P; p += step) {
+        const cplx<R> o = row[p];
+        const c128 xv = x[p];
         ar += double(o.re) * xv.re - double(o.im) * xv.im;
         ai += double(o.re) * xv.im + double(o.im) * xv.re;
     }
@@ -276,7 +306,7 @@ static void construct_t(yq_sr_s* sr) {
         nsplit = std::min(nsplit, ns);
         int chunk = (ns + nsplit - 1) / nsplit;
         g.z = nsplit;
-        sr->part.ensure(std::max(size_t(nsplit) * (n + 1) * (m + 1), size_t(16) * P) * sizeof(c128));
+        sr->part.ensure(std::max(size_t(nsplit) * (n + 1) * (m + 1), size_t(64) * P) * sizeof(c128));
         oloc_partial_kernel<R><<<g, 256, 0, st>>>(n, m, ns, chunk, sigma, sr->tanhs.as<cplx<R>>(), sr->part.as<c128>());
         YQ_LAUNCH_CHECK();
         oloc_reduce_kernel<<<cdiv_u(size_t(n + 1) * (m + 1), 256), 256, 0, st>>>(
@@ -303,9 +333,10 @@ static void construct_t(yq_sr_s* sr) {
                                                           sr->y.as<c128>());
     YQ_LAUNCH_CHECK();
     {
-        const int nsplit = std::max(1, std::min(16, int(4 * 148 / std::max(1u, cdiv_u(P, 256)))));
+        const unsigned gx = cdiv_u(P, 256);
+        const int nsplit = std::max(1, std::min({64, ns, int(8 * 148 / gx)}));
         const int chunk = (ns + nsplit - 1) / nsplit;
-        dim3 g(cdiv_u(P, 256), nsplit);
+        dim3 g(gx, nsplit);
         ohy_partial_kernel<R><<<g, 256, 0, st>>>(P, ns, chunk, sr->O.as<cplx<R>>(), sr->y.as<c128>(),
                                                  sr->part.as<c128>());
         YQ_LAUNCH_CHECK();
@@ -402,9 +433,10 @@ static void op_ohy(yq_sr_s* sr, const c128* x, double alpha, c128* out, const c1
     cudaStream_t st = sr->q->ctx->stream;
     const size_t P = sr->q->P;
     const int ns = sr->ns;
-    const int nsplit = std::max(1, std::min(16, int(4 * 148 / std::max(1u, cdiv_u(P, 256)))));
+    const unsigned gx = cdiv_u(P, 256);
+    const int nsplit = std::max(1, std::min({64, ns, int(8 * 148 / gx)}));
     const int chunk = (ns + nsplit - 1) / nsplit;
-    dim3 g(cdiv_u(P, 256), nsplit);
+    dim3 g(gx, nsplit);
     ohy_partial_kernel<R><<<g, 256, 0, st>>>(P, ns, chunk, sr->O.as<cplx<R>>(), x, sr->part.as<c128>());
     YQ_LAUNCH_CHECK();
     reduce_parts_kernel<<<cdiv_u(P, 256), 256, 0, st>>>(P, nsplit, alpha, sr->part.as<c128>(), addv, beta, out);
