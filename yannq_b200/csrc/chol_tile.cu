@@ -125,90 +125,152 @@ __device__ __forceinline__ void warp_mma(const c128* A, int lda, const c128* B, 
 }
 
 // Factorisation of the 64 x 64 tile F (lower part) in shared memory and its
-// inverse X = L^{-1}, fused into one right-looking sweep with one barrier per
-// step.  The 128 threads form a 16 x 8 grid; thread (tr, tq) owns the elements
-// (tr + 16 a, tq + 8 b), a < 4, b < 8, of F and of X, so every step gives each
-// thread up to 32 independent updates.  Step c, with d = F_cc:
-//   L[:, c] = F[:, c] / sqrt(d)                      (written to T)
-//   F_rq -= F_rc conj(F_qc) / d       for c < q <= r (trailing Schur complement)
-//   R_rq -= F_rc R_cq / d             for q <= c < r (row elimination of R = I)
-// and row c of R becomes row c of X = L^{-1} after scaling by 1 / sqrt(d), which
-// is done one step later (step c reads R_c*, nothing reads it afterwards).  Every
-// write goes to an element that no thread reads in the same step.  On exit F
-// holds L (upper part zero).  Needs blockDim.x == 128.
-__device__ void factor_tile(c128* F, c128* X, c128* T, int* status) {
-    const int tid = threadIdx.x;
-    const int tr = tid & 15, tq = tid >> 4;
-    for (int e = tid; e < TB * TB; e += 128) {
-        const int r = e / TB, c = e % TB;
-        X[r * FLS + c] = mk(r == c ? 1.0 : 0.0, 0.0);
-        T[r * FLS + c] = mk(0., 0.);
-    }
-    __syncthreads();
-    double is_prev = 1.0;
-    for (int c = 0; c < TB; ++c) {
-        double d = F[c * FLS + c].re;
+// inverse X = L^{-1}, by recursive halving (128 threads):
+//   chol(A11) -> L11, X11;   L21 = A21 X11^H;   A22 -= L21 L21^H;
+//   chol(A22) -> L22, X22;   X21 = -X22 (L21 X11),
+// with the products on DMMA (m8n8k4, one 8 x 8 output tile per warp at a time)
+// and 8 x 8 leaves factored and inverted by one warp in registers (lane r holds
+// row r; pivots and columns move by shuffles).  Levels of size 16 and below run
+// in warp 0 alone (warp barriers), the levels above use all four warps.  T is
+// scratch.  On exit F holds L in its lower triangle (the caller reads only that)
+// and X holds L^{-1} with zeros above the diagonal.
+
+// Lane r < 8 of warp 0: rows o + r of the 8 x 8 diagonal block.
+__device__ __forceinline__ void leaf8(c128* F, c128* X, int o, int* status) {
+    const int lane = threadIdx.x & 31, r = lane & 7;
+    c128 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = q <= r ? F[(o + r) * FLS + o + q] : mk(0., 0.);
+    double diag = 1.0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        double d = __shfl_sync(0xffffffffu, v[c].re, c);
         if (!(d > 0.0)) {
-            if (tid == 0) atomicOr(status, DS_NOT_PD);
+            if (lane == 0) atomicOr(status, DS_NOT_PD);
             d = 1.0;  // unit pivot keeps the launch well defined
         }
-        const double is = rsqrt(d), id = is * is;
-        c128 fc[4], fq[8], xq[8];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) fc[a] = F[(tr + 16 * a) * FLS + c];
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const int q = tq + 8 * b;
-            fq[b] = F[q * FLS + c];
-            xq[b] = X[c * FLS + q];
-        }
-        if (tq == (c & 7)) {
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const int r = tr + 16 * a;
-                if (r == c) T[r * FLS + c] = mk(d * is, 0.0);
-                else if (r > c) T[r * FLS + c] = is * fc[a];
-            }
-        }
-        if (c > 0 && tr == ((c - 1) & 15)) {
-            const int r = c - 1;  // = tr + 16 ((c - 1) >> 4)
-#pragma unroll
-            for (int b = 0; b < 8; ++b) {
-                const int q = tq + 8 * b;
-                if (q <= r) X[r * FLS + q] = is_prev * X[r * FLS + q];
-            }
+        const double is = rsqrt(d);
+        const c128 lc = r > c ? is * v[c] : mk(0., 0.);  // L_rc
+        if (r == c) {
+            diag = d * is;
+            v[c] = mk(diag, 0.0);
+        } else if (r > c) {
+            v[c] = lc;
         }
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int r = tr + 16 * a;
-            if (r > c) {
-                const c128 g = id * fc[a];
-#pragma unroll
-                for (int b = 0; b < 8; ++b) {
-                    const int q = tq + 8 * b;
-                    if (q > c) {
-                        if (q <= r) F[r * FLS + q] = F[r * FLS + q] - g * conj(fq[b]);
-                    } else {
-                        X[r * FLS + q] = X[r * FLS + q] - g * xq[b];
-                    }
-                }
-            }
-        }
-        is_prev = is;
-        __syncthreads();
-    }
-    if (tr == ((TB - 1) & 15)) {
-        const int r = TB - 1;
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const int q = tq + 8 * b;
-            X[r * FLS + q] = is_prev * X[r * FLS + q];
+        for (int q = c + 1; q < 8; ++q) {
+            c128 lq;  // L_qc
+            lq.re = __shfl_sync(0xffffffffu, lc.re, q);
+            lq.im = __shfl_sync(0xffffffffu, lc.im, q);
+            if (r >= q) v[q] = v[q] - lc * conj(lq);
         }
     }
-    for (int e = tid; e < TB * TB; e += 128) {
-        const int r = e / TB, c = e % TB;
-        F[r * FLS + c] = T[r * FLS + c];
+    // X row r: X_rr = 1 / L_rr, X_rj = -(1 / L_rr) sum_{j <= k < r} L_rk X_kj
+    const double idg = 1.0 / diag;
+    c128 x[8], acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = acc[j] = mk(0., 0.);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (r == k) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (j < k) x[j] = (-idg) * acc[j];
+                else if (j == k) x[j] = mk(idg, 0.0);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j <= k; ++j) {
+            c128 xk;  // X_kj
+            xk.re = __shfl_sync(0xffffffffu, x[j].re, k);
+            xk.im = __shfl_sync(0xffffffffu, x[j].im, k);
+            if (r > k) acc[j] = acc[j] + v[k] * xk;
+        }
     }
+    if (lane < 8) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            F[(o + r) * FLS + o + q] = v[q];
+            X[(o + r) * FLS + o + q] = x[q];
+        }
+    }
+}
+
+enum { OP_BH = 0, OP_B = 1 };  // op(B) = B^H (B stored by output columns) or B (stored K x n)
+
+// out (h x h, row stride FLS) = (acc ? out : 0) + alpha A op(B), K = h; A row-major
+// (stride FLS).  Output 8 x 8 tiles are spread over `nw` warps starting at warp 0.
+template <int H, int OP>
+__device__ __forceinline__ void tile_prod(c128* out, const c128* A, const c128* B, double alpha, bool acc, int nw) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fk = lane & 3;
+    constexpr int NT = H / 8;
+    for (int t = warp; t < NT * NT; t += nw) {
+        const int ti = t / NT, tj = t % NT;
+        double cre[2] = {0., 0.}, cim[2] = {0., 0.};
+#pragma unroll
+        for (int ks = 0; ks < H / 4; ++ks) {
+            const int k = ks * 4 + fk;
+            const c128 a = A[(ti * 8 + fr) * FLS + k];
+            c128 b;
+            if (OP == OP_BH) b = conj(B[(tj * 8 + fr) * FLS + k]);
+            else b = B[k * FLS + tj * 8 + fr];
+            dmma(cre, a.re, b.re);
+            dmma(cre, -a.im, b.im);
+            dmma(cim, a.re, b.im);
+            dmma(cim, a.im, b.re);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            c128* po = out + (ti * 8 + fr) * FLS + tj * 8 + 2 * fk + h;
+            const c128 v = mk(alpha * cre[h], alpha * cim[h]);
+            *po = acc ? *po + v : v;
+        }
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void level_sync() {
+    if (N <= 16) __syncwarp();
+    else __syncthreads();
+}
+
+template <int N>
+__device__ void chol_rec(c128* F, c128* X, c128* T, int o, int* status) {
+    if constexpr (N == 8) {
+        if ((threadIdx.x >> 5) == 0) leaf8(F, X, o, status);
+    } else {
+        constexpr int H = N / 2;
+        const int nw = N <= 16 ? 1 : 4;
+        const bool active = N > 16 || (threadIdx.x >> 5) == 0;
+        c128* A21 = F + (o + H) * FLS + o;
+        c128* A22 = F + (o + H) * FLS + o + H;
+        c128* X11 = X + o * FLS + o;
+        c128* X21 = X + (o + H) * FLS + o;
+        c128* X22 = X + (o + H) * FLS + o + H;
+        c128* L21 = T + (o + H) * FLS + o;   // lower scratch
+        c128* W = T + o * FLS + o + H;       // upper scratch: L21 X11
+        chol_rec<H>(F, X, T, o, status);
+        level_sync<N>();
+        if (active) tile_prod<H, OP_BH>(L21, A21, X11, 1.0, false, nw);
+        level_sync<N>();
+        if (active) {
+            for (int e = threadIdx.x; e < H * H; e += 32 * nw) A21[(e / H) * FLS + e % H] = L21[(e / H) * FLS + e % H];
+            tile_prod<H, OP_BH>(A22, L21, L21, -1.0, true, nw);
+        }
+        level_sync<N>();
+        chol_rec<H>(F, X, T, o + H, status);
+        level_sync<N>();
+        if (active) tile_prod<H, OP_B>(W, L21, X11, 1.0, false, nw);
+        level_sync<N>();
+        if (active) tile_prod<H, OP_B>(X21, X22, W, -1.0, false, nw);
+        level_sync<N>();
+    }
+}
+
+__device__ void factor_tile(c128* F, c128* X, c128* T, int* status) {
+    for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) X[(e / TB) * FLS + e % TB] = mk(0., 0.);
+    __syncthreads();
+    chol_rec<TB>(F, X, T, 0, status);
     __syncthreads();
 }
 
