@@ -42,6 +42,7 @@ enum { YQ_MOVE_LOCAL = 0, YQ_MOVE_EXCHANGE_ANY = 1, YQ_MOVE_EXCHANGE_NN = 2 };
 enum { YQ_SR_AUTO = 0, YQ_SR_S = 1, YQ_SR_T = 2 };             /* S = <O^H O>, T = O O^H dual */
 enum { YQ_PREC_FP64 = 0, YQ_PREC_MIXED = 1 };
 enum { YQ_SOLVE_LLT = 0, YQ_SOLVE_CG = 1 };
+enum { YQ_BASIS_FULL = 0, YQ_BASIS_JZ = 1 };                   /* Basis/BasisFull.hpp, Basis/BasisJz.hpp */
 
 typedef struct yq_ctx_s* yq_ctx;
 typedef struct yq_rbm_s* yq_rbm;
@@ -160,6 +161,13 @@ int yq_sampler_get_samples(yq_sampler S, int8_t* sigma, double* theta);
 int yq_sampler_get_accepts(yq_sampler S, uint64_t* acc);
 /* Replace the device samples by host ones (for SR on externally supplied samples). */
 int yq_sampler_put_samples(yq_sampler S, int ns, const int8_t* sigma, const double* theta);
+/* ExactSampler<Machine>(qs, basis).sample(ns, 0) -- Samplers/ExactSampler.hpp:49-79:
+ * replaces the sampler's samples by ns draws from |psi|^2 over the full basis
+ * (sampler created with nup < 0) or the basis with nup spins down, at most 2^24
+ * configurations.  Draw i uses the exact-sampler Philox stream (seed, counter
+ * (i, epoch, 0, tag)) in place of the reference's unseeded engine.  positions
+ * (optional, ns entries) receives the drawn basis positions. */
+int yq_sampler_sample_exact(yq_sampler S, int ns, uint64_t seed, uint32_t epoch, uint64_t* positions);
 
 /* ---- stochastic reconfiguration (GroundState/SRMat.hpp) ------------------- */
 /* SRMat<Machine, Hamiltonian>(qs, ham) -- SRMat.hpp:83-87, bound to a sampler.
@@ -183,6 +191,15 @@ int yq_sr_solve(yq_sr sr, double shift, int solver, double cg_tol, double* v, in
 /* corrMat() -- SRMat.hpp:142-149: the Hermitian matrix the last LLT solve used
  * (S or T, including the shift), lower triangle, dim x dim complex row-major. */
 int yq_sr_matrix(yq_sr sr, int* dim, double* out);
+
+/* ---- exact summation (GroundState/SRMatExact.hpp) ------------------------- */
+/* SRMatExact<Machine, Hamiltonian>(qs, ham).constructExact() followed by eloc(),
+ * elocVar(), oloc(), energyGrad() and corrMat() -- SRMatExact.hpp:97-132 -- over
+ * the full basis (YQ_BASIS_FULL, Basis/BasisFull.hpp, n <= 24) or the basis with
+ * nup spins down (YQ_BASIS_JZ, Basis/BasisJz.hpp; XXZ only), at most 2^24
+ * configurations, FP64 sums.  stats = {E, Var}; oloc, grad: P complex
+ * (interleaved re, im); S: P x P complex row-major, or NULL to skip it. */
+int yq_exact(yq_rbm q, yq_ham H, int basis_kind, int nup, double* stats, double* oloc, double* grad, double* S);
 
 /* ---- FeedForward machine (Machines/FeedForward.hpp) ------------------------ */
 /* FeedForward with addLayer<Conv1D>(1, channels, kernel, stride 1, no bias),

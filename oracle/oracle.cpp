@@ -1,6 +1,8 @@
 // yannq oracle implementation -- TEST INFRASTRUCTURE ONLY (see oracle.hpp).
 #include "oracle.hpp"
 
+#include <algorithm>
+
 #include <numeric>
 #include <stdexcept>
 
@@ -436,7 +438,7 @@ CSR build_csr(const Ham& H, const std::vector<uint64_t>& basis, int nt) {
 }
 }  // namespace
 
-ExactResult exact_sr(const RBM& q, const Ham& H, const std::vector<uint64_t>& basis, int nthreads) {
+ExactResult exact_sr(const RBM& q, const Ham& H, const std::vector<uint64_t>& basis, int nthreads, bool with_S) {
     const int nt = nthreads_or_default(nthreads);
     const size_t dim = basis.size(), P = q.dim();
     ExactResult X;
@@ -485,6 +487,7 @@ ExactResult exact_sr(const RBM& q, const Ham& H, const std::vector<uint64_t>& ba
         X.grad[p] = g;
     }
     for (size_t p = 0; p < P; ++p) X.grad[p] -= t * std::conj(X.oloc[p]);
+    if (!with_S) return X;
     X.S.assign(P * P, cd{});
 #pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
     for (long long a = 0; a < (long long)P; ++a)
@@ -494,6 +497,38 @@ ExactResult exact_sr(const RBM& q, const Ham& H, const std::vector<uint64_t>& ba
             X.S[size_t(a) * P + b] = acc - std::conj(X.oloc[a]) * X.oloc[b];
         }
     return X;
+}
+
+std::vector<uint32_t> exact_sample(const RBM& q, const std::vector<uint64_t>& basis, int nsamples, uint64_t seed,
+                                   uint32_t epoch, int nthreads) {
+    const int nt = nthreads_or_default(nthreads);
+    const size_t dim = basis.size();
+    std::vector<double> probs(dim);
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (long long s = 0; s < (long long)dim; ++s) {
+        std::vector<int8_t> sg(q.n);
+        std::vector<cd> th(q.m);
+        for (int i = 0; i < q.n; ++i) sg[i] = ((basis[s] >> i) & 1u) ? int8_t(-1) : int8_t(1);
+        q.theta(sg.data(), th.data());
+        probs[s] = std::norm(q.coeff(sg.data(), th.data()));
+    }
+    std::vector<long double> accum;
+    accum.reserve(dim);
+    long double tot = 0.0L;
+    for (size_t k = 0; k < dim; ++k) {
+        tot += probs[k];
+        accum.push_back(tot);
+    }
+    const long double total = accum.back();
+    accum.back() += 1e-8L;
+    std::vector<uint32_t> out(static_cast<size_t>(nsamples));
+    for (int i = 0; i < nsamples; ++i) {
+        uint32_t x[4];
+        Philox4x32::draw(seed, uint32_t(i), epoch, 0u, TAG_EXACT, x);
+        const long double r = (long double)draw_u53(x[2], x[3]) * total;
+        out[size_t(i)] = uint32_t(std::lower_bound(accum.begin(), accum.end(), r) - accum.begin());
+    }
+    return out;
 }
 
 // Lanczos with full reorthogonalisation; smallest Ritz value by Sturm bisection.

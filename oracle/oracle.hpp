@@ -220,7 +220,15 @@ struct ExactResult {
     double energy = 0., energy_var = 0.;
     std::vector<cd> oloc, grad, S;  // S is P x P row-major
 };
-ExactResult exact_sr(const RBM& q, const Ham& H, const std::vector<uint64_t>& basis, int nthreads);
+ExactResult exact_sr(const RBM& q, const Ham& H, const std::vector<uint64_t>& basis, int nthreads,
+                     bool with_S = true);
+
+// Samplers/ExactSampler.hpp:49-79 restated: CDF of the unnormalised |psi|^2 over the
+// basis accumulated in long double, r = u * total with u from the exact-sampler
+// stream (counter (i, epoch, 0, TAG_EXACT), u53 draw), accum.back() += 1e-8, then
+// std::lower_bound.  Returns basis positions, one per sample.
+std::vector<uint32_t> exact_sample(const RBM& q, const std::vector<uint64_t>& basis, int nsamples, uint64_t seed,
+                                   uint32_t epoch, int nthreads);
 
 // Basis/BasisFull.hpp:126-153, Basis/BasisJz.hpp:25-104
 std::vector<uint64_t> basis_full(int n);

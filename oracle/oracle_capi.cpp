@@ -194,13 +194,25 @@ int orc_exact(int kind, int n, int lx, int ly, double J, double h, double sign, 
     Ham H = make_ham(kind, n, lx, ly, J, h, sign);
     RBM q = make_rbm(n, m, use_bias, params);
     auto basis = basis_kind == 0 ? basis_full(n) : basis_jz(n, nup);
-    ExactResult X = exact_sr(q, H, basis, nthreads);
+    ExactResult X = exact_sr(q, H, basis, nthreads, out_S != nullptr);
     const size_t P = q.dim();
     out_stats[0] = X.energy;
     out_stats[1] = X.energy_var;
     if (out_oloc) std::memcpy(out_oloc, X.oloc.data(), P * sizeof(cd));
     if (out_grad) std::memcpy(out_grad, X.grad.data(), P * sizeof(cd));
     if (out_S) std::memcpy(out_S, X.S.data(), P * P * sizeof(cd));
+    return int(basis.size());
+}
+
+int orc_exact_sample(int n, int m, int use_bias, const double* params, int basis_kind, int nup, int nsamples,
+                     uint64_t seed, uint32_t epoch, uint32_t* out_pos, uint64_t* out_index, int nthreads) {
+    RBM q = make_rbm(n, m, use_bias, params);
+    auto basis = basis_kind == 0 ? basis_full(n) : basis_jz(n, nup);
+    auto pos = exact_sample(q, basis, nsamples, seed, epoch, nthreads);
+    for (int i = 0; i < nsamples; ++i) {
+        out_pos[i] = pos[size_t(i)];
+        if (out_index) out_index[i] = basis[pos[size_t(i)]];
+    }
     return int(basis.size());
 }
 

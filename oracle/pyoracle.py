@@ -68,6 +68,7 @@ def _declare(L):
         "orc_sr_step": (i, [i, i, i, i, d, d, d, i, i, vp, i, vp, vp, d, i, i, d, vp, vp, vp, vp, vp, i]),
         "orc_cholesky_solve": (i, [i, vp, vp]),
         "orc_exact": (i, [i, i, i, i, d, d, d, i, i, vp, i, i, vp, vp, vp, vp, i]),
+        "orc_exact_sample": (i, [i, i, i, vp, i, i, i, u64, u32, vp, vp, i]),
         "orc_basis": (i, [i, i, i, vp, i]),
         "orc_ed_ground": (d, [i, i, i, i, d, d, d, i, i, i, i]),
         "orc_ff_forward": (d, [i, i, i, i, vp, vp]),
@@ -253,6 +254,16 @@ def exact(ham, m, params, basis_kind=0, nup=0, with_S=True, use_bias=True, nthre
     dim = lib().orc_exact(*ham.args(), m, int(use_bias), _p(params), basis_kind, nup, _p(st), _p(ol), _p(g), _p(S),
                           nthreads or os.cpu_count())
     return dict(energy=st[0], energy_var=st[1], oloc=ol, grad=g, S=S, dim=dim)
+
+
+def exact_sample(n, m, params, nsamples, seed, epoch=0, basis_kind=0, nup=0, use_bias=True, nthreads=0):
+    """Samplers/ExactSampler.hpp:49-79 restated: basis positions and configuration
+    indices of `nsamples` draws from |psi|^2 (exact-sampler Philox stream)."""
+    pos = np.zeros(nsamples, np.uint32)
+    idx = np.zeros(nsamples, np.uint64)
+    dim = lib().orc_exact_sample(n, m, int(use_bias), _p(params), basis_kind, nup, nsamples, seed, epoch, _p(pos),
+                                 _p(idx), nthreads or os.cpu_count())
+    return pos, idx, dim
 
 
 def sigma_of(index, n):

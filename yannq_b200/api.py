@@ -21,6 +21,7 @@ MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN = 0, 1, 2
 SR_AUTO, SR_S, SR_T = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 SOLVE_LLT, SOLVE_CG = 0, 1
+BASIS_FULL, BASIS_JZ = 0, 1
 STAGES = {"sample": 0, "eloc": 1, "O": 2, "gram": 3, "solve": 4, "update": 5, "total": 6, "mean": 7}
 
 
@@ -80,6 +81,8 @@ SIGNATURES = {
     "yq_sampler_get_samples": [_vp, _vp, _vp],
     "yq_sampler_get_accepts": [_vp, _vp],
     "yq_sampler_put_samples": [_vp, _i, _vp, _vp],
+    "yq_sampler_sample_exact": [_vp, _i, _u64, _u32, _vp],
+    "yq_exact": [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp],
     "yq_sr_create": [_vp, _vp, _vp, _i, _i, _vp],
     "yq_sr_destroy": [_vp],
     "yq_sr_construct": [_vp],
@@ -129,6 +132,18 @@ def last_error():
 def check(code):
     if code != OK:
         raise YQError(code, last_error())
+
+
+def exact(rbm, ham, basis_kind=0, nup=0, with_S=True):
+    """SRMatExact::constructExact + eloc/elocVar/oloc/energyGrad/corrMat
+    (GroundState/SRMatExact.hpp:97-132) on the device."""
+    P = rbm.dim
+    st = np.zeros(2)
+    ol = np.zeros(P, np.complex128)
+    g = np.zeros(P, np.complex128)
+    S = np.zeros((P, P), np.complex128) if with_S else None
+    check(lib().yq_exact(rbm.h, ham.h, basis_kind, nup, _p(st), _p(ol), _p(g), _p(S) if with_S else None))
+    return dict(energy=st[0], energy_var=st[1], oloc=ol, grad=g, S=S)
 
 
 def launch_count():
@@ -344,6 +359,14 @@ class Sampler:
         s = _s8(sigma)
         th = _c128(theta)
         check(lib().yq_sampler_put_samples(self.h, s.shape[0], _p(s), _p(th)))
+
+    def sample_exact(self, ns, seed, epoch=0, positions=False):
+        """ExactSampler::sample (Samplers/ExactSampler.hpp:49-79): ns draws from |psi|^2
+        over the full basis (nup < 0) or the fixed-Sz basis; returns the drawn basis
+        positions when asked."""
+        pos = np.zeros(ns, np.uint64) if positions else None
+        check(lib().yq_sampler_sample_exact(self.h, ns, seed, epoch, _p(pos) if positions else None))
+        return pos
 
 
 class SR:

@@ -587,6 +587,18 @@ int yq_sampler_get_accepts(yq_sampler S, uint64_t* acc) {
     });
 }
 
+int yq_sampler_sample_exact(yq_sampler S, int ns, uint64_t seed, uint32_t epoch, uint64_t* positions) {
+    return guard([&] {
+        need(S, "sampler");
+        if (ns < 1) throw Error(YQ_E_ARG, "sample_exact: ns must be >= 1");
+        DevBuf pos;
+        if (positions) pos.ensure(size_t(ns) * sizeof(uint64_t));
+        sampler_sample_exact(S, ns, seed, epoch, positions ? pos.as<uint64_t>() : nullptr);
+        if (positions) down(positions, pos.p, size_t(ns), S->q->ctx->stream);
+        raise_device_status(S->q->ctx);
+    });
+}
+
 int yq_sampler_put_samples(yq_sampler S, int ns, const int8_t* sigma, const double* theta) {
     return guard([&] {
         need(S, "sampler");
@@ -694,6 +706,31 @@ int yq_sr_solve(yq_sr sr, double shift, int solver, double cg_tol, double* v, in
         sr_solve(sr, shift, solver, cg_tol, ir, iterations, relres);
         raise_device_status(sr->q->ctx);
         if (v) down(reinterpret_cast<c128*>(v), sr->v.p, sr->q->P, sr->q->ctx->stream);
+    });
+}
+
+int yq_exact(yq_rbm q, yq_ham H, int basis_kind, int nup, double* stats, double* oloc, double* grad, double* S) {
+    return guard([&] {
+        need(q, "rbm");
+        need(H, "hamiltonian");
+        need(stats, "stats");
+        if (q->ctx != H->ctx) throw Error(YQ_E_ARG, "exact: RBM and Hamiltonian belong to different contexts");
+        const size_t P = q->P;
+        DevBuf d_ol, d_g, d_S;
+        d_ol.ensure(P * sizeof(c128));
+        d_g.ensure(P * sizeof(c128));
+        if (S) d_S.ensure(P * P * sizeof(c128));
+        exact_summation(q, H, basis_kind, nup, stats, d_ol.as<c128>(), d_g.as<c128>(), S ? d_S.as<c128>() : nullptr);
+        cudaStream_t st = q->ctx->stream;
+        if (oloc) down(reinterpret_cast<c128*>(oloc), d_ol.p, P, st);
+        if (grad) down(reinterpret_cast<c128*>(grad), d_g.p, P, st);
+        if (S) {
+            c128* h = reinterpret_cast<c128*>(S);
+            down(h, d_S.p, P * P, st);
+            for (size_t a = 0; a < P; ++a)  // lower triangle computed; Hermitian upper part
+                for (size_t b = a + 1; b < P; ++b) h[a * P + b] = conj(h[b * P + a]);
+        }
+        raise_device_status(q->ctx);
     });
 }
 

@@ -124,6 +124,9 @@ void ham_enumerate(yq_ham_s* H, int ns, const int8_t* d_sigma, int* d_a, int* d_
 void ham_eloc(yq_ham_s* H, yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_theta, c128* d_out);
 
 void sr_construct(yq_sr_s* sr);
+void exact_summation(yq_rbm_s* q, yq_ham_s* H, int kind, int nup, double* stats, c128* d_oloc, c128* d_grad,
+                     c128* d_S);
+void sampler_sample_exact(yq_sampler_s* S, int ns, uint64_t seed, uint32_t epoch, uint64_t* d_pos);
 void sr_solve(yq_sr_s* sr, double shift, int solver, double cg_tol, int ir_steps, int* iters, double* relres);
 void sr_update_params(yq_sr_s* sr, double lr);
 void sr_form_matrix_public(yq_sr_s* sr, double shift);
