@@ -255,6 +255,21 @@ typedef struct {
 /* sampler.randomize + sample + constructFromSamples + solve + update params by -lr v. */
 int yq_vmc_iteration(yq_sr sr, const yq_iter_params* p, yq_iter_result* r);
 
+/* ---- batches of independent problems --------------------------------------- */
+/* No reference counterpart (the reference runs one problem per process): advances
+ * nprob SR objects -- each with its own machine, Hamiltonian and sampler, normally
+ * each on its own context -- by one RunRBM iteration (Runners/RunRBM.hpp:166-214,
+ * LLT solver) per yq_batch_iteration.  The first call (and any call whose
+ * parameters other than epoch/reinit change) runs eagerly and captures the next
+ * iteration of all problems into one CUDA graph on ctx's stream; later calls
+ * replay it, advancing the epoch by one per call from the capturing call's epoch
+ * and keeping the chains.  Problem k samples with seed + k.  results: nprob
+ * entries; the call fails with the first problem's error code if any failed. */
+typedef struct yq_batch_s* yq_batch;
+int yq_batch_create(yq_ctx ctx, int nprob, const yq_sr* srs, yq_batch* out);
+int yq_batch_iteration(yq_batch B, const yq_iter_params* p, yq_iter_result* results);
+int yq_batch_destroy(yq_batch B);
+
 #ifdef __cplusplus
 }
 #endif

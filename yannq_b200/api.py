@@ -83,6 +83,9 @@ SIGNATURES = {
     "yq_sampler_put_samples": [_vp, _i, _vp, _vp],
     "yq_sampler_sample_exact": [_vp, _i, _u64, _u32, _vp],
     "yq_exact": [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp],
+    "yq_batch_create": [_vp, _i, _vp, _vp],
+    "yq_batch_iteration": [_vp, _vp, _vp],
+    "yq_batch_destroy": [_vp],
     "yq_sr_create": [_vp, _vp, _vp, _i, _i, _vp],
     "yq_sr_destroy": [_vp],
     "yq_sr_construct": [_vp],
@@ -413,6 +416,29 @@ class SR:
         r = IterResult()
         check(lib().yq_vmc_iteration(self.h, C.byref(p), C.byref(r)))
         return r
+
+
+class Batch:
+    """Independent SR problems advanced together; calls after the first replay one
+    captured CUDA graph (yq_batch_* in include/yannq_b200.h)."""
+
+    def __init__(self, ctx, srs):
+        self.srs = list(srs)
+        arr = (C.c_void_p * len(self.srs))(*[s.h.value if isinstance(s.h, C.c_void_p) else s.h for s in self.srs])
+        h = C.c_void_p()
+        check(lib().yq_batch_create(ctx.h, len(self.srs), arr, C.byref(h)))
+        self.h = h
+
+    def iteration(self, n_sweeps, n_discard, seed, epoch, shift, lr, reinit=True, ir_steps=0):
+        p = IterParams(n_sweeps, n_discard, int(reinit), seed, epoch, shift, lr, SOLVE_LLT, 1e-4, ir_steps)
+        res = (IterResult * len(self.srs))()
+        check(lib().yq_batch_iteration(self.h, C.byref(p), res))
+        return list(res)
+
+    def close(self):
+        if self.h:
+            check(lib().yq_batch_destroy(self.h))
+            self.h = None
 
 
 class FeedForward:

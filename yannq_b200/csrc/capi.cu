@@ -113,9 +113,10 @@ void raise_device_status(yq_ctx_s* ctx) {
 
 // ---------------------------------------------------------------------------
 void yq_ctx_s::stage_begin(int s) {
-    cudaEventRecord(ev_start[s], stream);
+    if (timing) cudaEventRecord(ev_start[s], stream);
 }
 void yq_ctx_s::stage_end(int s) {
+    if (!timing) return;
     cudaEventRecord(ev_stop[s], stream);
     ev_used[s] = true;
 }
@@ -786,6 +787,40 @@ int yq_vmc_iteration(yq_sr sr, const yq_iter_params* p, yq_iter_result* r) {
         int code = status_to_code(ctx->read_status_and_clear());
         r->status = code;
         if (code != YQ_OK) throw Error(code, status_msg(code));
+    });
+}
+
+int yq_batch_create(yq_ctx ctx, int nprob, const yq_sr* srs, yq_batch* out) {
+    return guard([&] {
+        need(ctx, "ctx");
+        need(srs, "srs");
+        need(out, "out");
+        *out = nullptr;
+        batch_create(ctx, nprob, srs, out);
+    });
+}
+
+int yq_batch_destroy(yq_batch B) {
+    return guard([&] {
+        if (!B) return;
+        YQ_CUDA(cudaStreamSynchronize(B->ctx->stream));
+        batch_destroy(B);
+    });
+}
+
+int yq_batch_iteration(yq_batch B, const yq_iter_params* p, yq_iter_result* results) {
+    return guard([&] {
+        need(B, "batch");
+        need(p, "params");
+        need(results, "results");
+        std::memset(results, 0, B->srs.size() * sizeof(yq_iter_result));
+        batch_iteration(B, *p, results);
+        int first = YQ_OK;
+        for (size_t k = 0; k < B->srs.size(); ++k) {
+            results[k].status = status_to_code(results[k].status);
+            if (first == YQ_OK) first = results[k].status;
+        }
+        if (first != YQ_OK) throw Error(first, status_msg(first));
     });
 }
 

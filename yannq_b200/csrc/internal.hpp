@@ -26,6 +26,7 @@ struct yq_ctx_s {
     bool ev_used[yq::ST_COUNT] = {};
     yq::DevBuf status;  // int device status word
     yq::DevBuf scratch; // small reduction scratch (doubles)
+    bool timing = true; // stage events recorded (off while a batch graph is captured)
 
     void stage_begin(int s);
     void stage_end(int s);
@@ -63,6 +64,7 @@ struct yq_sampler_s {
     yq::DevBuf acc;      // n_chains u64
     int ns = 0;
     uint64_t proposals = 0;  // per chain, last call
+    const uint32_t* epoch_dev = nullptr;  // device epoch offset added to the call's epoch (batched graphs)
 };
 
 // FeedForward machine Conv1D(1 -> C, kernel K, periodic, no bias) -> LnCosh ->
@@ -108,6 +110,30 @@ struct yq_sr_s {
     double host_stats[8] = {};
 };
 
+// A batch of SR problems advanced together (batch.cu).
+struct yq_batch_s {
+    yq_ctx_s* ctx = nullptr;
+    std::vector<yq_sr_s*> srs;
+    yq::DevBuf epoch;  // uint32 device epoch offset
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> joins;
+    yq_iter_params captured{};
+    bool have_graph = false;
+    std::vector<double> host_stats;
+    std::vector<unsigned long long> host_acc;
+    yq::DevBuf dev_acc_sum;  // per problem accepted proposals (u64)
+
+    ~yq_batch_s() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (fork) cudaEventDestroy(fork);
+        for (auto e : joins)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
 namespace yq {
 // kernels launched from the objects (defined in the .cu files)
 void rbm_prepare(yq_rbm_s* q);
@@ -127,6 +153,9 @@ void sr_construct(yq_sr_s* sr);
 void exact_summation(yq_rbm_s* q, yq_ham_s* H, int kind, int nup, double* stats, c128* d_oloc, c128* d_grad,
                      c128* d_S);
 void sampler_sample_exact(yq_sampler_s* S, int ns, uint64_t seed, uint32_t epoch, uint64_t* d_pos);
+void batch_create(yq_ctx_s* ctx, int np, yq_sr_s* const* srs, yq_batch_s** out);
+void batch_destroy(yq_batch_s* B);
+void batch_iteration(yq_batch_s* B, const yq_iter_params& p, yq_iter_result* res);
 void sr_solve(yq_sr_s* sr, double shift, int solver, double cg_tol, int ir_steps, int* iters, double* relres);
 void sr_update_params(yq_sr_s* sr, double lr);
 void sr_form_matrix_public(yq_sr_s* sr, double shift);

@@ -26,6 +26,7 @@ struct SampArgs {
     bool bias;
     uint64_t seed;
     uint32_t epoch;
+    const uint32_t* epoch_dev;  // optional device-side epoch offset (graph replays)
     const c128* p64;
     const cplx<R>* W;
     const cplx<R>* tau;
@@ -90,6 +91,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     const int c = blockIdx.x * (blockDim.x >> 5) + warp;
     if (c >= A.n_chains) return;  // warp-uniform
     const int n = A.n, m = A.m;
+    const uint32_t epoch = A.epoch_dev ? A.epoch + *A.epoch_dev : A.epoch;
     int8_t* s = smem_sig + warp * A.nstride;
     int8_t* cs = A.chains + size_t(c) * n;
 
@@ -97,14 +99,14 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     if (A.reinit) {
         if (A.nup < 0) {
             for (int i = lane; i < n; i += 32) {
-                U4 x = draw(A.seed, uint32_t(i), A.epoch, uint32_t(c), TAG_INIT);
+                U4 x = draw(A.seed, uint32_t(i), epoch, uint32_t(c), TAG_INIT);
                 s[i] = (x.x & 1u) ? int8_t(-1) : int8_t(1);
             }
         } else {
             if (lane == 0) {
                 for (int i = 0; i < n; ++i) s[i] = (i < A.nup) ? int8_t(-1) : int8_t(1);
                 for (int i = n - 1; i >= 1; --i) {
-                    U4 x = draw(A.seed, uint32_t(i), A.epoch, uint32_t(c), TAG_SHUF);
+                    U4 x = draw(A.seed, uint32_t(i), epoch, uint32_t(c), TAG_SHUF);
                     int j = int(draw_site(x.x, uint32_t(i + 1)));
                     int8_t tmp = s[i];
                     s[i] = s[j];
@@ -129,7 +131,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
 
     // prefetch of the first proposal's columns
     {
-        U4 x0 = draw(A.seed, 0u, A.epoch, uint32_t(c), TAG_SWEEP);
+        U4 x0 = draw(A.seed, 0u, epoch, uint32_t(c), TAG_SWEEP);
         int k0 = int(draw_site(x0.x, uint32_t(n)));
 #pragma unroll
         for (int r = 0; r < JPL; ++r) {
@@ -144,10 +146,10 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     for (int sw = 0; sw < A.n_total; ++sw) {
         for (uint32_t p = 0; p < L; ++p) {
             const uint32_t g = uint32_t(sw) * L + p;
-            U4 x = draw(A.seed, g, A.epoch, uint32_t(c), TAG_SWEEP);
+            U4 x = draw(A.seed, g, epoch, uint32_t(c), TAG_SWEEP);
             // prefetch the next proposal's columns into L1
             {
-                U4 xn = draw(A.seed, g + 1u, A.epoch, uint32_t(c), TAG_SWEEP);
+                U4 xn = draw(A.seed, g + 1u, epoch, uint32_t(c), TAG_SWEEP);
                 int kn = int(draw_site(xn.x, uint32_t(n)));
                 int ln = (MOVE == YQ_MOVE_EXCHANGE_ANY) ? int(draw_site(xn.y, uint32_t(n))) : (kn + 1) % n;
 #pragma unroll
@@ -338,6 +340,7 @@ static void run_t(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, u
     A.bias = q->use_bias;
     A.seed = seed;
     A.epoch = epoch;
+    A.epoch_dev = S->epoch_dev;
     A.p64 = q->p64.as<c128>();
     A.W = q->W.as<cplx<R>>();
     A.tau = q->tau.as<cplx<R>>();
