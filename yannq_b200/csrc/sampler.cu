@@ -129,10 +129,29 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     const R two = R(2);
     constexpr int G = LogGroup<R>::G;
 
-    // prefetch of the first proposal's columns
-    {
-        U4 x0 = draw(A.seed, 0u, epoch, uint32_t(c), TAG_SWEEP);
-        int k0 = int(draw_site(x0.x, uint32_t(n)));
+    // The proposal sites do not depend on acceptance, so the next proposal's draw
+    // and (local moves) its tau and W columns and L_k, a_k are loaded into
+    // registers one proposal ahead; exchange moves prefetch their two columns
+    // into L1.
+    // (register pipelining for complex64 only: complex128 would spill)
+    constexpr bool REGPIPE = MOVE == YQ_MOVE_LOCAL && sizeof(R) == 4;
+    U4 xcur = draw(A.seed, 0u, epoch, uint32_t(c), TAG_SWEEP);
+    cplx<R> tvn[JPL], wvn[JPL];
+    double lkn = 0., abn = 0.;
+    auto load_cols = [&](int kq) {
+#pragma unroll
+        for (int r = 0; r < JPL; ++r) {
+            const int j = lane + 32 * r;
+            tvn[r] = j < m ? A.tau[size_t(kq) * m + j] : mk(R(0), R(0));
+            wvn[r] = j < m ? A.W[size_t(kq) * m + j] : mk(R(0), R(0));
+        }
+        lkn = A.Lk[kq].re;
+        abn = A.bias ? A.p64[size_t(n) * m + kq].re : 0.0;
+    };
+    if (REGPIPE) {
+        load_cols(int(draw_site(xcur.x, uint32_t(n))));
+    } else {
+        const int k0 = int(draw_site(xcur.x, uint32_t(n)));
 #pragma unroll
         for (int r = 0; r < JPL; ++r) {
             int j = lane + 32 * r;
@@ -146,10 +165,11 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     for (int sw = 0; sw < A.n_total; ++sw) {
         for (uint32_t p = 0; p < L; ++p) {
             const uint32_t g = uint32_t(sw) * L + p;
-            U4 x = draw(A.seed, g, epoch, uint32_t(c), TAG_SWEEP);
-            // prefetch the next proposal's columns into L1
-            {
-                U4 xn = draw(A.seed, g + 1u, epoch, uint32_t(c), TAG_SWEEP);
+            const U4 x = xcur;
+            const U4 xn = draw(A.seed, g + 1u, epoch, uint32_t(c), TAG_SWEEP);
+            xcur = xn;
+            if (!REGPIPE) {
+                // prefetch the next proposal's columns into L1
                 int kn = int(draw_site(xn.x, uint32_t(n)));
                 int ln = (MOVE == YQ_MOVE_EXCHANGE_ANY) ? int(draw_site(xn.y, uint32_t(n))) : (kn + 1) % n;
 #pragma unroll
@@ -169,20 +189,36 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
             const int k = int(draw_site(x.x, uint32_t(n)));
             if (MOVE == YQ_MOVE_LOCAL) {
                 const R sk = R(s[k]);
-                const cplx<R>* tk = A.tau + size_t(k) * m;
                 const cplx<R>* wk = A.W + size_t(k) * m;
-                cplx<R> tv[JPL], d[JPL];
+                cplx<R> tv[JPL], wv[JPL], d[JPL];
+                double lk, ab;
+                if (REGPIPE) {
+#pragma unroll
+                    for (int r = 0; r < JPL; ++r) {
+                        tv[r] = tvn[r];
+                        wv[r] = wvn[r];
+                    }
+                    lk = lkn;
+                    ab = abn;
+                    load_cols(int(draw_site(xn.x, uint32_t(n))));  // next proposal, in flight meanwhile
+                } else {
+#pragma unroll
+                    for (int r = 0; r < JPL; ++r) {
+                        const int j = lane + 32 * r;
+                        tv[r] = j < m ? A.tau[size_t(k) * m + j] : mk(R(0), R(0));
+                    }
+                    lk = A.Lk[k].re;
+                    ab = A.bias ? A.p64[size_t(n) * m + k].re : 0.0;
+                }
                 unsigned exact = 0u;  // bit r: factor r re-evaluated in logcosh form (ratio.cuh)
 #pragma unroll
                 for (int r = 0; r < JPL; ++r) {
                     int j = lane + 32 * r;
                     if (j < m) {
-                        tv[r] = tk[j];
                         bool ex;
-                        d[r] = factor1<R>(t[r], tv[r], sk, th[r], wk + j, ex);
+                        d[r] = factor1<R>(t[r], tv[r], sk, th[r], REGPIPE ? &wv[r] : wk + j, ex);
                         exact |= unsigned(ex) << r;
                     } else {
-                        tv[r] = mk(R(0), R(0));
                         d[r] = one<R>();
                     }
                 }
@@ -197,8 +233,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                     }
                 }
                 ls = warp_allsum(ls);
-                double base = A.Lk[k].re;
-                if (A.bias) base -= 2.0 * double(sk) * A.p64[size_t(n) * m + k].re;
+                const double base = lk - 2.0 * double(sk) * ab;
                 const R logr = R(0.5) * ls + R(base);
                 // LocalSweeper.hpp:45-47: p = min(1, exp(beta * 2 * Re logRatio)); accept if u < p
                 if (u < exp(two * logr)) {
@@ -206,7 +241,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                     for (int r = 0; r < JPL; ++r) {
                         int j = lane + 32 * r;
                         if (j < m) {
-                            cplx<R> w = wk[j];
+                            const cplx<R> w = REGPIPE ? wv[r] : wk[j];
                             th[r] = th[r] - (two * sk) * w;
                             t[r] = ((exact >> r) & 1u) ? ctanh(th[r]) : cdiv(t[r] - sk * tv[r], d[r]);
                         }
