@@ -1,6 +1,6 @@
 // Persistent tile Cholesky and triangular solves (FP64, complex, lower, in place).
 //
-// One cooperative launch with one CTA per SM factors the whole matrix.  Tiles of
+// One launch with at most one CTA per SM factors the whole matrix.  Tiles of
 // 64 x 64 are numbered column by column (diagonal tile first in each column) and
 // handed out in that order by an atomic counter; tile (i, j) computes
 //   F = A_ij - sum_{k<j} L_ik L_jk^H          (DMMA m8n8k4, operands staged by cp.async)
@@ -412,8 +412,20 @@ struct SolveArgs {
     const c128* LinvH;
     c128* b;    // in: right-hand side; forward result written here per block
     int* flags; // nt
+    int* counter;  // block rows are claimed in sweep order from this counter
     Sync S;
 };
+
+// Next block row of the sweep for this CTA (nt when done or aborted).  Rows are
+// claimed in order by running CTAs only, so a row's wait is always on rows held
+// by CTAs that are already running: no co-residency is needed.
+__device__ __forceinline__ int claim_row(const SolveArgs& a, int* s_row) {
+    if (threadIdx.x == 0) *s_row = ld_acquire(a.S.abort_word) ? a.nt : atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int t = *s_row;
+    __syncthreads();
+    return t;
+}
 
 // Solve sweeps.  One CTA per 64-row block (persistent over blocks r = blockIdx.x,
 // + gridDim.x, ...).  The L tiles a block needs do not depend on the sweep, so they
@@ -438,9 +450,9 @@ __global__ void __launch_bounds__(128, 1) chol_fwd_tile_kernel(SolveArgs a) {
     c128* Li = buf + 2 * TB * SLD;             // diagonal inverse
     c128* xk = Li + TB * SLD;                  // published block
     c128* acc = xk + TB;
-    __shared__ int s_ok;
+    __shared__ int s_ok, s_row;
     const int tid = threadIdx.x, row = tid >> 1, half = tid & 1;
-    for (int r = blockIdx.x; r < a.nt; r += gridDim.x) {
+    for (int r = claim_row(a, &s_row); r < a.nt; r = claim_row(a, &s_row)) {
         stage_tile(Li, a.Linv + size_t(r) * TB * TB, TB);
         cpa_commit();
         if (r > 0) stage_tile(buf, a.G + size_t(r) * TB * a.ld, a.ld);
@@ -486,9 +498,9 @@ __global__ void __launch_bounds__(128, 1) chol_bwd_tile_kernel(SolveArgs a) {
     c128* Li = buf + 2 * TB * SLD;
     c128* zk = Li + TB * SLD;
     c128* acc = zk + TB;
-    __shared__ int s_ok;
+    __shared__ int s_ok, s_row;
     const int tid = threadIdx.x, col = tid >> 1, half = tid & 1;
-    for (int t = blockIdx.x; t < a.nt; t += gridDim.x) {
+    for (int t = claim_row(a, &s_row); t < a.nt; t = claim_row(a, &s_row)) {
         const int r = a.nt - 1 - t;
         stage_tile(Li, a.LinvH + size_t(r) * TB * TB, TB);
         cpa_commit();
@@ -542,7 +554,8 @@ int coresident_blocks(const void* fn, int threads, size_t smem, int sm_count) {
 }  // namespace
 
 // Scratch layout (ints): [0] tile counter of the full factorisation, [1] abort word
-// of the factorisation, [2] abort word of the solves, [16 .. 16 + nt) tile counters
+// of the factorisation, [2] abort word of the solves, [3] / [4] block-row counters
+// of the forward / backward sweeps, [16 .. 16 + nt) tile counters
 // of the panels, then the tile flags (nt x nt), the solve flags (2 nt), and the
 // 16-byte aligned tile list.
 struct Scratch {
@@ -586,12 +599,12 @@ static int tile_grid() {
     return per_sm;
 }
 
+// Ordinary launch: tiles are handed out by the counter to running CTAs only, so the
+// grid needs no co-residency and can share the device with other work.  Small
+// matrices get a grid proportional to their tile columns.
 static void launch_tiles(const TileArgs& a, int nitems, int sm_count, cudaStream_t st) {
-    const int grid = std::min(tile_grid() * sm_count, std::max(1, nitems));
-    TileArgs copy = a;
-    void* args[] = {&copy};
-    YQ_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(chol_tile_kernel), dim3(grid), dim3(128), args,
-                                        SM_TILE, st));
+    const int grid = std::min({tile_grid() * sm_count, std::max(1, nitems), std::max(8, 4 * a.nt)});
+    chol_tile_kernel<<<grid, 128, SM_TILE, st>>>(a);
     YQ_LAUNCH_CHECK();
 }
 
@@ -648,7 +661,7 @@ void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c
     int* words = sc.words;
     int* sflags = sc.sflags;
     YQ_CUDA(cudaMemsetAsync(sflags, 0, 2 * size_t(nt) * sizeof(int), st));
-    YQ_CUDA(cudaMemsetAsync(words + 2, 0, sizeof(int), st));  // abort word of the solves
+    YQ_CUDA(cudaMemsetAsync(words + 2, 0, 3 * sizeof(int), st));  // abort word and row counters of the solves
     static bool attr = false;
     if (!attr) {
         YQ_CUDA(cudaFuncSetAttribute(chol_fwd_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SM_SOLVE)));
@@ -659,15 +672,11 @@ void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c
                                                       SM_SOLVE, sm_count));
     const int grid_b = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_bwd_tile_kernel), 128,
                                                       SM_SOLVE, sm_count));
-    SolveArgs fa{G, ld, nt, Linv, LinvH, b, sflags, Sync{status, words + 2, 1u << 24}};
-    void* fargs[] = {&fa};
-    YQ_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(chol_fwd_tile_kernel), dim3(grid_f), dim3(128),
-                                        fargs, SM_SOLVE, st));
+    SolveArgs fa{G, ld, nt, Linv, LinvH, b, sflags, words + 3, Sync{status, words + 2, 1u << 24}};
+    chol_fwd_tile_kernel<<<grid_f, 128, SM_SOLVE, st>>>(fa);
     YQ_LAUNCH_CHECK();
-    SolveArgs ba{G, ld, nt, Linv, LinvH, b, sflags + nt, Sync{status, words + 2, 1u << 24}};
-    void* bargs[] = {&ba};
-    YQ_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(chol_bwd_tile_kernel), dim3(grid_b), dim3(128),
-                                        bargs, SM_SOLVE, st));
+    SolveArgs ba{G, ld, nt, Linv, LinvH, b, sflags + nt, words + 4, Sync{status, words + 2, 1u << 24}};
+    chol_bwd_tile_kernel<<<grid_b, 128, SM_SOLVE, st>>>(ba);
     YQ_LAUNCH_CHECK();
     if (out != b) YQ_CUDA(cudaMemcpyAsync(out, b, size_t(n) * sizeof(c128), cudaMemcpyDeviceToDevice, st));
 }
