@@ -181,6 +181,7 @@ def _run_precision(api, ctx, precision, steps, warmup, pg, device, with_e2e):
         out["h2d_bytes"] = q.dim * 16
         out["d2h_bytes"] = q.dim * 16 + 8 * 8 + W["chains"] * 8
         pin.free()
+    out["chains_per_cta"] = S.chains_per_cta()  # the sampler autotuner's choice
     for x in (sr, S, H, q):
         x.close()
     return out
@@ -440,7 +441,8 @@ def main():
                        W["alpha"] * W["lx"] * W["ly"], "P": P, "Ns": Ns, "chains": W["chains"],
                        "sweeps": f"{W['n_discard']} discard + {W['n_sweeps']} recorded per step, {W['therm']} therm",
                        "sr": "T-form, shift 1e-3, Cholesky", "parallelism": f"replicas{ws}",
-                       "inputs": "larger than L2 (O~ and operands >= 2.7 GB)"},
+                       "inputs": "larger than L2 (O~ and operands >= 2.7 GB)",
+                       "sampler_chains_per_cta": head.get("chains_per_cta")},
             "gpu_launches": head["launches"], "clocks": head["clocks"], "roofline": roof,
             "stages_ms": head["stages_ms"], "energy_per_site": head["energy_per_site"], "device_peaks": dev_peaks,
             "accept_rate": head["accept_rate"]}

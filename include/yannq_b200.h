@@ -157,6 +157,11 @@ int yq_sample(yq_sampler S, int n_sweeps, int n_discard, uint64_t seed, uint32_t
 int yq_sampler_num_samples(yq_sampler S, int* ns);
 /* Copy the last samples to the host: sigma ns x n int8, theta ns x m complex (may be null). */
 int yq_sampler_get_samples(yq_sampler S, int8_t* sigma, double* theta);
+/* No reference counterpart: chains per CTA (warps per block) that the sampler's
+ * autotuner chose for the configuration of the last yq_sample (0 before any).  The
+ * choice is timed once per configuration per process (1, 2 or 4); YQ_AUTOTUNE=0
+ * in the environment fixes it at 4. */
+int yq_sampler_chains_per_cta(yq_sampler S, int* out);
 /* Accepted proposals per chain in the last yq_sample (LocalSweeper::sweep's return). */
 int yq_sampler_get_accepts(yq_sampler S, uint64_t* acc);
 /* Replace the device samples by host ones (for SR on externally supplied samples). */

@@ -207,3 +207,25 @@ def test_vmc_converges_towards_ed(ctx, orc):
     es = [sr.iteration(16, 16, 3, it, 1e-3, 0.05).energy for it in range(60)]
     assert np.mean(es[-10:]) < es[0]
     assert abs(np.mean(es[-10:]) - e0) / abs(e0) < 0.02
+
+
+def test_sampler_autotuned_launch_shape(ctx, orc):
+    """The autotuner picks 1, 2 or 4 chains per CTA once per configuration; a
+    second sampler with the same configuration reuses the choice, and the chains
+    are the same whatever the choice (each warp owns one chain)."""
+    from yannq_b200 import api
+
+    n, m, chains = 10, 20, 48
+    p = orc.init_params(n, m, 3, 0.1)
+    out = []
+    for _ in range(2):
+        q = api.RBM(ctx, n, m, True, api.C128)
+        q.set_params(p)
+        S = api.Sampler(q, chains)
+        S.sample(4, 4, seed=9, epoch=0, reinit=True)
+        out.append((S.chains_per_cta(), S.get_samples()[0]))
+        S.close()
+        q.close()
+    assert out[0][0] in (1, 2, 4)
+    assert out[1][0] == out[0][0]
+    assert np.array_equal(out[0][1], out[1][1])

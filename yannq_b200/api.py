@@ -82,6 +82,7 @@ SIGNATURES = {
     "yq_sampler_get_accepts": [_vp, _vp],
     "yq_sampler_put_samples": [_vp, _i, _vp, _vp],
     "yq_sampler_sample_exact": [_vp, _i, _u64, _u32, _vp],
+    "yq_sampler_chains_per_cta": [_vp, _vp],
     "yq_exact": [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp],
     "yq_batch_create": [_vp, _i, _vp, _vp],
     "yq_batch_iteration": [_vp, _vp, _vp],
@@ -352,6 +353,11 @@ class Sampler:
         th = np.zeros((ns, self.rbm.m), np.complex128) if theta else None
         check(lib().yq_sampler_get_samples(self.h, _p(s), _p(th)))
         return s, th
+
+    def chains_per_cta(self):
+        v = C.c_int()
+        check(lib().yq_sampler_chains_per_cta(self.h, C.byref(v)))
+        return v.value
 
     def get_accepts(self):
         out = np.zeros(self.n_chains, np.uint64)

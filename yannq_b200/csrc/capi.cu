@@ -588,6 +588,14 @@ int yq_sampler_get_accepts(yq_sampler S, uint64_t* acc) {
     });
 }
 
+int yq_sampler_chains_per_cta(yq_sampler S, int* out) {
+    return guard([&] {
+        need(S, "sampler");
+        need(out, "out");
+        *out = S->chains_per_cta;
+    });
+}
+
 int yq_sampler_sample_exact(yq_sampler S, int ns, uint64_t seed, uint32_t epoch, uint64_t* positions) {
     return guard([&] {
         need(S, "sampler");

@@ -65,6 +65,7 @@ struct yq_sampler_s {
     int ns = 0;
     uint64_t proposals = 0;  // per chain, last call
     const uint32_t* epoch_dev = nullptr;  // device epoch offset added to the call's epoch (batched graphs)
+    int chains_per_cta = 0;               // autotuned launch shape of the last sample call
 };
 
 // FeedForward machine Conv1D(1 -> C, kernel K, periodic, no bias) -> LnCosh ->

@@ -15,6 +15,12 @@
 //
 // Random numbers: Philox4x32-10 with counter (proposal, epoch, chain, tag); the
 // next proposal's columns are prefetched into L1 while the current one is scored.
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
 #include "internal.hpp"
 #include "ratio.cuh"
 
@@ -337,21 +343,103 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
 }
 
 template <typename R, int MOVE, int JPL>
-static void launch_t(const SampArgs<R>& A, cudaStream_t st) {
-    const int warps = 4;
+static void launch_w(const SampArgs<R>& A, int warps, cudaStream_t st) {
     dim3 grid(cdiv_u(A.n_chains, warps));
     size_t smem = size_t(warps) * A.nstride;
     metropolis_kernel<R, MOVE, JPL><<<grid, warps * 32, smem, st>>>(A);
     YQ_LAUNCH_CHECK();
 }
 
+// Autotuned chains per CTA (warps per block).  On the first call of a
+// configuration (type, move, hidden units per lane, n, m, chains, sweep length) the
+// kernel runs two sweeps from a scratch copy of the chains into scratch outputs at
+// 1, 2 and 4 chains per CTA (the kernel's launch bound is 128 threads), timed with
+// CUDA events on the library stream; the
+// fastest is kept for the process.  The chains evolve identically whatever the
+// choice (each warp owns one chain and its own Philox counters).  Calls made while
+// the stream is being captured, and YQ_AUTOTUNE=0, use 4.
+constexpr int N_TUNE = 3;
+struct TuneEntry {
+    int warps;
+    float ms[N_TUNE];
+};
+static std::mutex g_tune_mu;
+static std::map<std::vector<long long>, TuneEntry> g_tune;
+
+template <typename R, int MOVE, int JPL>
+static int tuned_warps(const SampArgs<R>& A, cudaStream_t st) {
+    static const bool enabled = [] {
+        const char* e = std::getenv("YQ_AUTOTUNE");
+        return !(e && std::string(e) == "0");
+    }();
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    YQ_CUDA(cudaStreamIsCapturing(st, &cap));
+    const std::vector<long long> key = {static_cast<long long>(sizeof(R)), MOVE, JPL, A.n, A.m, A.n_chains, A.L};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) return it->second.warps;
+    }
+    if (!enabled || cap != cudaStreamCaptureStatusNone) return 4;
+    DevBuf ch, sg, th, acc;
+    ch.ensure(size_t(A.n_chains) * A.n);
+    sg.ensure(size_t(A.n_chains) * A.n);
+    th.ensure(size_t(A.n_chains) * A.m * sizeof(cplx<R>));
+    acc.ensure(size_t(A.n_chains) * sizeof(unsigned long long));
+    SampArgs<R> T = A;
+    T.chains = ch.as<int8_t>();
+    T.out_sigma = sg.as<int8_t>();
+    T.out_theta = th.as<cplx<R>>();
+    T.acc = acc.as<unsigned long long>();
+    T.n_total = 2;
+    T.n_discard = 1;
+    T.epoch_dev = nullptr;
+    if (!A.reinit)
+        YQ_CUDA(cudaMemcpyAsync(ch.p, A.chains, size_t(A.n_chains) * A.n, cudaMemcpyDeviceToDevice, st));
+    cudaEvent_t e0, e1;
+    YQ_CUDA(cudaEventCreate(&e0));
+    YQ_CUDA(cudaEventCreate(&e1));
+    TuneEntry best{4, {0.f, 0.f, 0.f}};
+    float best_ms = 1e30f;
+    const int cand[N_TUNE] = {1, 2, 4};
+    for (int c = 0; c < N_TUNE; ++c) {
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {  // the first run also warms the caches
+            YQ_CUDA(cudaEventRecord(e0, st));
+            launch_w<R, MOVE, JPL>(T, cand[c], st);
+            YQ_CUDA(cudaEventRecord(e1, st));
+            YQ_CUDA(cudaEventSynchronize(e1));
+            float t = 0.f;
+            YQ_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            ms = std::min(ms, t);
+        }
+        best.ms[c] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best.warps = cand[c];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = best;
+    return best.warps;
+}
+
+template <typename R, int MOVE, int JPL>
+static void launch_t(const SampArgs<R>& A, cudaStream_t st, int* chosen) {
+    const int warps = tuned_warps<R, MOVE, JPL>(A, st);
+    if (chosen) *chosen = warps;
+    launch_w<R, MOVE, JPL>(A, warps, st);
+}
+
 template <typename R, int MOVE>
-static void dispatch_jpl(const SampArgs<R>& A, cudaStream_t st) {
+static void dispatch_jpl(const SampArgs<R>& A, cudaStream_t st, int* chosen) {
     const int need = (A.m + 31) / 32;
-#define YQ_JPL(J)                        \
-    if (need <= J) {                     \
-        launch_t<R, MOVE, J>(A, st);     \
-        return;                          \
+#define YQ_JPL(J)                                \
+    if (need <= J) {                             \
+        launch_t<R, MOVE, J>(A, st, chosen);     \
+        return;                                  \
     }
     YQ_JPL(1) YQ_JPL(2) YQ_JPL(4) YQ_JPL(8) YQ_JPL(9) YQ_JPL(12) YQ_JPL(16) YQ_JPL(32)
 #undef YQ_JPL
@@ -386,9 +474,9 @@ static void run_t(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, u
     A.acc = S->acc.as<unsigned long long>();
     cudaStream_t st = q->ctx->stream;
     switch (S->move) {
-        case YQ_MOVE_LOCAL: dispatch_jpl<R, YQ_MOVE_LOCAL>(A, st); break;
-        case YQ_MOVE_EXCHANGE_ANY: dispatch_jpl<R, YQ_MOVE_EXCHANGE_ANY>(A, st); break;
-        default: dispatch_jpl<R, YQ_MOVE_EXCHANGE_NN>(A, st); break;
+        case YQ_MOVE_LOCAL: dispatch_jpl<R, YQ_MOVE_LOCAL>(A, st, &S->chains_per_cta); break;
+        case YQ_MOVE_EXCHANGE_ANY: dispatch_jpl<R, YQ_MOVE_EXCHANGE_ANY>(A, st, &S->chains_per_cta); break;
+        default: dispatch_jpl<R, YQ_MOVE_EXCHANGE_NN>(A, st, &S->chains_per_cta); break;
     }
 }
 
