@@ -157,6 +157,17 @@ int yq_sample(yq_sampler S, int n_sweeps, int n_discard, uint64_t seed, uint32_t
 int yq_sampler_num_samples(yq_sampler S, int* ns);
 /* Copy the last samples to the host: sigma ns x n int8, theta ns x m complex (may be null). */
 int yq_sampler_get_samples(yq_sampler S, int8_t* sigma, double* theta);
+/* SamplerMT(qs, nTmps, nChainsPer, sweeper) with nTmps > 1 -- Samplers/SamplerMT.hpp:
+ * 44-60, 120-204: the sampler's n_chains = nTmps x nChainsPer chains form groups of
+ * ntemps consecutive chains with betas (nTmps - t) / nTmps; every sweep each chain
+ * sweeps at its beta, then mixChains swaps temperatures between neighbouring
+ * slots of a group (even pairs, then odd pairs; u from the parallel-tempering
+ * Philox stream), and recorded sweeps keep the beta = 1 chain of every group, so a
+ * sample call returns nChainsPer x n_sweeps samples.  ntemps = 1 (default) is the
+ * plain sampler.  The ladder positions persist across calls (reset by reinit). */
+int yq_sampler_set_tempering(yq_sampler S, int ntemps);
+/* Ladder slot of every chain (0 = beta 1), n_chains entries. */
+int yq_sampler_get_slots(yq_sampler S, int* slots);
 /* No reference counterpart: chains per CTA (warps per block) that the sampler's
  * autotuner chose for the configuration of the last yq_sample (0 before any).  The
  * choice is timed once per configuration per process (1, 2 or 4); YQ_AUTOTUNE=0

@@ -196,6 +196,87 @@ void sample(const RBM& q, const SampleSpec& sp, int8_t* chain_sigma, int8_t* out
     }
 }
 
+void sample_pt(const RBM& q, const SampleSpec& sp, int ntemps, int8_t* chain_sigma, int* slot, int8_t* out_sigma,
+               cd* out_theta, uint64_t* acc, int nthreads) {
+    const int n = q.n, m = q.m, nc = sp.n_chains, groups = nc / ntemps;
+    const int L = sp.sweep_len > 0 ? sp.sweep_len : n;
+    const int total = sp.n_discard + sp.n_sweeps;
+    const int nt = nthreads_or_default(nthreads);
+    std::vector<int8_t> s(size_t(nc) * n);
+    std::vector<cd> th(size_t(nc) * m);
+    std::vector<double> lp(nc);
+    std::vector<uint64_t> nacc(nc, 0);
+    for (int c = 0; c < nc; ++c) {
+        int8_t* sc = s.data() + size_t(c) * n;
+        if (sp.reinit) {
+            random_sigma(n, sp.nup, sp.seed, sp.epoch, uint32_t(c), sc);
+            slot[c] = c % ntemps;
+        } else {
+            std::copy(chain_sigma + size_t(c) * n, chain_sigma + size_t(c + 1) * n, sc);
+        }
+        q.theta(sc, th.data() + size_t(c) * m);
+    }
+    auto beta_of = [&](int t) { return double(ntemps - t) / double(ntemps); };
+    for (int sw = 0; sw < total; ++sw) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+        for (int c = 0; c < nc; ++c) {
+            int8_t* sc = s.data() + size_t(c) * n;
+            cd* tc = th.data() + size_t(c) * m;
+            const double beta = beta_of(slot[c]);
+            uint32_t x[4];
+            for (int p = 0; p < L; ++p) {
+                const uint32_t g = uint32_t(sw) * uint32_t(L) + uint32_t(p);
+                Philox4x32::draw(sp.seed, g, sp.epoch, uint32_t(c), TAG_SWEEP, x);
+                const double u = draw_u53(x[2], x[3]);
+                if (sp.move == MOVE_LOCAL) {
+                    int k = int(draw_site(x[0], uint32_t(n)));
+                    double pr = std::min(1.0, std::exp(beta * 2.0 * q.logRatio1(sc, tc, k).real()));
+                    if (u < pr) {
+                        q.flip1(sc, tc, k);
+                        ++nacc[c];
+                    }
+                } else {
+                    int k = int(draw_site(x[0], uint32_t(n)));
+                    int l = (sp.move == MOVE_EXCHANGE_ANY) ? int(draw_site(x[1], uint32_t(n))) : (k + 1) % n;
+                    if (sc[k] == sc[l]) continue;
+                    double pr = std::min(1.0, std::exp(beta * 2.0 * q.logRatio2(sc, tc, k, l).real()));
+                    if (u < pr) {
+                        q.flip2(sc, tc, k, l);
+                        ++nacc[c];
+                    }
+                }
+            }
+            lp[c] = q.logCoeff(sc, tc).real();
+        }
+        // mixChains (SamplerMT.hpp:120-153)
+        for (int gr = 0; gr < groups; ++gr) {
+            std::vector<int> at(ntemps);
+            for (int k = 0; k < ntemps; ++k) at[size_t(slot[gr * ntemps + k])] = gr * ntemps + k;
+            auto attempt = [&](int t) {
+                const int a = at[size_t(t)], b = at[size_t(t + 1)];
+                const double pr = std::exp((beta_of(t + 1) - beta_of(t)) * 2.0 * (lp[a] - lp[b]));
+                uint32_t x[4];
+                Philox4x32::draw(sp.seed, uint32_t(sw) * 64u + uint32_t(t), sp.epoch, uint32_t(gr), TAG_PT, x);
+                if (draw_u53(x[2], x[3]) < pr) std::swap(at[size_t(t)], at[size_t(t + 1)]);
+            };
+            for (int t = 0; t + 1 < ntemps; t += 2) attempt(t);
+            for (int t = 1; t + 1 < ntemps - 1; t += 2) attempt(t);
+            for (int t = 0; t < ntemps; ++t) slot[at[size_t(t)]] = t;
+        }
+        if (sw >= sp.n_discard) {
+            for (int c = 0; c < nc; ++c) {
+                if (slot[c] != 0) continue;
+                const size_t idx = size_t(sw - sp.n_discard) * groups + c / ntemps;
+                std::copy(s.begin() + size_t(c) * n, s.begin() + size_t(c + 1) * n, out_sigma + idx * n);
+                std::copy(th.begin() + size_t(c) * m, th.begin() + size_t(c + 1) * m, out_theta + idx * m);
+            }
+        }
+    }
+    std::copy(s.begin(), s.end(), chain_sigma);
+    if (acc)
+        for (int c = 0; c < nc; ++c) acc[c] = nacc[c];
+}
+
 // ---------------------------------------------------------------------------
 int cholesky_lower(int nn, cd* A) {
     for (int j = 0; j < nn; ++j) {

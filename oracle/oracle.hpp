@@ -187,6 +187,19 @@ struct SampleSpec {
     int sweep_len = 0;     // proposals per sweep (0 -> n, LocalSweeper nSweep_=1)
 };
 void random_sigma(int n, int nup, uint64_t seed, uint32_t epoch, uint32_t chain, int8_t* s);
+// SamplerMT with nTmps = ntemps > 1 (Samplers/SamplerMT.hpp:44-60, :120-204): chain c
+// belongs to group c / ntemps; slot[c] is its place in the group's ladder, beta =
+// (ntemps - slot) / ntemps.  Every sweep: each chain sweeps at its beta (proposal
+// draws as in `sample`), then mixChains per group -- even slot pairs (0,1),(2,3),...
+// then odd pairs (1,2),...,(ntemps-3, ntemps-2) -- accepts a swap with
+// p = exp((beta_{t+1} - beta_t) 2 (Re log psi(slot t) - Re log psi(slot t+1))) and
+// u from counter (64 sweep + t, epoch, group, TAG_PT); swapping exchanges the two
+// chains' slots (temperatures) instead of their states.  Recorded sweeps append
+// the slot-0 chain of every group: output row (sweep - n_discard) groups + group.
+// The chain state (sigma, theta) carries over exactly from sweep to sweep; slot
+// is in/out (reset to c % ntemps when sp.reinit).
+void sample_pt(const RBM& q, const SampleSpec& sp, int ntemps, int8_t* chain_sigma, int* slot, int8_t* out_sigma,
+               cd* out_theta, uint64_t* acc, int nthreads);
 // chain_sigma: n_chains x n, in/out.  Outputs sample-major (sweep, chain).
 void sample(const RBM& q, const SampleSpec& sp, int8_t* chain_sigma, int8_t* out_sigma, cd* out_theta,
             uint64_t* acc, int nthreads);

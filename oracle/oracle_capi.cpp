@@ -154,6 +154,24 @@ void orc_sample(int n, int m, int use_bias, const double* params, int n_chains, 
     sample(q, sp, chain_sigma, out_sigma, reinterpret_cast<cd*>(out_theta), acc, nthreads);
 }
 
+void orc_sample_pt(int n, int m, int use_bias, const double* params, int n_chains, int ntemps, int move, int nup,
+                   uint64_t seed, uint32_t epoch, int reinit, int n_sweeps, int n_discard, int sweep_len,
+                   int8_t* chain_sigma, int* slot, int8_t* out_sigma, double* out_theta, uint64_t* acc,
+                   int nthreads) {
+    RBM q = make_rbm(n, m, use_bias, params);
+    SampleSpec sp;
+    sp.n_chains = n_chains;
+    sp.move = move;
+    sp.nup = nup;
+    sp.seed = seed;
+    sp.epoch = epoch;
+    sp.reinit = reinit;
+    sp.n_sweeps = n_sweeps;
+    sp.n_discard = n_discard;
+    sp.sweep_len = sweep_len;
+    sample_pt(q, sp, ntemps, chain_sigma, slot, out_sigma, reinterpret_cast<cd*>(out_theta), acc, nthreads);
+}
+
 // One SR step on given samples.  out_v/out_grad/out_oloc: P complex; out_eloc: ns complex;
 // out_stats: [energy, energy_var, cg_iters, cg_relres].  Returns the Cholesky status.
 int orc_sr_step(int kind, int n, int lx, int ly, double J, double h, double sign, int m, int use_bias,

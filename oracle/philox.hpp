@@ -27,6 +27,7 @@ enum : uint32_t {
     TAG_SHUF = 0x53485546u,   // fixed-magnetisation shuffle
     TAG_PARAM = 0x50415241u,  // normal draws for parameter initialisation
     TAG_EXACT = 0x45584143u,  // exact-sampler draws
+    TAG_PT = 0x50544d58u,     // parallel-tempering swap draws
 };
 
 struct Philox4x32 {

@@ -65,6 +65,7 @@ def _declare(L):
         "orc_eloc": (None, [i, i, i, i, d, d, d, i, i, vp, i, vp, vp, vp, i]),
         "orc_random_sigma": (None, [i, i, u64, u32, u32, vp]),
         "orc_sample": (None, [i, i, i, vp, i, i, i, u64, u32, i, i, i, i, vp, vp, vp, vp, i]),
+        "orc_sample_pt": (None, [i, i, i, vp, i, i, i, i, u64, u32, i, i, i, i, vp, vp, vp, vp, vp, i]),
         "orc_sr_step": (i, [i, i, i, i, d, d, d, i, i, vp, i, vp, vp, d, i, i, d, vp, vp, vp, vp, vp, i]),
         "orc_cholesky_solve": (i, [i, vp, vp]),
         "orc_exact": (i, [i, i, i, i, d, d, d, i, i, vp, i, i, vp, vp, vp, vp, i]),
@@ -220,6 +221,22 @@ def sample(n, m, params, n_chains, move=MOVE_LOCAL, nup=-1, seed=0, epoch=0, rei
     lib().orc_sample(n, m, int(use_bias), _p(params), n_chains, move, nup, seed, epoch, int(reinit), n_sweeps,
                      n_discard, sweep_len, _p(cs), _p(osig), _p(oth), _p(acc), nthreads or os.cpu_count())
     return osig, oth, cs, acc
+
+
+def sample_pt(n, m, params, n_chains, ntemps, move=MOVE_LOCAL, nup=-1, seed=0, epoch=0, reinit=True, n_sweeps=1,
+              n_discard=0, sweep_len=0, chain_sigma=None, slot=None, use_bias=True, nthreads=0):
+    """Restated SamplerMT with nTmps = ntemps > 1 (temperature swaps between the
+    chains of a group).  Returns (sigma[groups * n_sweeps, n], theta, chain_sigma, slot, acc)."""
+    cs = np.zeros((n_chains, n), dtype=np.int8) if chain_sigma is None else np.ascontiguousarray(chain_sigma, np.int8)
+    sl = np.zeros(n_chains, dtype=np.int32) if slot is None else np.ascontiguousarray(slot, np.int32)
+    ns = (n_chains // ntemps) * n_sweeps
+    osig = np.zeros((ns, n), dtype=np.int8)
+    oth = np.zeros((ns, m), dtype=np.complex128)
+    acc = np.zeros(n_chains, dtype=np.uint64)
+    lib().orc_sample_pt(n, m, int(use_bias), _p(params), n_chains, ntemps, move, nup, seed, epoch, int(reinit),
+                        n_sweeps, n_discard, sweep_len, _p(cs), _p(sl), _p(osig), _p(oth), _p(acc),
+                        nthreads or os.cpu_count())
+    return osig, oth, cs, sl, acc
 
 
 def sr_step(ham, m, params, sigma, th, shift, mode=SR_S, solver=SOLVE_LLT, cgtol=1e-4, use_bias=True, nthreads=0):

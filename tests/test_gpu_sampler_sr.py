@@ -229,3 +229,61 @@ def test_sampler_autotuned_launch_shape(ctx, orc):
     assert out[0][0] in (1, 2, 4)
     assert out[1][0] == out[0][0]
     assert np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("move,nup,ntemps", [(0, -1, 4), (1, 5, 2), (0, -1, 8)])
+def test_tempering_fp64_matches_oracle_draw_for_draw(ctx, orc, move, nup, ntemps):
+    """SamplerMT with nTmps > 1: every chain sweeps at its beta, temperatures swap
+    within groups after every sweep, the beta = 1 chains are recorded; device and
+    oracle agree draw for draw, swap for swap, and across a second call."""
+    from yannq_b200 import api
+
+    n, m, per = 10, 20, 4
+    nc = per * ntemps
+    q, p = _mk(api, ctx, orc, n, m, 23, 0.4, api.C128)
+    S = api.Sampler(q, nc, move, nup)
+    S.set_tempering(ntemps)
+    S.sample(6, 5, seed=77, epoch=2, reinit=True)
+    s, th = S.get_samples()
+    os_, oth, ocs, osl, oacc = orc.sample_pt(n, m, p, nc, ntemps, move=move, nup=nup, seed=77, epoch=2, reinit=True,
+                                             n_sweeps=6, n_discard=5)
+    assert s.shape == (per * 6, n)
+    np.testing.assert_array_equal(s, os_)
+    assert np.max(np.abs(th - oth)) <= 1e-13 * max(1.0, np.max(np.abs(oth)))
+    np.testing.assert_array_equal(S.get_slots(), osl)
+    np.testing.assert_array_equal(S.get_accepts(), oacc)
+    assert len(set(osl.tolist())) == ntemps
+    if ntemps >= 4:  # temperatures moved (a two-slot ladder may return to where it started)
+        assert not np.array_equal(osl, np.arange(nc) % ntemps)
+    S.sample(4, 0, seed=77, epoch=3, reinit=False)
+    s2, _ = S.get_samples()
+    os2, _, _, osl2, _ = orc.sample_pt(n, m, p, nc, ntemps, move=move, nup=nup, seed=77, epoch=3, reinit=False,
+                                       n_sweeps=4, n_discard=0, chain_sigma=ocs, slot=osl)
+    np.testing.assert_array_equal(s2, os2)
+    np.testing.assert_array_equal(S.get_slots(), osl2)
+    S.close()
+    q.close()
+
+
+def test_tempering_complex64_distribution(ctx, orc):
+    """The beta = 1 samples of a tempered complex64 sampler follow |psi|^2 (chi^2)."""
+    from scipy import stats
+    from yannq_b200 import api
+
+    n, m, ntemps, per = 6, 12, 4, 64
+    q, p = _mk(api, ctx, orc, n, m, 24, 0.5, api.C64)
+    S = api.Sampler(q, per * ntemps)
+    S.set_tempering(ntemps)
+    S.sample(200, 100, seed=5, epoch=0, reinit=True)
+    s, _ = S.get_samples()
+    idx = np.array([orc.index_of(x) for x in s])
+    counts = np.bincount(idx, minlength=1 << n)
+    lp = np.array([orc.logpsi(n, m, p, orc.sigma_of(k, n)).real for k in range(1 << n)])
+    w = np.exp(2 * (lp - lp.max()))
+    w /= w.sum()
+    # consecutive sweeps of one chain are correlated: compare against a conservative
+    # effective sample size (every 4th sample)
+    chi2, pval = stats.chisquare(np.bincount(idx[::4], minlength=1 << n), len(idx[::4]) * w)
+    assert pval > 1e-4, (chi2, pval)
+    S.close()
+    q.close()

@@ -158,3 +158,20 @@ def test_ff_forward_matches_numpy(orc):
     z2 = Wfc.T @ a1
     want = np.log(np.cosh(z2)).sum()
     assert orc.ff_forward(L, C, K, F, p, s) == pytest.approx(want, rel=1e-12)
+
+
+def test_oracle_tempering_samples_follow_psi2(orc):
+    """The oracle's restated SamplerMT with nTmps = 4 records beta = 1 chains whose
+    configurations follow |psi|^2 (chi^2 on a 6-spin RBM)."""
+    from scipy import stats
+
+    n, m, ntemps, per = 6, 12, 4, 32
+    p = orc.init_params(n, m, 25, 0.5)
+    s, _, _, slots, _ = orc.sample_pt(n, m, p, per * ntemps, ntemps, seed=11, n_sweeps=400, n_discard=100)
+    assert sorted(slots[:ntemps].tolist()) == list(range(ntemps))
+    idx = np.array([orc.index_of(x) for x in s[::4]])
+    lp = np.array([orc.logpsi(n, m, p, orc.sigma_of(k, n)).real for k in range(1 << n)])
+    w = np.exp(2 * (lp - lp.max()))
+    w /= w.sum()
+    chi2, pval = stats.chisquare(np.bincount(idx, minlength=1 << n), len(idx) * w)
+    assert pval > 1e-4, (chi2, pval)

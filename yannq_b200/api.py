@@ -83,6 +83,8 @@ SIGNATURES = {
     "yq_sampler_put_samples": [_vp, _i, _vp, _vp],
     "yq_sampler_sample_exact": [_vp, _i, _u64, _u32, _vp],
     "yq_sampler_chains_per_cta": [_vp, _vp],
+    "yq_sampler_set_tempering": [_vp, _i],
+    "yq_sampler_get_slots": [_vp, _vp],
     "yq_exact": [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp],
     "yq_batch_create": [_vp, _i, _vp, _vp],
     "yq_batch_iteration": [_vp, _vp, _vp],
@@ -353,6 +355,15 @@ class Sampler:
         th = np.zeros((ns, self.rbm.m), np.complex128) if theta else None
         check(lib().yq_sampler_get_samples(self.h, _p(s), _p(th)))
         return s, th
+
+    def set_tempering(self, ntemps):
+        """SamplerMT with nTmps = ntemps (parallel tempering between the chains of each group)."""
+        check(lib().yq_sampler_set_tempering(self.h, ntemps))
+
+    def get_slots(self):
+        out = np.zeros(self.n_chains, np.int32)
+        check(lib().yq_sampler_get_slots(self.h, _p(out)))
+        return out
 
     def chains_per_cta(self):
         v = C.c_int()

@@ -588,6 +588,33 @@ int yq_sampler_get_accepts(yq_sampler S, uint64_t* acc) {
     });
 }
 
+int yq_sampler_set_tempering(yq_sampler S, int ntemps) {
+    return guard([&] {
+        need(S, "sampler");
+        if (ntemps < 1 || ntemps > 64 || (ntemps > 1 && ntemps % 2 != 0))
+            throw Error(YQ_E_ARG, "set_tempering: ntemps must be 1 or even and at most 64");
+        if (S->n_chains % ntemps != 0) throw Error(YQ_E_ARG, "set_tempering: n_chains must be a multiple of ntemps");
+        S->ntemps = ntemps;
+        S->pt_ready = false;
+        if (ntemps > 1) {
+            S->pt_slot.ensure(size_t(S->n_chains) * sizeof(int));
+            S->pt_beta.ensure(size_t(S->n_chains) * sizeof(double));
+        }
+    });
+}
+
+int yq_sampler_get_slots(yq_sampler S, int* slots) {
+    return guard([&] {
+        need(S, "sampler");
+        need(slots, "slots");
+        if (S->ntemps <= 1 || !S->pt_ready) {
+            for (int c = 0; c < S->n_chains; ++c) slots[c] = S->ntemps > 1 ? c % S->ntemps : 0;
+            return;
+        }
+        down(slots, S->pt_slot.p, size_t(S->n_chains), S->q->ctx->stream);
+    });
+}
+
 int yq_sampler_chains_per_cta(yq_sampler S, int* out) {
     return guard([&] {
         need(S, "sampler");

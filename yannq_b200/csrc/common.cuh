@@ -190,6 +190,7 @@ enum : uint32_t {
     TAG_SHUF = 0x53485546u,
     TAG_PARAM = 0x50415241u,
     TAG_EXACT = 0x45584143u,
+    TAG_PT = 0x50544d58u,
 };
 
 struct U4 {

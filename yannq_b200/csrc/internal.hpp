@@ -66,6 +66,11 @@ struct yq_sampler_s {
     uint64_t proposals = 0;  // per chain, last call
     const uint32_t* epoch_dev = nullptr;  // device epoch offset added to the call's epoch (batched graphs)
     int chains_per_cta = 0;               // autotuned launch shape of the last sample call
+    // parallel tempering (SamplerMT nTmps > 1): chains c = ntemps group + k
+    int ntemps = 1;
+    bool pt_ready = false;
+    yq::DevBuf pt_slot, pt_beta;  // per chain: ladder slot (int), beta (double)
+    yq::DevBuf pt_theta, pt_lp;   // theta carried between sweep launches, Re log psi
 };
 
 // FeedForward machine Conv1D(1 -> C, kernel K, periodic, no bias) -> LnCosh ->

@@ -33,6 +33,14 @@ struct SampArgs {
     uint64_t seed;
     uint32_t epoch;
     const uint32_t* epoch_dev;  // optional device-side epoch offset (graph replays)
+    // parallel tempering (one launch per sweep): per-chain beta, theta carried over
+    // between launches, recording of the slot-0 chain of each group, Re log psi out
+    const double* beta;
+    const cplx<R>* theta_in;
+    cplx<R>* theta_out;
+    double* lp_out;
+    const int* slot;
+    int ntemps, groups, rec_index, sw0, acc_add;
     const c128* p64;
     const cplx<R>* W;
     const cplx<R>* tau;
@@ -125,8 +133,17 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     }
     __syncwarp();
 
+    const R beta = A.beta ? R(A.beta[c]) : R(1);
     cplx<R> th[JPL], t[JPL];
-    theta_fp64<R, JPL>(A, s, lane, th);
+    if (A.theta_in) {
+#pragma unroll
+        for (int r = 0; r < JPL; ++r) {
+            const int j = lane + 32 * r;
+            th[r] = j < m ? A.theta_in[size_t(c) * m + j] : mk(R(0), R(0));
+        }
+    } else {
+        theta_fp64<R, JPL>(A, s, lane, th);
+    }
 #pragma unroll
     for (int r = 0; r < JPL; ++r) t[r] = ctanh(th[r]);
 
@@ -141,7 +158,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     // into L1.
     // (register pipelining for complex64 only: complex128 would spill)
     constexpr bool REGPIPE = MOVE == YQ_MOVE_LOCAL && sizeof(R) == 4;
-    U4 xcur = draw(A.seed, 0u, epoch, uint32_t(c), TAG_SWEEP);
+    U4 xcur = draw(A.seed, uint32_t(A.sw0) * L, epoch, uint32_t(c), TAG_SWEEP);
     cplx<R> tvn[JPL], wvn[JPL];
     double lkn = 0., abn = 0.;
     auto load_cols = [&](int kq) {
@@ -170,7 +187,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
 
     for (int sw = 0; sw < A.n_total; ++sw) {
         for (uint32_t p = 0; p < L; ++p) {
-            const uint32_t g = uint32_t(sw) * L + p;
+            const uint32_t g = uint32_t(A.sw0 + sw) * L + p;
             const U4 x = xcur;
             const U4 xn = draw(A.seed, g + 1u, epoch, uint32_t(c), TAG_SWEEP);
             xcur = xn;
@@ -242,7 +259,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 const double base = lk - 2.0 * double(sk) * ab;
                 const R logr = R(0.5) * ls + R(base);
                 // LocalSweeper.hpp:45-47: p = min(1, exp(beta * 2 * Re logRatio)); accept if u < p
-                if (u < exp(two * logr)) {
+                if (u < exp(two * beta * logr)) {
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
                         int j = lane + 32 * r;
@@ -299,7 +316,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                     base -= 2.0 * double(sk) * A.p64[size_t(n) * m + k].re +
                             2.0 * double(sl) * A.p64[size_t(n) * m + l].re;
                 const R logr = R(0.5) * ls + R(base);
-                if (u < exp(two * logr)) {
+                if (u < exp(two * beta * logr)) {
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
                         int j = lane + 32 * r;
@@ -324,7 +341,8 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
             }
         }
         // ---- end of sweep: record (SamplerMT.hpp:196-201), resync
-        if (sw >= A.n_discard) {
+        // tempered sampling records after mixChains, in pt_mix_kernel
+        if (sw >= A.n_discard && !A.slot) {
             const size_t idx = size_t(sw - A.n_discard) * A.n_chains + c;
             for (int i = lane; i < n; i += 32) A.out_sigma[idx * n + i] = s[i];
 #pragma unroll
@@ -333,13 +351,81 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 if (j < m) A.out_theta[idx * m + j] = th[r];
             }
         }
-        if (A.resync > 0 && ((sw + 1) % A.resync) == 0) theta_fp64<R, JPL>(A, s, lane, th);
+        if (A.resync > 0 && ((A.sw0 + sw + 1) % A.resync) == 0) theta_fp64<R, JPL>(A, s, lane, th);
 #pragma unroll
         for (int r = 0; r < JPL; ++r) t[r] = ctanh(th[r]);
     }
     __syncwarp();
     for (int i = lane; i < n; i += 32) cs[i] = s[i];
-    if (lane == 0) A.acc[c] = nacc;
+    if (A.theta_out) {
+#pragma unroll
+        for (int r = 0; r < JPL; ++r) {
+            const int j = lane + 32 * r;
+            if (j < m) A.theta_out[size_t(c) * m + j] = th[r];
+        }
+    }
+    if (A.lp_out) {
+        // Re log psi = Re(a) . sigma + sum_j Re logcosh(theta_j)   (RBM.hpp:367-378)
+        double lp = 0.;
+#pragma unroll
+        for (int r = 0; r < JPL; ++r) {
+            const int j = lane + 32 * r;
+            if (j < m) lp += clogcosh(cast<double>(th[r])).re;
+        }
+        if (A.bias)
+            for (int i = lane; i < n; i += 32) lp += double(s[i]) * A.p64[size_t(n) * m + i].re;
+        lp = warp_allsum(lp);
+        if (lane == 0) A.lp_out[c] = lp;
+    }
+    if (lane == 0) A.acc[c] = (A.acc_add ? A.acc[c] : 0ull) + nacc;
+}
+
+// mixChains (SamplerMT.hpp:120-153) for one group per thread: even slot pairs
+// (0,1),(2,3),..., then odd pairs (1,2),...,(ntemps-3, ntemps-2); a swap exchanges
+// the chains' slots (temperatures).  p = exp((beta_{t+1} - beta_t) 2 (lp(slot t) -
+// lp(slot t+1))), u from counter (64 sweep + t, epoch, group, TAG_PT).
+// A recorded sweep then appends the slot-0 chain of the group (SamplerMT.hpp:196-201,
+// after mixChains): sigma from the chains, theta (tbytes per chain) from the
+// carried-over theta, into output row rec_index * groups + group.
+__global__ void pt_mix_kernel(int groups, int ntemps, const double* __restrict__ lp, int* __restrict__ slot,
+                              double* __restrict__ beta, uint64_t seed, uint32_t epoch, const uint32_t* epoch_dev,
+                              uint32_t sweep, int record, int rec_index, int n, const int8_t* __restrict__ chains,
+                              int tbytes, const uint8_t* __restrict__ theta, int8_t* __restrict__ out_sigma,
+                              uint8_t* __restrict__ out_theta) {
+    const int gr = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gr >= groups) return;
+    const uint32_t ep = epoch_dev ? epoch + *epoch_dev : epoch;
+    int at[64];
+    for (int k = 0; k < ntemps; ++k) at[slot[gr * ntemps + k]] = gr * ntemps + k;
+    auto bt = [&](int t) { return double(ntemps - t) / double(ntemps); };
+    auto attempt = [&](int t) {
+        const int a = at[t], b = at[t + 1];
+        const double pr = exp((bt(t + 1) - bt(t)) * 2.0 * (lp[a] - lp[b]));
+        const U4 x = draw(seed, sweep * 64u + uint32_t(t), ep, uint32_t(gr), TAG_PT);
+        if (draw_u53(x.z, x.w) < pr) {
+            at[t] = b;
+            at[t + 1] = a;
+        }
+    };
+    for (int t = 0; t + 1 < ntemps; t += 2) attempt(t);
+    for (int t = 1; t + 1 < ntemps - 1; t += 2) attempt(t);
+    for (int t = 0; t < ntemps; ++t) {
+        slot[at[t]] = t;
+        beta[at[t]] = bt(t);
+    }
+    if (record) {
+        const size_t row = size_t(rec_index) * groups + gr;
+        const int c0 = at[0];
+        for (int i = 0; i < n; ++i) out_sigma[row * n + i] = chains[size_t(c0) * n + i];
+        for (int b = 0; b < tbytes; ++b) out_theta[row * tbytes + b] = theta[size_t(c0) * tbytes + b];
+    }
+}
+
+__global__ void pt_reset_kernel(int n_chains, int ntemps, int* __restrict__ slot, double* __restrict__ beta) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_chains) return;
+    slot[c] = c % ntemps;
+    beta[c] = double(ntemps - c % ntemps) / double(ntemps);
 }
 
 template <typename R, int MOVE, int JPL>
@@ -394,6 +480,12 @@ static int tuned_warps(const SampArgs<R>& A, cudaStream_t st) {
     T.n_total = 2;
     T.n_discard = 1;
     T.epoch_dev = nullptr;
+    T.theta_in = nullptr;  // nothing of the real chain state is read or written
+    T.theta_out = nullptr;
+    T.lp_out = nullptr;
+    T.slot = nullptr;
+    T.acc_add = 0;
+    T.sw0 = 0;
     if (!A.reinit)
         YQ_CUDA(cudaMemcpyAsync(ch.p, A.chains, size_t(A.n_chains) * A.n, cudaMemcpyDeviceToDevice, st));
     cudaEvent_t e0, e1;
@@ -447,6 +539,15 @@ static void dispatch_jpl(const SampArgs<R>& A, cudaStream_t st, int* chosen) {
 }
 
 template <typename R>
+static void launch_sweeps(yq_sampler_s* S, const SampArgs<R>& A, cudaStream_t st) {
+    switch (S->move) {
+        case YQ_MOVE_LOCAL: dispatch_jpl<R, YQ_MOVE_LOCAL>(A, st, &S->chains_per_cta); break;
+        case YQ_MOVE_EXCHANGE_ANY: dispatch_jpl<R, YQ_MOVE_EXCHANGE_ANY>(A, st, &S->chains_per_cta); break;
+        default: dispatch_jpl<R, YQ_MOVE_EXCHANGE_NN>(A, st, &S->chains_per_cta); break;
+    }
+}
+
+template <typename R>
 static void run_t(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, uint32_t epoch, int reinit) {
     yq_rbm_s* q = S->q;
     SampArgs<R> A;
@@ -464,6 +565,16 @@ static void run_t(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, u
     A.seed = seed;
     A.epoch = epoch;
     A.epoch_dev = S->epoch_dev;
+    A.beta = nullptr;
+    A.theta_in = nullptr;
+    A.theta_out = nullptr;
+    A.lp_out = nullptr;
+    A.slot = nullptr;
+    A.ntemps = 1;
+    A.groups = S->n_chains;
+    A.rec_index = 0;
+    A.sw0 = 0;
+    A.acc_add = 0;
     A.p64 = q->p64.as<c128>();
     A.W = q->W.as<cplx<R>>();
     A.tau = q->tau.as<cplx<R>>();
@@ -473,10 +584,40 @@ static void run_t(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, u
     A.out_theta = S->theta.as<cplx<R>>();
     A.acc = S->acc.as<unsigned long long>();
     cudaStream_t st = q->ctx->stream;
-    switch (S->move) {
-        case YQ_MOVE_LOCAL: dispatch_jpl<R, YQ_MOVE_LOCAL>(A, st, &S->chains_per_cta); break;
-        case YQ_MOVE_EXCHANGE_ANY: dispatch_jpl<R, YQ_MOVE_EXCHANGE_ANY>(A, st, &S->chains_per_cta); break;
-        default: dispatch_jpl<R, YQ_MOVE_EXCHANGE_NN>(A, st, &S->chains_per_cta); break;
+    if (S->ntemps <= 1) {
+        launch_sweeps<R>(S, A, st);
+        return;
+    }
+    // parallel tempering: one launch per sweep, then mixChains per group
+    const int nt = S->ntemps, groups = S->n_chains / nt;
+    S->pt_theta.ensure(size_t(S->n_chains) * q->m * sizeof(cplx<R>));
+    S->pt_lp.ensure(size_t(S->n_chains) * sizeof(double));
+    if (reinit || !S->pt_ready) {
+        pt_reset_kernel<<<cdiv_u(S->n_chains, 128), 128, 0, st>>>(S->n_chains, nt, S->pt_slot.as<int>(),
+                                                                 S->pt_beta.as<double>());
+        YQ_LAUNCH_CHECK();
+        S->pt_ready = true;
+    }
+    A.beta = S->pt_beta.as<double>();
+    A.slot = S->pt_slot.as<int>();
+    A.theta_out = S->pt_theta.as<cplx<R>>();
+    A.lp_out = S->pt_lp.as<double>();
+    A.ntemps = nt;
+    A.groups = groups;
+    A.n_total = 1;
+    for (int sw = 0; sw < n_discard + n_sweeps; ++sw) {
+        A.sw0 = sw;
+        A.reinit = sw == 0 ? reinit : 0;
+        A.theta_in = sw == 0 ? nullptr : S->pt_theta.as<cplx<R>>();
+        A.n_discard = sw < n_discard ? 1 : 0;
+        A.rec_index = sw - n_discard;
+        A.acc_add = sw > 0;
+        launch_sweeps<R>(S, A, st);
+        pt_mix_kernel<<<cdiv_u(groups, 128), 128, 0, st>>>(
+            groups, nt, S->pt_lp.as<double>(), S->pt_slot.as<int>(), S->pt_beta.as<double>(), seed, epoch,
+            S->epoch_dev, uint32_t(sw), sw >= n_discard ? 1 : 0, sw - n_discard, q->n, S->chains.as<int8_t>(),
+            int(q->m * sizeof(cplx<R>)), S->pt_theta.as<uint8_t>(), S->sigma.as<int8_t>(), S->theta.as<uint8_t>());
+        YQ_LAUNCH_CHECK();
     }
 }
 
@@ -487,7 +628,7 @@ void sampler_run(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, ui
     const long long L = S->sweep_len > 0 ? S->sweep_len : q->n;
     YQ_CHECK_ARG((long long)(n_sweeps + n_discard) * L < (1LL << 32) - 1, "sample: too many proposals per call");
     rbm_prepare(q);
-    const size_t ns = size_t(S->n_chains) * n_sweeps;
+    const size_t ns = size_t(S->n_chains / std::max(1, S->ntemps)) * n_sweeps;
     S->sigma.ensure(ns * q->n);
     S->theta.ensure(ns * q->m * q->csize());
     if (q->dtype == YQ_C64)
