@@ -196,7 +196,8 @@ struct SampleSet {
     std::size_t size() const { return std::size_t(ns); }
 };
 
-// Samplers/SamplerMT.hpp with nTmps = 1 (parallel tempering is not built).
+// Samplers/SamplerMT.hpp: nTmps temperatures x nChainsPer chains (nTmps = 1 or even;
+// parallel tempering swaps temperatures between the chains of a group).
 template <class Machine, class Sweeper>
 class SamplerMT {
     yq_sampler h_ = nullptr;
@@ -206,9 +207,11 @@ class SamplerMT {
 
 public:
     SamplerMT(const Machine& qs, uint32_t nTmps, uint32_t nChainsPer, const Sweeper& sw, int nup = -1) {
-        if (nTmps != 1) throw std::invalid_argument("SamplerMT: only nTmps = 1 is built (no parallel tempering)");
+        if (nTmps == 0 || (nTmps != 1 && nTmps % 2 != 0))
+            throw std::invalid_argument("SamplerMT: nTmps must be 1 or even");  // SamplerMT.hpp:50
         if (sw.n != qs.getN()) throw std::invalid_argument("SamplerMT: sweeper size differs from the machine");
-        check(yq_sampler_create(qs.handle(), int(nChainsPer), Sweeper::move, nup, 0, &h_));
+        check(yq_sampler_create(qs.handle(), int(nTmps * nChainsPer), Sweeper::move, nup, 0, &h_));
+        if (nTmps > 1) check(yq_sampler_set_tempering(h_, int(nTmps)));
     }
     ~SamplerMT() { yq_sampler_destroy(h_); }
     SamplerMT(const SamplerMT&) = delete;
