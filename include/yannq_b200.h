@@ -37,7 +37,8 @@ enum {
 };
 
 enum { YQ_C64 = 0, YQ_C128 = 1 };                             /* RBM<complex<float|double>> */
-enum { YQ_HAM_TFI = 0, YQ_HAM_XXZ = 1, YQ_HAM_TFI2D = 2 };    /* Hamiltonian kinds          */
+enum { YQ_HAM_TFI = 0, YQ_HAM_XXZ = 1, YQ_HAM_TFI2D = 2,       /* Hamiltonian kinds          */
+       YQ_HAM_XXX = 3, YQ_HAM_J1J2 = 4, YQ_HAM_XYZNNN = 5, YQ_HAM_KITAEV_HEX = 6 };
 enum { YQ_MOVE_LOCAL = 0, YQ_MOVE_EXCHANGE_ANY = 1, YQ_MOVE_EXCHANGE_NN = 2 };
 enum { YQ_SR_AUTO = 0, YQ_SR_S = 1, YQ_SR_T = 2 };             /* S = <O^H O>, T = O O^H dual */
 enum { YQ_PREC_FP64 = 0, YQ_PREC_MIXED = 1 };
@@ -122,16 +123,33 @@ int yq_rbm_log_deriv(yq_rbm q, int ns, const int8_t* sigma, const double* theta,
  * capture. */
 int yq_rbm_oloc_noalloc(yq_rbm q, int ns, const int8_t* d_sigma, const void* d_theta, double* d_oloc);
 
-/* ---- Hamiltonians (Hamiltonians/TFIsing.hpp, Hamiltonians/XXZ.hpp) -------- */
+/* ---- Hamiltonians (Hamiltonians/TFIsing.hpp, XXZ.hpp, XXX.hpp, J1J2.hpp, ------
+ * ---- XYZNNN.hpp, KitaevHex.hpp) ------------------------------------------ */
 /* kind YQ_HAM_TFI: TFIsing(n, J, h); YQ_HAM_XXZ: XXZ(n, J, Delta = h, signRule);
  * YQ_HAM_TFI2D: periodic lx x ly square lattice (no reference counterpart; same
- * duck-typed concept: E_loc = sum J s_i (s_right + s_down) + h ratio(i)). */
+ * duck-typed concept: E_loc = sum J s_i (s_right + s_down) + h ratio(i));
+ * YQ_HAM_XXX: XXX(n) (Hamiltonians/XXX.hpp:11-22; J, h unused);
+ * YQ_HAM_J1J2: J1J2(n, J1 = J, J2 = h, signRule) (Hamiltonians/J1J2.hpp:14-56);
+ * YQ_HAM_XYZNNN: XYZNNN(n, a = J, b = h) (Hamiltonians/XYZNNN.hpp:16-53).
+ * J1J2 and XYZNNN need n >= 3.  lx, ly are read by YQ_HAM_TFI2D only; KitaevHex
+ * has its own creator below. */
 int yq_ham_create(yq_ctx ctx, int kind, int n, int lx, int ly, double J, double h, int sign_rule, yq_ham* out);
+/* KitaevHex(ncol, nrow, Jx, Jy, Jz) with the field term h * ratio(i) of
+ * KitaevHex(n, m, J, h) (Hamiltonians/KitaevHex.hpp:19-31, 119-146): ncol and
+ * nrow even, sites = ncol * nrow, links as in blackIdx / whiteIdx / xLinks /
+ * yLinks / zLinks (KitaevHex.hpp:33-103). */
+int yq_ham_create_kitaev_hex(yq_ctx ctx, int ncol, int nrow, double Jx, double Jy, double Jz, double h,
+                             yq_ham* out);
 int yq_ham_destroy(yq_ham H);
+/* Number of off-diagonal requests per sample that yq_ham_enumerate writes
+ * (n for TFI, XXZ, TFI2D and XXX; 2n for J1J2 and XYZNNN; 2 * sites for KitaevHex). */
+int yq_ham_num_offdiag(yq_ham H, int* count);
 /* The state form's off-diagonal flips for each sample, in the order the
  * reference's operator()(State) requests them (Hamiltonians/TFIsing.hpp:28-39,
- * XXZ.hpp:37-49), zero coefficients included: per sample n terms of (site_a,
- * site_b or -1, coeff) and the diagonal sum.  Arrays: ns*n ints / doubles, ns doubles. */
+ * XXZ.hpp:37-49, XXX.hpp:11-22, J1J2.hpp:35-56, XYZNNN.hpp:33-53,
+ * KitaevHex.hpp:119-146), zero coefficients included: per sample K =
+ * yq_ham_num_offdiag terms of (site_a, site_b or -1, coeff) and the diagonal
+ * sum.  Arrays: ns*K ints / doubles, ns doubles. */
 int yq_ham_enumerate(yq_ham H, int ns, const int8_t* sigma, int* site_a, int* site_b, double* coeff, double* diag);
 /* Energy::eachSample over a batch -- Observables/Energy.hpp:47-51 with
  * State = RBMStateRef(sigma, theta) (GroundState/utils.hpp:108-126). out: ns complex. */

@@ -149,6 +149,7 @@ protected:
     Hamiltonian(Context& ctx, int kind, int n, int lx, int ly, double J, double h, bool sign) : n_(n) {
         check(yq_ham_create(ctx.handle(), kind, n, lx, ly, J, h, sign ? 1 : 0, &h_));
     }
+    Hamiltonian(int n, yq_ham h) : h_(h), n_(n) {}
 
 public:
     virtual ~Hamiltonian() { yq_ham_destroy(h_); }
@@ -170,6 +171,32 @@ struct XXZ : Hamiltonian {
 struct TFIsing2D : Hamiltonian {
     TFIsing2D(Context& ctx, int lx, int ly, double J, double h)
         : Hamiltonian(ctx, YQ_HAM_TFI2D, lx * ly, lx, ly, J, h, false) {}
+};
+// Hamiltonians/XXX.hpp
+struct XXX : Hamiltonian {
+    XXX(Context& ctx, int n) : Hamiltonian(ctx, YQ_HAM_XXX, n, 0, 0, 0.0, 0.0, false) {}
+};
+// Hamiltonians/J1J2.hpp
+struct J1J2 : Hamiltonian {
+    J1J2(Context& ctx, int n, double J1, double J2, bool signRule)
+        : Hamiltonian(ctx, YQ_HAM_J1J2, n, 0, 0, J1, J2, signRule) {}
+};
+// Hamiltonians/XYZNNN.hpp
+struct XYZNNN : Hamiltonian {
+    XYZNNN(Context& ctx, int n, double a, double b) : Hamiltonian(ctx, YQ_HAM_XYZNNN, n, 0, 0, a, b, false) {}
+};
+// Hamiltonians/KitaevHex.hpp: both reference constructors
+struct KitaevHex : Hamiltonian {
+    KitaevHex(Context& ctx, int n, int m, double J, double h = 0.0) : Hamiltonian(n * m, make(ctx, n, m, J, J, J, h)) {}
+    KitaevHex(Context& ctx, int n, int m, double Jx, double Jy, double Jz)
+        : Hamiltonian(n * m, make(ctx, n, m, Jx, Jy, Jz, 0.0)) {}
+
+private:
+    static yq_ham make(Context& ctx, int n, int m, double Jx, double Jy, double Jz, double h) {
+        yq_ham out = nullptr;
+        check(yq_ham_create_kitaev_hex(ctx.handle(), n, m, Jx, Jy, Jz, h, &out));
+        return out;
+    }
 };
 
 // Samplers/LocalSweeper.hpp, Samplers/SwapSweeper.hpp (+ neighbour-pair variant)

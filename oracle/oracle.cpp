@@ -63,10 +63,79 @@ static inline int down_of(const Ham& H, int i) {
     return x + H.lx * ((y + 1) % H.ly);
 }
 
+// KitaevHex.hpp:33-103.  Sites of row r: n_/2 black ones (r * n_ + c), then
+// n_/2 white ones (r * n_ + n_/2 + c); rows and columns wrap around.
+std::vector<std::pair<int, int>> kitaev_links(const Ham& H, int axis) {
+    const int nc = H.lx, nr = H.ly, k = nc / 2;
+    auto wrap = [](int v, int p) { return ((v % p) + p) % p; };
+    auto black = [&](int r, int c) { return wrap(r, nr) * nc + wrap(c, k); };
+    auto white = [&](int r, int c) { return wrap(r, nr) * nc + wrap(c, k) + k; };
+    std::vector<std::pair<int, int>> out;
+    if (axis == 2) {  // zLinks: white (r, c) to black (r + 1, c)
+        for (int r = 0; r < nr; ++r)
+            for (int c = 0; c < k; ++c) out.emplace_back(white(r, c), black(r + 1, c));
+        return out;
+    }
+    // xLinks: even rows to white (r, c - 1), odd rows to white (r, c);
+    // yLinks: even rows to white (r, c), odd rows to white (r, c + 1).  Even rows first.
+    for (int parity = 0; parity < 2; ++parity)
+        for (int r = parity; r < nr; r += 2)
+            for (int c = 0; c < k; ++c) {
+                int dc = axis == 0 ? (parity == 0 ? -1 : 0) : (parity == 0 ? 0 : 1);
+                out.emplace_back(black(r, c), white(r, c + dc));
+            }
+    return out;
+}
+
+// State forms of XXX (XXX.hpp:11-22), J1J2 (J1J2.hpp:35-56), XYZNNN
+// (XYZNNN.hpp:33-53) and KitaevHex (KitaevHex.hpp:119-146) in the reference's
+// evaluation order: diag(d) for every real addend, ratio(a, b, c) for every
+// c * ratio(a, b) addend (b = -1 for one flip), with the coefficients formed as
+// the reference forms them.
+template <class Diag, class Ratio>
+static void ModelStateForm(const Ham& H, const int8_t* s, Diag diag, Ratio ratio) {
+    const int n = H.n;
+    if (H.kind == HAM_XXX) {
+        for (int i = 0; i < n; ++i) {
+            int j = (i + 1) % n;
+            double yy = double(s[i] * s[j]);
+            diag(yy);
+            ratio(i, j, 1.0 - yy);
+        }
+    } else if (H.kind == HAM_J1J2 || H.kind == HAM_XYZNNN) {
+        const bool j1j2 = H.kind == HAM_J1J2;
+        const double J1 = j1j2 ? H.J : -1.0, J2 = j1j2 ? H.h : -1.0;
+        for (int d = 1; d <= 2; ++d)
+            for (int i = 0; i < n; ++i) {
+                int j = (i + d) % n;
+                double yy = -double(s[i] * s[j]);
+                const double Jd = d == 1 ? J1 : J2;
+                diag(-Jd * yy);
+                double c;
+                if (j1j2)
+                    c = d == 1 ? J1 * H.sign * (1.0 + yy) : J2 * (1.0 + yy);
+                else
+                    c = d == 1 ? J1 * (H.J + yy * H.h) : J2 * (H.h + yy * H.J);
+                ratio(i, j, c);
+            }
+    } else if (H.kind == HAM_KITAEV) {
+        for (int i = 0; i < n; ++i) ratio(i, -1, H.h);
+        for (auto& e : kitaev_links(H, 0)) ratio(e.first, e.second, H.J);
+        for (auto& e : kitaev_links(H, 1)) {
+            int zz = s[e.first] * s[e.second];
+            ratio(e.first, e.second, -H.jy * zz);
+        }
+        for (auto& e : kitaev_links(H, 2)) {
+            int zz = s[e.first] * s[e.second];
+            diag(H.jz * zz);
+        }
+    }
+}
+
 double ham_enumerate(const Ham& H, const int8_t* s, std::vector<FlipTerm>& terms) {
     terms.clear();
     double diag = 0.;
-    for (int i = 0; i < H.n; ++i) {
+    for (int i = 0; i < (H.kind <= HAM_TFI2D ? H.n : 0); ++i) {
         if (H.kind == 0) {  // TFIsing.hpp:31-36
             diag += H.J * s[i] * s[(i + 1) % H.n];
             terms.push_back({uint64_t(1) << i, H.h});
@@ -75,19 +144,23 @@ double ham_enumerate(const Ham& H, const int8_t* s, std::vector<FlipTerm>& terms
             int zz = s[i] * s[j];
             diag += H.J * H.h * zz;
             terms.push_back({(uint64_t(1) << i) | (uint64_t(1) << j), H.sign * H.J * (1 - zz)});
-        } else {  // TFIsing2D: right and down bonds of every site, then the field
+        } else if (H.kind == 2) {  // TFIsing2D: right and down bonds of every site, then the field
             diag += H.J * s[i] * s[right_of(H, i)];
             diag += H.J * s[i] * s[down_of(H, i)];
             terms.push_back({uint64_t(1) << i, H.h});
         }
     }
+    // state forms of the further models, recorded as (mask, coeff) requests
+    ModelStateForm(H, s, [&](double d) { diag += d; }, [&](int a, int b, double c) {
+        terms.push_back({(uint64_t(1) << a) | (b >= 0 ? uint64_t(1) << b : uint64_t(0)), c});
+    });
     return diag;
 }
 
 std::map<uint64_t, double> ham_column(const Ham& H, uint64_t col) {
     std::map<uint64_t, double> res;
     auto z = [&](int i) { return 1 - 2 * int((col >> i) & 1u); };
-    for (int i = 0; i < H.n; ++i) {
+    for (int i = 0; i < (H.kind <= HAM_TFI2D ? H.n : 0); ++i) {
         if (H.kind == 0) {  // TFIsing.hpp:53-65
             res[col ^ (uint64_t(1) << i)] += H.h;
             res[col] += H.J * z(i) * z((i + 1) % H.n);
@@ -97,17 +170,49 @@ std::map<uint64_t, double> ham_column(const Ham& H, uint64_t col) {
             uint64_t x = (uint64_t(1) << i) | (uint64_t(1) << j);
             res[col] += H.J * H.h * zz;
             res[col ^ x] += H.sign * H.J * (1 - zz);
-        } else {
+        } else if (H.kind == 2) {
             res[col ^ (uint64_t(1) << i)] += H.h;
             res[col] += H.J * z(i) * z(right_of(H, i)) + H.J * z(i) * z(down_of(H, i));
         }
+    }
+    auto bit = [](int i) { return uint64_t(1) << i; };
+    const int n = H.n;
+    if (H.kind == HAM_XXX) {  // XXX.hpp:21-34
+        for (int i = 0; i < n; ++i) {
+            int j = (i + 1) % n, sgn = z(i) * z(j);
+            res[col ^ (bit(i) | bit(j))] += 1 - sgn;
+            res[col] += sgn;
+        }
+    } else if (H.kind == HAM_J1J2 || H.kind == HAM_XYZNNN) {  // J1J2.hpp:57-79, XYZNNN.hpp:67-89
+        const bool j1j2 = H.kind == HAM_J1J2;
+        const double J1 = j1j2 ? H.J : -1.0, J2 = j1j2 ? H.h : -1.0;
+        for (int d = 1; d <= 2; ++d)
+            for (int i = 0; i < n; ++i) {
+                int j = (i + d) % n, zz = z(i) * z(j);
+                uint64_t x = bit(i) | bit(j);
+                double off;
+                if (j1j2)
+                    off = d == 1 ? J1 * H.sign * (1.0 - zz * 1.0) : J2 * (1.0 - zz * 1.0);
+                else
+                    off = d == 1 ? J1 * (H.J - zz * H.h) : J2 * (H.h - zz * H.J);
+                res[col ^ x] += off;
+                res[col] += (d == 1 ? J1 : J2) * zz;
+            }
+    } else if (H.kind == HAM_KITAEV) {  // KitaevHex.hpp:148-177
+        for (int i = 0; i < n; ++i) res[col ^ bit(i)] += H.h;
+        for (auto& e : kitaev_links(H, 0)) res[col ^ (bit(e.first) | bit(e.second))] += H.J;
+        for (auto& e : kitaev_links(H, 1)) {
+            int zz = z(e.first) * z(e.second);
+            res[col ^ (bit(e.first) | bit(e.second))] += -H.jy * zz;
+        }
+        for (auto& e : kitaev_links(H, 2)) res[col] += H.jz * (z(e.first) * z(e.second));
     }
     return res;
 }
 
 cd ham_eloc(const Ham& H, const RBM& q, const int8_t* s, const cd* th) {
     cd acc = 0.;
-    for (int i = 0; i < H.n; ++i) {
+    for (int i = 0; i < (H.kind <= HAM_TFI2D ? H.n : 0); ++i) {
         if (H.kind == 0) {
             acc += H.J * s[i] * s[(i + 1) % H.n];
             acc += H.h * std::exp(q.logRatio1(s, th, i));
@@ -116,12 +221,15 @@ cd ham_eloc(const Ham& H, const RBM& q, const int8_t* s, const cd* th) {
             int zz = s[i] * s[j];
             acc += H.J * H.h * zz;
             acc += H.sign * H.J * (1 - zz) * std::exp(q.logRatio2(s, th, i, j));
-        } else {
+        } else if (H.kind == 2) {
             acc += H.J * s[i] * s[right_of(H, i)];
             acc += H.J * s[i] * s[down_of(H, i)];
             acc += H.h * std::exp(q.logRatio1(s, th, i));
         }
     }
+    ModelStateForm(H, s, [&](double d) { acc += d; }, [&](int a, int b, double c) {
+        acc += c * std::exp(b < 0 ? q.logRatio1(s, th, a) : q.logRatio2(s, th, a, b));
+    });
     return acc;
 }
 

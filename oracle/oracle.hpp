@@ -149,14 +149,23 @@ double normal_pair(uint64_t seed, uint32_t idx, double* second);
 // ---------------------------------------------------------------------------
 // Hamiltonians.  kind: 0 = TFIsing (1D ring, Hamiltonians/TFIsing.hpp),
 // 1 = XXZ (1D ring, Hamiltonians/XXZ.hpp), 2 = TFIsing2D (periodic Lx x Ly; no
-// reference counterpart, built on the same duck-typed concept).
+// reference counterpart, built on the same duck-typed concept), 3 = XXX
+// (Hamiltonians/XXX.hpp), 4 = J1J2 (Hamiltonians/J1J2.hpp), 5 = XYZNNN
+// (Hamiltonians/XYZNNN.hpp), 6 = KitaevHex (Hamiltonians/KitaevHex.hpp).
+enum HamKind { HAM_TFI = 0, HAM_XXZ = 1, HAM_TFI2D = 2, HAM_XXX = 3, HAM_J1J2 = 4, HAM_XYZNNN = 5, HAM_KITAEV = 6 };
 struct Ham {
     int kind = 0;
     int n = 0;        // number of sites
-    int lx = 0, ly = 0;  // 2D extents (kind 2)
-    double J = 0., h = 0.;  // TFI: J zz coupling, h field.  XXZ: J, h = Delta
-    double sign = 1.;       // XXZ sign rule (-1 when signRule)
+    int lx = 0, ly = 0;  // 2D extents (TFI2D); KitaevHex: lx = n_ (even), ly = m_ rows (even)
+    // TFI: J zz coupling, h field.  XXZ: J, h = Delta.  J1J2: J = J1, h = J2.
+    // XYZNNN: J = a, h = b.  KitaevHex: J = Jx, jy, jz, h = field.
+    double J = 0., h = 0.;
+    double sign = 1.;       // XXZ / J1J2 sign rule (-1 when signRule)
+    double jy = 0., jz = 0.;
 };
+// KitaevHex link lists (KitaevHex.hpp:33-103), pairs of site indices in the
+// reference's order.
+std::vector<std::pair<int, int>> kitaev_links(const Ham& H, int axis);  // axis 0 = x, 1 = y, 2 = z
 
 // Off-diagonal flip enumeration of the state form (the "mock state" technique of
 // Tests/HamiltonianHelper.hpp:44-92): each requested ratio becomes a (mask, coeff)

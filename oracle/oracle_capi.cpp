@@ -15,15 +15,18 @@ RBM make_rbm(int n, int m, int use_bias, const double* params) {
     q.p = reinterpret_cast<const cd*>(params);
     return q;
 }
-Ham make_ham(int kind, int n, int lx, int ly, double J, double h, double sign) {
+// hp = {J, h, sign, jy, jz} (the Ham fields of the same names)
+Ham make_ham(int kind, int n, int lx, int ly, const double* hp) {
     Ham H;
     H.kind = kind;
     H.n = n;
     H.lx = lx;
     H.ly = ly;
-    H.J = J;
-    H.h = h;
-    H.sign = sign;
+    H.J = hp[0];
+    H.h = hp[1];
+    H.sign = hp[2];
+    H.jy = hp[3];
+    H.jz = hp[4];
     return H;
 }
 }  // namespace
@@ -90,10 +93,11 @@ void orc_logderiv(int n, int m, int use_bias, const double* params, const int8_t
     make_rbm(n, m, use_bias, params).logDeriv(s, reinterpret_cast<const cd*>(theta), reinterpret_cast<cd*>(out));
 }
 
-// Hamiltonian: kind 0 TFI ring, 1 XXZ ring, 2 TFI 2D torus.
-double orc_ham_enumerate(int kind, int n, int lx, int ly, double J, double h, double sign, const int8_t* s,
+// Hamiltonian: kind 0 TFI ring, 1 XXZ ring, 2 TFI 2D torus, 3 XXX, 4 J1J2, 5 XYZNNN,
+// 6 KitaevHex (oracle.hpp HamKind).
+double orc_ham_enumerate(int kind, int n, int lx, int ly, const double* hp, const int8_t* s,
                          uint64_t* masks, double* coeffs, int cap, int* count) {
-    Ham H = make_ham(kind, n, lx, ly, J, h, sign);
+    Ham H = make_ham(kind, n, lx, ly, hp);
     std::vector<FlipTerm> t;
     double d = ham_enumerate(H, s, t);
     int c = 0;
@@ -108,9 +112,9 @@ double orc_ham_enumerate(int kind, int n, int lx, int ly, double J, double h, do
     return d;
 }
 
-int orc_ham_column(int kind, int n, int lx, int ly, double J, double h, double sign, uint64_t col, uint64_t* rows,
+int orc_ham_column(int kind, int n, int lx, int ly, const double* hp, uint64_t col, uint64_t* rows,
                    double* vals, int cap) {
-    Ham H = make_ham(kind, n, lx, ly, J, h, sign);
+    Ham H = make_ham(kind, n, lx, ly, hp);
     auto mp = ham_column(H, col);
     int c = 0;
     for (auto& kv : mp) {
@@ -123,9 +127,9 @@ int orc_ham_column(int kind, int n, int lx, int ly, double J, double h, double s
     return c;
 }
 
-void orc_eloc(int kind, int n, int lx, int ly, double J, double h, double sign, int m, int use_bias,
+void orc_eloc(int kind, int n, int lx, int ly, const double* hp, int m, int use_bias,
               const double* params, int ns, const int8_t* s, const double* theta, double* out, int nthreads) {
-    Ham H = make_ham(kind, n, lx, ly, J, h, sign);
+    Ham H = make_ham(kind, n, lx, ly, hp);
     RBM q = make_rbm(n, m, use_bias, params);
     const cd* th = reinterpret_cast<const cd*>(theta);
     cd* o = reinterpret_cast<cd*>(out);
@@ -174,11 +178,11 @@ void orc_sample_pt(int n, int m, int use_bias, const double* params, int n_chain
 
 // One SR step on given samples.  out_v/out_grad/out_oloc: P complex; out_eloc: ns complex;
 // out_stats: [energy, energy_var, cg_iters, cg_relres].  Returns the Cholesky status.
-int orc_sr_step(int kind, int n, int lx, int ly, double J, double h, double sign, int m, int use_bias,
+int orc_sr_step(int kind, int n, int lx, int ly, const double* hp, int m, int use_bias,
                 const double* params, int ns, const int8_t* s, const double* theta, double shift, int mode, int solver,
                 double cgtol, double* out_v, double* out_grad, double* out_oloc, double* out_eloc,
                 double* out_stats, int nthreads) {
-    Ham H = make_ham(kind, n, lx, ly, J, h, sign);
+    Ham H = make_ham(kind, n, lx, ly, hp);
     RBM q = make_rbm(n, m, use_bias, params);
     SRResult R = sr_step(q, H, ns, s, reinterpret_cast<const cd*>(theta), shift, mode, solver, cgtol, nthreads);
     const size_t P = q.dim();
@@ -206,10 +210,10 @@ int orc_cholesky_solve(int nn, double* A, double* b) {
 }
 
 // basis_kind: 0 full, 1 fixed popcount nup.  out_S may be null.
-int orc_exact(int kind, int n, int lx, int ly, double J, double h, double sign, int m, int use_bias,
+int orc_exact(int kind, int n, int lx, int ly, const double* hp, int m, int use_bias,
               const double* params, int basis_kind, int nup, double* out_stats, double* out_oloc, double* out_grad,
               double* out_S, int nthreads) {
-    Ham H = make_ham(kind, n, lx, ly, J, h, sign);
+    Ham H = make_ham(kind, n, lx, ly, hp);
     RBM q = make_rbm(n, m, use_bias, params);
     auto basis = basis_kind == 0 ? basis_full(n) : basis_jz(n, nup);
     ExactResult X = exact_sr(q, H, basis, nthreads, out_S != nullptr);
@@ -240,9 +244,9 @@ int orc_basis(int n, int basis_kind, int nup, uint64_t* out, int cap) {
     return int(b.size());
 }
 
-double orc_ed_ground(int kind, int n, int lx, int ly, double J, double h, double sign, int basis_kind, int nup,
+double orc_ed_ground(int kind, int n, int lx, int ly, const double* hp, int basis_kind, int nup,
                      int maxit, int nthreads) {
-    Ham H = make_ham(kind, n, lx, ly, J, h, sign);
+    Ham H = make_ham(kind, n, lx, ly, hp);
     auto basis = basis_kind == 0 ? basis_full(n) : basis_jz(n, nup);
     return ed_ground_energy(H, basis, maxit, nthreads);
 }

@@ -16,7 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
 # Hamiltonian kinds (oracle.hpp)
-TFI, XXZ, TFI2D = 0, 1, 2
+TFI, XXZ, TFI2D, XXX, J1J2, XYZNNN, KITAEV_HEX = 0, 1, 2, 3, 4, 5, 6
 MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN = 0, 1, 2
 SR_S, SR_T = 0, 1
 SOLVE_LLT, SOLVE_CG = 0, 1
@@ -60,18 +60,18 @@ def _declare(L):
         "orc_logratio": (None, [i, i, i, vp, vp, vp, i, vp, vp]),
         "orc_flip": (None, [i, i, i, vp, vp, vp, i, vp]),
         "orc_logderiv": (None, [i, i, i, vp, vp, vp, vp]),
-        "orc_ham_enumerate": (d, [i, i, i, i, d, d, d, vp, vp, vp, i, vp]),
-        "orc_ham_column": (i, [i, i, i, i, d, d, d, u64, vp, vp, i]),
-        "orc_eloc": (None, [i, i, i, i, d, d, d, i, i, vp, i, vp, vp, vp, i]),
+        "orc_ham_enumerate": (d, [i, i, i, i, vp, vp, vp, vp, i, vp]),
+        "orc_ham_column": (i, [i, i, i, i, vp, u64, vp, vp, i]),
+        "orc_eloc": (None, [i, i, i, i, vp, i, i, vp, i, vp, vp, vp, i]),
         "orc_random_sigma": (None, [i, i, u64, u32, u32, vp]),
         "orc_sample": (None, [i, i, i, vp, i, i, i, u64, u32, i, i, i, i, vp, vp, vp, vp, i]),
         "orc_sample_pt": (None, [i, i, i, vp, i, i, i, i, u64, u32, i, i, i, i, vp, vp, vp, vp, vp, i]),
-        "orc_sr_step": (i, [i, i, i, i, d, d, d, i, i, vp, i, vp, vp, d, i, i, d, vp, vp, vp, vp, vp, i]),
+        "orc_sr_step": (i, [i, i, i, i, vp, i, i, vp, i, vp, vp, d, i, i, d, vp, vp, vp, vp, vp, i]),
         "orc_cholesky_solve": (i, [i, vp, vp]),
-        "orc_exact": (i, [i, i, i, i, d, d, d, i, i, vp, i, i, vp, vp, vp, vp, i]),
+        "orc_exact": (i, [i, i, i, i, vp, i, i, vp, i, i, vp, vp, vp, vp, i]),
         "orc_exact_sample": (i, [i, i, i, vp, i, i, i, u64, u32, vp, vp, i]),
         "orc_basis": (i, [i, i, i, vp, i]),
-        "orc_ed_ground": (d, [i, i, i, i, d, d, d, i, i, i, i]),
+        "orc_ed_ground": (d, [i, i, i, i, vp, i, i, i, i]),
         "orc_ff_forward": (d, [i, i, i, i, vp, vp]),
         "orc_ff_backward": (None, [i, i, i, i, vp, vp, vp]),
         "orc_ff_batch": (None, [i, i, i, i, vp, i, vp, vp, vp, i]),
@@ -86,13 +86,19 @@ def _declare(L):
 class Ham:
     """Hamiltonian descriptor with the reference's sign conventions.
 
-    TFI:   E_loc = sum_i J s_i s_{i+1} + h ratio(i)         (TFIsing(n, J, h))
-    XXZ:   E_loc = sum_i J Delta zz_i + sign J (1 - zz_i) ratio(i, i+1)
-    TFI2D: E_loc = sum_i J s_i (s_right + s_down) + h ratio(i)  on an lx x ly torus
+    TFI:    E_loc = sum_i J s_i s_{i+1} + h ratio(i)         (TFIsing(n, J, h))
+    XXZ:    E_loc = sum_i J Delta zz_i + sign J (1 - zz_i) ratio(i, i+1)
+    TFI2D:  E_loc = sum_i J s_i (s_right + s_down) + h ratio(i)  on an lx x ly torus
+    XXX:    XXX(n)                      J = h = 0
+    J1J2:   J1J2(n, J1, J2, signRule)   J = J1, h = J2
+    XYZNNN: XYZNNN(n, a, b)             J = a, h = b
+    KITAEV_HEX: KitaevHex(n_, m_, Jx, Jy, Jz) plus field h; lx = n_, ly = m_
     """
 
-    def __init__(self, kind, n, J, h, sign=1.0, lx=0, ly=0):
+    def __init__(self, kind, n, J, h, sign=1.0, lx=0, ly=0, jy=0.0, jz=0.0):
         self.kind, self.n, self.J, self.h, self.sign, self.lx, self.ly = kind, n, J, h, sign, lx, ly
+        self.jy, self.jz = jy, jz
+        self._hp = np.array([J, h, sign, jy, jz], dtype=np.float64)
 
     @classmethod
     def tfi(cls, n, J, h):
@@ -106,8 +112,24 @@ class Ham:
     def tfi2d(cls, lx, ly, J, h):
         return cls(TFI2D, lx * ly, J, h, 1.0, lx, ly)
 
+    @classmethod
+    def xxx(cls, n):
+        return cls(XXX, n, 0.0, 0.0)
+
+    @classmethod
+    def j1j2(cls, n, J1, J2, sign_rule=False):
+        return cls(J1J2, n, J1, J2, -1.0 if sign_rule else 1.0)
+
+    @classmethod
+    def xyznnn(cls, n, a, b):
+        return cls(XYZNNN, n, a, b)
+
+    @classmethod
+    def kitaev_hex(cls, ncol, nrow, Jx, Jy, Jz, h=0.0):
+        return cls(KITAEV_HEX, ncol * nrow, Jx, h, 1.0, ncol, nrow, Jy, Jz)
+
     def args(self):
-        return (self.kind, self.n, self.lx, self.ly, self.J, self.h, self.sign)
+        return (self.kind, self.n, self.lx, self.ly, _p(self._hp))
 
 
 def rbm_dim(n, m, use_bias=True):

@@ -1,0 +1,54 @@
+// The further Hamiltonian adapters (XXX, J1J2, XYZNNN, KitaevHex) in the
+// reference's constructor forms, and a RunRBM-style run on the J1J2 chain
+// (Hamiltonians/J1J2.hpp:14-56, N = 12, J1 = 1, J2 = 0.2, sign rule) with
+// exchange moves at zero magnetisation.  Prints "TERMS <name> <n> <requests>"
+// for every model and a final "OK E/N first last" line; exits non-zero if the
+// energy does not go down.
+#include <cstdio>
+#include <vector>
+
+#include "yannq_gpu/yannq_gpu.hpp"
+
+namespace {
+void terms(const char* name, const yannq::gpu::Hamiltonian& h) {
+    int k = 0;
+    yannq::gpu::check(yq_ham_num_offdiag(h.handle(), &k));
+    std::printf("TERMS %s %d %d\n", name, h.size(), k);
+}
+}  // namespace
+
+int main(int argc, char** argv) {
+    using namespace yannq::gpu;
+    const unsigned N = 12, alpha = 1;
+    const int epochs = argc > 1 ? std::atoi(argv[1]) : 40;
+    Context ctx(0);
+    {
+        XXX xxx(ctx, 10);
+        XYZNNN xyz(ctx, 10, 0.3, 0.7);
+        KitaevHex kit(ctx, 4, 4, 1.0, 0.2);
+        KitaevHex kita(ctx, 4, 4, 0.2, 0.4, 0.6);
+        terms("XXX", xxx);
+        terms("XYZNNN", xyz);
+        terms("KitaevHex", kit);
+        terms("KitaevHexAniso", kita);
+    }
+    J1J2 ham(ctx, int(N), 1.0, 0.2, true);
+    terms("J1J2", ham);
+    RunRBM<std::complex<double>> runner(ctx, N, alpha, true);
+    runner.initializeRandom(20261204, 0.01);
+    runner.setLambda(1e-3, 1.0, 1e-3);
+    runner.setIterParams(epochs, 0);
+    runner.setOptimizer(SGD{0.05, 0.0});
+    SwapSweeper sweeper{N};
+    SamplerMT<RBM<std::complex<double>>, SwapSweeper> sampler(runner.getQs(), 1, 64, sweeper, int(N / 2));
+    std::vector<double> es;
+    auto callback = [&](int ll, double e, double nv, double cgErr, float smp, float slv) {
+        std::printf("%d\t%.10f\t%.4e\t%.1e\t%.3f\t%.3f\n", ll, e, nv, cgErr, smp, slv);
+        es.push_back(e);
+    };
+    runner.run(sampler, callback, ham, 16, 16, 7);
+    double first = es.front(), last = 0.0;
+    for (size_t i = es.size() - 5; i < es.size(); ++i) last += es[i] / 5.0;
+    std::printf("OK %.8f %.8f\n", first / N, last / N);
+    return last < first ? 0 : 1;
+}

@@ -1,27 +1,30 @@
-"""The header-only C++ adapters (include/yannq_gpu/yannq_gpu.hpp): a RunRBM-style
-driver in the reference example's call pattern compiles against them (CPU), and
-on a GPU it runs, the energy goes down towards the exact ground energy."""
+"""The header-only C++ adapters (include/yannq_gpu/yannq_gpu.hpp): RunRBM-style
+drivers in the reference example's call pattern compile against them (CPU), and
+on a GPU they run and the energy goes down towards the exact ground energy: the
+TFI chain with local moves, and the J1J2 chain with exchange moves (which also
+constructs the XXX, XYZNNN and KitaevHex adapters)."""
 import os
 import subprocess
 
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-SRC = os.path.join(ROOT, "tests", "cpp", "rbm_tfi_driver.cpp")
 LIBDIR = os.path.join(ROOT, "yannq_b200")
 
 
-def _build(tmp_path):
-    exe = str(tmp_path / "rbm_tfi_driver")
-    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), SRC, "-o", exe,
+def _build(tmp_path, name="rbm_tfi_driver"):
+    exe = str(tmp_path / name)
+    src = os.path.join(ROOT, "tests", "cpp", name + ".cpp")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), src, "-o", exe,
            "-L", LIBDIR, "-lyannq_b200", f"-Wl,-rpath,{LIBDIR}"]
     out = subprocess.run(cmd, capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
     return exe
 
 
-def test_adapters_compile(tmp_path):
-    _build(tmp_path)
+@pytest.mark.parametrize("name", ["rbm_tfi_driver", "j1j2_driver"])
+def test_adapters_compile(tmp_path, name):
+    _build(tmp_path, name)
 
 
 @pytest.mark.gpu
@@ -32,5 +35,21 @@ def test_adapter_driver_runs(tmp_path, orc):
     last = [l for l in out.stdout.splitlines() if l.startswith("OK")][0].split()
     e_first, e_last = float(last[1]), float(last[2])
     e0 = orc.ed_ground(orc.Ham.tfi(10, -1.0, -1.0)) / 10
+    assert e_last < e_first
+    assert e_last >= e0 - 1e-3
+
+
+@pytest.mark.gpu
+def test_j1j2_driver_runs(tmp_path, orc):
+    exe = _build(tmp_path, "j1j2_driver")
+    out = subprocess.run([exe, "40"], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    terms = {l.split()[1]: (int(l.split()[2]), int(l.split()[3])) for l in out.stdout.splitlines()
+             if l.startswith("TERMS")}
+    assert terms == {"XXX": (10, 10), "XYZNNN": (10, 20), "KitaevHex": (16, 32), "KitaevHexAniso": (16, 32),
+                     "J1J2": (12, 24)}
+    last = [l for l in out.stdout.splitlines() if l.startswith("OK")][0].split()
+    e_first, e_last = float(last[1]), float(last[2])
+    e0 = orc.ed_ground(orc.Ham.j1j2(12, 1.0, 0.2, True), 1, 6) / 12
     assert e_last < e_first
     assert e_last >= e0 - 1e-3

@@ -35,6 +35,13 @@ CASES = [
      1, 5),
     ("tfi2d_3x3_full", lambda o: o.Ham.tfi2d(3, 3, -1.0, -3.0), lambda a, c: a.Hamiltonian.tfi2d(c, 3, 3, -1.0, -3.0),
      9, 18, 0, 0),
+    ("j1j2_12_jz", lambda o: o.Ham.j1j2(12, 1.0, 0.5, True), lambda a, c: a.Hamiltonian.j1j2(c, 12, 1.0, 0.5, True),
+     12, 12, 1, 6),
+    ("xxx10_jz", lambda o: o.Ham.xxx(10), lambda a, c: a.Hamiltonian.xxx(c, 10), 10, 10, 1, 5),
+    ("xyznnn10_full", lambda o: o.Ham.xyznnn(10, 0.3, 0.7), lambda a, c: a.Hamiltonian.xyznnn(c, 10, 0.3, 0.7), 10, 10,
+     0, 0),
+    ("kitaev4x2_full", lambda o: o.Ham.kitaev_hex(4, 2, 1.0, 0.8, 0.6, 0.2),
+     lambda a, c: a.Hamiltonian.kitaev_hex(c, 4, 2, 1.0, 0.8, 0.6, 0.2), 8, 16, 0, 0),
 ]
 
 
@@ -97,9 +104,13 @@ def test_exact_jz_needs_conserving_hamiltonian(ctx, orc):
 
     q = api.RBM(ctx, 8, 8, True, api.C128)
     q.set_params(orc.init_params(8, 8, 1, 0.1))
-    H = api.Hamiltonian.tfi(ctx, 8, -1.0, -1.0)
-    with pytest.raises(api.YQError):
-        api.exact(q, H, api.BASIS_JZ, 4)
+    for H in (api.Hamiltonian.tfi(ctx, 8, -1.0, -1.0), api.Hamiltonian.xyznnn(ctx, 8, 0.3, 0.7),
+              api.Hamiltonian.kitaev_hex(ctx, 4, 2, 1.0, 1.0, 1.0)):
+        with pytest.raises(api.YQError):
+            api.exact(q, H, api.BASIS_JZ, 4)
+        H.close()
+    H = api.Hamiltonian.xyznnn(ctx, 8, 0.5, 0.5)  # a == b: the parallel-pair flips vanish
+    api.exact(q, H, api.BASIS_JZ, 4)
     H.close()
     q.close()
 

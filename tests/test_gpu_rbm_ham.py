@@ -96,14 +96,30 @@ HAMS = [
     ("xxz", lambda o: o.Ham.xxz(12, 1.0, 1.0, True)),
     ("xxz_d", lambda o: o.Ham.xxz(10, 0.7, 1.3, False)),
     ("tfi2d", lambda o: o.Ham.tfi2d(3, 4, -1.0, -3.0)),
+    ("xxx", lambda o: o.Ham.xxx(12)),
+    ("j1j2_sign", lambda o: o.Ham.j1j2(12, 1.0, 0.5, True)),
+    ("j1j2", lambda o: o.Ham.j1j2(11, -0.8, 0.3, False)),
+    ("xyznnn", lambda o: o.Ham.xyznnn(10, 0.3, 0.7)),
+    ("kitaev4x2_field", lambda o: o.Ham.kitaev_hex(4, 2, 1.0, 1.0, 1.0, 0.2)),
+    ("kitaev4x4_aniso", lambda o: o.Ham.kitaev_hex(4, 4, 0.2, 0.4, 0.6)),
+    ("kitaev2x4_field", lambda o: o.Ham.kitaev_hex(2, 4, 0.5, -0.7, 0.9, -0.3)),
 ]
 
 
 def _dev_ham(api, ctx, h):
+    """The device Hamiltonian of an oracle descriptor."""
     if h.kind == 2:
         return api.Hamiltonian.tfi2d(ctx, h.lx, h.ly, h.J, h.h)
     if h.kind == 1:
         return api.Hamiltonian.xxz(ctx, h.n, h.J, h.h, h.sign < 0)
+    if h.kind == 3:
+        return api.Hamiltonian.xxx(ctx, h.n)
+    if h.kind == 4:
+        return api.Hamiltonian.j1j2(ctx, h.n, h.J, h.h, h.sign < 0)
+    if h.kind == 5:
+        return api.Hamiltonian.xyznnn(ctx, h.n, h.J, h.h)
+    if h.kind == 6:
+        return api.Hamiltonian.kitaev_hex(ctx, h.lx, h.ly, h.J, h.jy, h.jz, h.h)
     return api.Hamiltonian.tfi(ctx, h.n, h.J, h.h)
 
 
@@ -120,7 +136,8 @@ def test_flip_enumeration_bit_exact(ctx, orc, name, mk):
     cols = np.arange(1 << n)
     sig = np.array([orc.sigma_of(c, n) for c in cols])
     a, b, c, d = H.enumerate(sig)
-    for k in range(0, len(cols), 7):
+    assert a.shape[1] == len(orc.ham_enumerate(h, sig[0])[1])
+    for k in range(0, len(cols), 7 if n <= 12 else 61):
         dg, masks, coeffs = orc.ham_enumerate(h, sig[k])
         gm = np.array([(1 << int(x)) | ((1 << int(y)) if y >= 0 else 0) for x, y in zip(a[k], b[k])], np.uint64)
         np.testing.assert_array_equal(gm, masks)
@@ -165,3 +182,51 @@ def test_eloc_full_size_2d(ctx, orc):
     got = H.eloc(q, s, th)
     want = orc.eloc(h, m, p, s, th)
     assert np.max(np.abs(got - want)) / (4 * n) < TOL64
+
+
+@pytest.mark.parametrize("name,mk,m", [
+    ("j1j2_64", lambda o: o.Ham.j1j2(64, 1.0, 0.45, True), 128),
+    ("xyznnn_48", lambda o: o.Ham.xyznnn(48, 0.6, -0.4), 96),
+    ("kitaev_12x12", lambda o: o.Ham.kitaev_hex(12, 12, 1.0, 0.8, 0.6, 0.1), 288),
+], ids=["j1j2_64", "xyznnn_48", "kitaev_12x12"])
+@pytest.mark.parametrize("dtype", [1, 0])
+def test_eloc_term_tables_large(ctx, orc, name, mk, m, dtype):
+    """Term-table kinds at sizes where one block covers several table strides."""
+    from yannq_b200 import api
+
+    h = mk(orc)
+    n = h.n
+    q, p = _rbm(api, ctx, orc, n, m, 5, 0.05, dtype)
+    H = _dev_ham(api, ctx, h)
+    rng = np.random.default_rng(9)
+    s = _rand_sigma(rng, 48, n)
+    th = np.array([orc.theta(n, m, p, x) for x in s])
+    got = H.eloc(q, s, th)
+    want = orc.eloc(h, m, p, s, th)
+    tol = TOL64 if dtype == api.C128 else TOL32
+    rel = np.abs(got - want) / np.maximum(np.abs(want), 1.0)
+    assert np.max(rel) < tol, np.max(rel)
+    a, b, c, d = H.enumerate(s)
+    for k in range(0, len(s), 5):
+        dg, masks, coeffs = orc.ham_enumerate(h, s[k], cap=8 * n)
+        np.testing.assert_array_equal(c[k], coeffs)
+        assert d[k] == dg
+    H.close()
+    q.close()
+
+
+def test_term_table_arguments(ctx):
+    from yannq_b200 import api
+
+    with pytest.raises(api.YQError):
+        api.Hamiltonian.j1j2(ctx, 2, 1.0, 0.5)
+    with pytest.raises(api.YQError):
+        api.Hamiltonian.kitaev_hex(ctx, 3, 4, 1.0, 1.0, 1.0)
+    with pytest.raises(api.YQError):
+        api.Hamiltonian(ctx, api.HAM_KITAEV_HEX, 16, 1.0, 0.0)
+    for mk, k in [(lambda: api.Hamiltonian.xxx(ctx, 10), 10), (lambda: api.Hamiltonian.j1j2(ctx, 10, 1, 0.2), 20),
+                  (lambda: api.Hamiltonian.kitaev_hex(ctx, 4, 4, 1, 1, 1), 32),
+                  (lambda: api.Hamiltonian.tfi2d(ctx, 3, 4, -1, -1), 12)]:
+        H = mk()
+        assert H.num_offdiag == k
+        H.close()

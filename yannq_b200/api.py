@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libyannq_b200.so")
 
 OK, E_ARG, E_CUDA, E_NOMEM, E_NOT_PD, E_NONFINITE, E_TIMEOUT, E_STATE, E_UNSUPPORTED = range(9)
 C64, C128 = 0, 1
-HAM_TFI, HAM_XXZ, HAM_TFI2D = 0, 1, 2
+HAM_TFI, HAM_XXZ, HAM_TFI2D, HAM_XXX, HAM_J1J2, HAM_XYZNNN, HAM_KITAEV_HEX = 0, 1, 2, 3, 4, 5, 6
 MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN = 0, 1, 2
 SR_AUTO, SR_S, SR_T = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
@@ -68,7 +68,9 @@ SIGNATURES = {
     "yq_rbm_log_deriv": [_vp, _i, _vp, _vp, _vp],
     "yq_rbm_oloc_noalloc": [_vp, _i, _vp, _vp, _vp],
     "yq_ham_create": [_vp, _i, _i, _i, _i, _d, _d, _i, _vp],
+    "yq_ham_create_kitaev_hex": [_vp, _i, _i, _d, _d, _d, _d, _vp],
     "yq_ham_destroy": [_vp],
+    "yq_ham_num_offdiag": [_vp, _vp],
     "yq_ham_enumerate": [_vp, _i, _vp, _vp, _vp, _vp, _vp],
     "yq_eloc": [_vp, _vp, _i, _vp, _vp, _vp],
     "yq_sampler_create": [_vp, _i, _i, _i, _i, _vp],
@@ -277,11 +279,13 @@ class RBM:
 
 
 class Hamiltonian:
-    def __init__(self, ctx, kind, n, J, h, sign_rule=False, lx=0, ly=0):
+    def __init__(self, ctx, kind, n, J, h, sign_rule=False, lx=0, ly=0, _handle=None):
         self.ctx, self.kind, self.n = ctx, kind, n
-        hh = C.c_void_p()
-        check(lib().yq_ham_create(ctx.h, kind, n, lx, ly, J, h, int(sign_rule), C.byref(hh)))
-        self.h = hh
+        if _handle is None:
+            hh = C.c_void_p()
+            check(lib().yq_ham_create(ctx.h, kind, n, lx, ly, J, h, int(sign_rule), C.byref(hh)))
+            _handle = hh
+        self.h = _handle
 
     @classmethod
     def tfi(cls, ctx, n, J, h):
@@ -295,17 +299,45 @@ class Hamiltonian:
     def tfi2d(cls, ctx, lx, ly, J, h):
         return cls(ctx, HAM_TFI2D, lx * ly, J, h, False, lx, ly)
 
+    @classmethod
+    def xxx(cls, ctx, n):
+        """Hamiltonians/XXX.hpp: XXX(n)."""
+        return cls(ctx, HAM_XXX, n, 0.0, 0.0)
+
+    @classmethod
+    def j1j2(cls, ctx, n, J1, J2, sign_rule=False):
+        """Hamiltonians/J1J2.hpp: J1J2(n, J1, J2, signRule)."""
+        return cls(ctx, HAM_J1J2, n, J1, J2, sign_rule)
+
+    @classmethod
+    def xyznnn(cls, ctx, n, a, b):
+        """Hamiltonians/XYZNNN.hpp: XYZNNN(n, a, b)."""
+        return cls(ctx, HAM_XYZNNN, n, a, b)
+
+    @classmethod
+    def kitaev_hex(cls, ctx, ncol, nrow, Jx, Jy, Jz, h=0.0):
+        """Hamiltonians/KitaevHex.hpp: KitaevHex(ncol, nrow, Jx, Jy, Jz) with field h."""
+        hh = C.c_void_p()
+        check(lib().yq_ham_create_kitaev_hex(ctx.h, ncol, nrow, Jx, Jy, Jz, h, C.byref(hh)))
+        return cls(ctx, HAM_KITAEV_HEX, ncol * nrow, Jx, h, _handle=hh)
+
     def close(self):
         if self.h:
             check(lib().yq_ham_destroy(self.h))
             self.h = None
 
+    @property
+    def num_offdiag(self):
+        k = C.c_int()
+        check(lib().yq_ham_num_offdiag(self.h, C.byref(k)))
+        return k.value
+
     def enumerate(self, sigma):
         s = _s8(sigma).reshape(-1, self.n)
-        ns = s.shape[0]
-        a = np.zeros((ns, self.n), np.int32)
-        b = np.zeros((ns, self.n), np.int32)
-        c = np.zeros((ns, self.n))
+        ns, K = s.shape[0], self.num_offdiag
+        a = np.zeros((ns, K), np.int32)
+        b = np.zeros((ns, K), np.int32)
+        c = np.zeros((ns, K))
         d = np.zeros(ns)
         check(lib().yq_ham_enumerate(self.h, ns, _p(s), _p(a), _p(b), _p(c), _p(d)))
         return a, b, c, d

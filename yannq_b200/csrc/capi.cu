@@ -1,6 +1,7 @@
 // C ABI of libyannq_b200 (include/yannq_b200.h): argument checks, host staging
 // for the batch entry points, and the VMC iteration driver.
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -407,26 +408,62 @@ int yq_ham_create(yq_ctx ctx, int kind, int n, int lx, int ly, double J, double 
         need(ctx, "ctx");
         need(out, "out");
         *out = nullptr;
-        if (kind != YQ_HAM_TFI && kind != YQ_HAM_XXZ && kind != YQ_HAM_TFI2D)
-            throw Error(YQ_E_ARG, "ham: unknown kind");
+        if (kind != YQ_HAM_TFI && kind != YQ_HAM_XXZ && kind != YQ_HAM_TFI2D && kind != YQ_HAM_XXX &&
+            kind != YQ_HAM_J1J2 && kind != YQ_HAM_XYZNNN)
+            throw Error(YQ_E_ARG, kind == YQ_HAM_KITAEV_HEX ? "ham: KitaevHex is made by yq_ham_create_kitaev_hex"
+                                                            : "ham: unknown kind");
         if (n < 2) throw Error(YQ_E_ARG, "ham: need n >= 2");
+        if ((kind == YQ_HAM_J1J2 || kind == YQ_HAM_XYZNNN) && n < 3)
+            throw Error(YQ_E_ARG, "ham: next-nearest-neighbour models need n >= 3");
         if (kind == YQ_HAM_TFI2D && (lx < 2 || ly < 2 || lx * ly != n))
             throw Error(YQ_E_ARG, "ham: TFI2D needs lx, ly >= 2 and lx * ly == n");
-        auto* H = new yq_ham_s();
+        auto H = std::make_unique<yq_ham_s>();
         H->ctx = ctx;
         H->kind = kind;
         H->n = n;
-        H->lx = lx;
-        H->ly = ly;
+        H->lx = kind == YQ_HAM_TFI2D ? lx : 0;
+        H->ly = kind == YQ_HAM_TFI2D ? ly : 0;
         H->J = J;
         H->h = h;
         H->sign = sign_rule ? -1.0 : 1.0;
-        *out = H;
+        H->conserves_sz = kind == YQ_HAM_XXZ;
+        if (kind >= YQ_HAM_XXX) ham_build_terms(H.get(), 0.0, 0.0);
+        *out = H.release();
+    });
+}
+
+int yq_ham_create_kitaev_hex(yq_ctx ctx, int ncol, int nrow, double Jx, double Jy, double Jz, double h,
+                             yq_ham* out) {
+    return guard([&] {
+        need(ctx, "ctx");
+        need(out, "out");
+        *out = nullptr;
+        if (ncol < 2 || nrow < 2 || ncol % 2 || nrow % 2)
+            throw Error(YQ_E_ARG, "ham: KitaevHex needs even ncol, nrow >= 2");
+        if (ncol > 65535 || nrow > 65535 || ncol * nrow > 65535) throw Error(YQ_E_ARG, "ham: KitaevHex lattice too large");
+        auto H = std::make_unique<yq_ham_s>();
+        H->ctx = ctx;
+        H->kind = YQ_HAM_KITAEV_HEX;
+        H->n = ncol * nrow;
+        H->lx = ncol;
+        H->ly = nrow;
+        H->J = Jx;
+        H->h = h;
+        ham_build_terms(H.get(), Jy, Jz);
+        *out = H.release();
     });
 }
 
 int yq_ham_destroy(yq_ham H) {
     return guard([&] { delete H; });
+}
+
+int yq_ham_num_offdiag(yq_ham H, int* count) {
+    return guard([&] {
+        need(H, "ham");
+        need(count, "count");
+        *count = ham_num_offdiag(H);
+    });
 }
 
 int yq_ham_enumerate(yq_ham H, int ns, const int8_t* sigma, int* site_a, int* site_b, double* coeff, double* diag) {
@@ -440,16 +477,17 @@ int yq_ham_enumerate(yq_ham H, int ns, const int8_t* sigma, int* site_a, int* si
         if (ns < 0) throw Error(YQ_E_ARG, "ns < 0");
         check_sigma(sigma, size_t(ns) * H->n);
         cudaStream_t st = H->ctx->stream;
+        const size_t K = size_t(ham_num_offdiag(H));
         Staging ss, sa, sb, sc, sd;
         int8_t* ds = ss.up(sigma, size_t(ns) * H->n, st);
-        int* da = sa.alloc<int>(size_t(ns) * H->n);
-        int* db = sb.alloc<int>(size_t(ns) * H->n);
-        double* dc = sc.alloc<double>(size_t(ns) * H->n);
+        int* da = sa.alloc<int>(size_t(ns) * K);
+        int* db = sb.alloc<int>(size_t(ns) * K);
+        double* dc = sc.alloc<double>(size_t(ns) * K);
         double* dd = sd.alloc<double>(ns);
         ham_enumerate(H, ns, ds, da, db, dc, dd);
-        down(site_a, da, size_t(ns) * H->n, st);
-        down(site_b, db, size_t(ns) * H->n, st);
-        down(coeff, dc, size_t(ns) * H->n, st);
+        down(site_a, da, size_t(ns) * K, st);
+        down(site_b, db, size_t(ns) * K, st);
+        down(coeff, dc, size_t(ns) * K, st);
         down(diag, dd, size_t(ns), st);
     });
 }

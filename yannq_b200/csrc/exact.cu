@@ -384,8 +384,8 @@ void basis_state(yq_rbm_s* q, int kind, int nup, BasisState& bs) {
 void exact_summation(yq_rbm_s* q, yq_ham_s* H, int kind, int nup, double* stats, c128* d_oloc, c128* d_grad,
                      c128* d_S) {
     YQ_CHECK_ARG(H->n == q->n, "exact: Hamiltonian and RBM sizes differ");
-    YQ_CHECK_ARG(kind != YQ_BASIS_JZ || H->kind == YQ_HAM_XXZ,
-                 "exact: the Jz basis needs a Hamiltonian that conserves Sz (XXZ)");
+    YQ_CHECK_ARG(kind != YQ_BASIS_JZ || H->conserves_sz,
+                 "exact: the Jz basis needs a Hamiltonian that conserves Sz (XXZ, XXX, J1J2)");
     cudaStream_t st = q->ctx->stream;
     rbm_prepare(q);
     BasisState bs;

@@ -2,6 +2,13 @@
 // E_loc(sigma) = sum_terms coeff * psi(sigma')/psi(sigma) + diagonal
 // (Hamiltonians/TFIsing.hpp:28-39, Hamiltonians/XXZ.hpp:37-49, and the 2D TFI
 // model built on the same concept), reusing the sample's theta cache.
+//
+// TFI, XXZ and TFI2D are evaluated from closed-form site rules.  XXX, J1J2,
+// XYZNNN and KitaevHex are term tables (HamTerm) built on the host in the
+// reference's evaluation order (XXX.hpp:11-22, J1J2.hpp:35-56,
+// XYZNNN.hpp:33-53, KitaevHex.hpp:119-146); the kernels walk the table.
+#include <vector>
+
 #include "internal.hpp"
 #include "ratio.cuh"
 
@@ -10,7 +17,26 @@ namespace yq {
 struct HamDesc {
     int kind, n, lx, ly;
     double J, h, sign;
+    const HamTerm* terms;  // term-table kinds, else null
+    int nterms;
 };
+
+// Diagonal addend and off-diagonal request of term T in state s: request flips
+// of a (and b >= 0) with coefficient c, or none when a < 0.
+__device__ __forceinline__ void table_term(const HamTerm& T, const int8_t* s, double& d, int& a, int& b,
+                                           double& c) {
+    const int zz = T.b >= 0 ? s[T.a] * s[T.b] : 1;
+    d = T.has_diag ? (zz > 0 ? T.dp : T.dm) : 0.0;
+    if (T.nflip == 0) {
+        a = -1;
+        b = -1;
+        c = 0.0;
+        return;
+    }
+    a = T.a;
+    b = T.nflip == 2 ? T.b : -1;
+    c = zz > 0 ? T.cp : T.cm;
+}
 
 __device__ __forceinline__ int right_of(const HamDesc& H, int i) {
     if (H.kind == YQ_HAM_TFI2D) {
@@ -70,12 +96,128 @@ __global__ void enumerate_kernel(HamDesc H, int ns, const int8_t* __restrict__ s
     od[smp] = diag;
 }
 
-static HamDesc desc(const yq_ham_s* H) { return HamDesc{H->kind, H->n, H->lx, H->ly, H->J, H->h, H->sign}; }
+// Term-table form: one thread per sample walks the table in order, so the
+// diagonal is summed in the reference's order and the requests come out in it.
+__global__ void enumerate_table_kernel(HamDesc H, int n_off, int ns, const int8_t* __restrict__ sigma,
+                                       int* __restrict__ oa, int* __restrict__ ob, double* __restrict__ oc,
+                                       double* __restrict__ od) {
+    int smp = blockIdx.x * blockDim.x + threadIdx.x;
+    if (smp >= ns) return;
+    const int8_t* s = sigma + size_t(smp) * H.n;
+    double diag = 0.;
+    int k = 0;
+    for (int t = 0; t < H.nterms; ++t) {
+        double d, c;
+        int a, b;
+        table_term(H.terms[t], s, d, a, b, c);
+        if (H.terms[t].has_diag) diag += d;
+        if (a < 0) continue;
+        const size_t o = size_t(smp) * n_off + k++;
+        oa[o] = a;
+        ob[o] = b;
+        oc[o] = c;
+    }
+    od[smp] = diag;
+}
+
+static HamDesc desc(const yq_ham_s* H) {
+    return HamDesc{H->kind, H->n, H->lx, H->ly, H->J, H->h, H->sign, H->terms.as<HamTerm>(), H->nterms};
+}
+
+int ham_num_offdiag(const yq_ham_s* H) { return H->nterms > 0 ? H->n_off : H->n; }
 
 void ham_enumerate(yq_ham_s* H, int ns, const int8_t* d_sigma, int* d_a, int* d_b, double* d_c, double* d_diag) {
     if (ns <= 0) return;
-    enumerate_kernel<<<cdiv_u(ns, 128), 128, 0, H->ctx->stream>>>(desc(H), ns, d_sigma, d_a, d_b, d_c, d_diag);
+    if (H->nterms > 0)
+        enumerate_table_kernel<<<cdiv_u(ns, 128), 128, 0, H->ctx->stream>>>(desc(H), H->n_off, ns, d_sigma, d_a, d_b,
+                                                                            d_c, d_diag);
+    else
+        enumerate_kernel<<<cdiv_u(ns, 128), 128, 0, H->ctx->stream>>>(desc(H), ns, d_sigma, d_a, d_b, d_c, d_diag);
     YQ_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Term tables.  The coefficients are formed with the reference's expressions,
+// once for zz = s_a s_b = +1 and once for zz = -1.
+namespace {
+
+HamTerm pair_term(int a, int b, bool diag, double dp, double dm, bool flip, double cp, double cm) {
+    return HamTerm{a, b, flip ? 2 : 0, diag ? 1 : 0, dp, dm, cp, cm};
+}
+
+// KitaevHex.hpp:33-103: row r holds ncol/2 black sites r*ncol + c, then ncol/2
+// white sites r*ncol + ncol/2 + c; rows and columns are periodic.
+std::vector<std::pair<int, int>> honeycomb_links(int ncol, int nrow, int axis) {
+    const int half = ncol / 2;
+    auto per = [](int v, int p) { return ((v % p) + p) % p; };
+    auto site = [&](int r, int c, bool white) { return per(r, nrow) * ncol + per(c, half) + (white ? half : 0); };
+    std::vector<std::pair<int, int>> links;
+    if (axis == 2) {  // z: white (r, c) -- black (r + 1, c)
+        for (int r = 0; r < nrow; ++r)
+            for (int c = 0; c < half; ++c) links.emplace_back(site(r, c, true), site(r + 1, c, false));
+        return links;
+    }
+    // x: black (r, c) -- white (r, c - 1) on even rows, white (r, c) on odd rows;
+    // y: black (r, c) -- white (r, c) on even rows, white (r, c + 1) on odd rows.
+    for (int odd = 0; odd < 2; ++odd)
+        for (int r = odd; r < nrow; r += 2)
+            for (int c = 0; c < half; ++c)
+                links.emplace_back(site(r, c, false), site(r, c + (axis == 0 ? odd - 1 : odd), true));
+    return links;
+}
+
+}  // namespace
+
+void ham_build_terms(yq_ham_s* H, double jy, double jz) {
+    std::vector<HamTerm> T;
+    const int n = H->n;
+    if (H->kind == YQ_HAM_XXX) {
+        // XXX.hpp:15-19: yysign = s_i s_{i+1}; s += yysign + (1 - yysign) ratio(i, i+1)
+        auto off = [](double yy) { return 1.0 - yy; };
+        for (int i = 0; i < n; ++i) T.push_back(pair_term(i, (i + 1) % n, true, 1.0, -1.0, true, off(1.0), off(-1.0)));
+    } else if (H->kind == YQ_HAM_J1J2 || H->kind == YQ_HAM_XYZNNN) {
+        // J1J2.hpp:40-53 / XYZNNN.hpp:38-51: yysign = -s_i s_j; s += -J yysign + c(yysign) ratio(i, j),
+        // nearest neighbours (j = i + 1) first, then next-nearest (j = i + 2)
+        const bool j1j2 = H->kind == YQ_HAM_J1J2;
+        const double J1 = j1j2 ? H->J : -1.0, J2 = j1j2 ? H->h : -1.0;
+        const double a = H->J, b = H->h, sign = H->sign;
+        for (int d = 1; d <= 2; ++d) {
+            const double Jd = d == 1 ? J1 : J2;
+            auto off = [&](double yy) {
+                if (j1j2) return d == 1 ? J1 * sign * (1.0 + yy) : J2 * (1.0 + yy);
+                return d == 1 ? J1 * (a + yy * b) : J2 * (b + yy * a);
+            };
+            // zz = +1 means yysign = -1
+            for (int i = 0; i < n; ++i)
+                T.push_back(pair_term(i, (i + d) % n, true, -Jd * -1.0, -Jd * 1.0, true, off(-1.0), off(1.0)));
+        }
+    } else if (H->kind == YQ_HAM_KITAEV_HEX) {
+        // KitaevHex.hpp:125-144: h ratio(i) for every site, Jx ratio(x-link),
+        // -Jy zz ratio(y-link), Jz zz for every z-link
+        const double Jx = H->J, h = H->h;
+        for (int i = 0; i < n; ++i) T.push_back(HamTerm{i, -1, 1, 0, 0.0, 0.0, h, h});
+        for (auto& e : honeycomb_links(H->lx, H->ly, 0))
+            T.push_back(pair_term(e.first, e.second, false, 0.0, 0.0, true, Jx, Jx));
+        for (auto& e : honeycomb_links(H->lx, H->ly, 1))
+            T.push_back(pair_term(e.first, e.second, false, 0.0, 0.0, true, -jy * 1, -jy * -1));
+        for (auto& e : honeycomb_links(H->lx, H->ly, 2))
+            T.push_back(pair_term(e.first, e.second, true, jz * 1, jz * -1, false, 0.0, 0.0));
+    } else {
+        throw Error(YQ_E_ARG, "ham: not a term-table kind");
+    }
+    int n_off = 0;
+    bool cons = true;
+    for (const HamTerm& t : T) {
+        if (t.nflip == 0) continue;
+        ++n_off;
+        // one flip changes Sz; two flips of parallel spins (zz = +1) change it by 2
+        if (t.cp != 0.0 || (t.nflip == 1 && t.cm != 0.0)) cons = false;
+    }
+    H->nterms = int(T.size());
+    H->n_off = n_off;
+    H->conserves_sz = cons;
+    H->terms.ensure(T.size() * sizeof(HamTerm));
+    YQ_CUDA(cudaMemcpy(H->terms.p, T.data(), T.size() * sizeof(HamTerm), cudaMemcpyHostToDevice));
 }
 
 // ---------------------------------------------------------------------------
@@ -111,11 +253,20 @@ __global__ void __launch_bounds__(256) eloc_kernel(ElocArgs<R> A) {
         }
         __syncthreads();
         c128 acc = mk(0., 0.);
-        for (int i = tid; i < n; i += nt) {
-            acc.re += diag_term(A.H, s, i);
+        const bool table = A.H.nterms > 0;
+        const int nterm = table ? A.H.nterms : n;
+        for (int i = tid; i < nterm; i += nt) {
             int ka, kb;
             double c;
-            offdiag_term(A.H, s, i, ka, kb, c);
+            if (table) {
+                double d;
+                table_term(A.H.terms[i], s, d, ka, kb, c);
+                acc.re += d;
+                if (ka < 0) continue;
+            } else {
+                acc.re += diag_term(A.H, s, i);
+                offdiag_term(A.H, s, i, ka, kb, c);
+            }
             if (c == 0.0) continue;  // zero coefficient: the reference multiplies the ratio by 0
             c128 val;
             if (kb < 0) {

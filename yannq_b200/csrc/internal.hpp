@@ -48,10 +48,24 @@ struct yq_rbm_s {
     size_t csize() const { return dtype == YQ_C64 ? sizeof(yq::c64) : sizeof(yq::c128); }
 };
 
+// One entry of a term-table Hamiltonian (kinds XXX, J1J2, XYZNNN, KitaevHex):
+// for zz = s_a s_b (1 when b < 0) the diagonal gains (zz > 0 ? dp : dm) when
+// has_diag, and flipping a (and b when nflip == 2) is requested with
+// coefficient (zz > 0 ? cp : cm) when nflip > 0.  The four values are formed on
+// the host with the reference's own expressions for zz = +1 and zz = -1.
+struct HamTerm {
+    int a, b, nflip, has_diag;
+    double dp, dm, cp, cm;
+};
+
 struct yq_ham_s {
     yq_ctx_s* ctx = nullptr;
     int kind = 0, n = 0, lx = 0, ly = 0;
     double J = 0., h = 0., sign = 1.;
+    // term-table kinds: terms in the reference's evaluation order
+    int nterms = 0, n_off = 0;  // n_off: off-diagonal requests per sample
+    bool conserves_sz = false;  // every request keeps the number of down spins
+    yq::DevBuf terms;           // nterms HamTerm
 };
 
 struct yq_sampler_s {
@@ -152,6 +166,8 @@ void rbm_init_params_host(int n, int m, bool bias, uint64_t seed, double sd, c12
 
 void sampler_run(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, uint32_t epoch, int reinit);
 
+void ham_build_terms(yq_ham_s* H, double jy, double jz);  // term-table kinds
+int ham_num_offdiag(const yq_ham_s* H);
 void ham_enumerate(yq_ham_s* H, int ns, const int8_t* d_sigma, int* d_a, int* d_b, double* d_c, double* d_diag);
 void ham_eloc(yq_ham_s* H, yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_theta, c128* d_out);
 
