@@ -39,7 +39,7 @@ enum {
 enum { YQ_C64 = 0, YQ_C128 = 1 };                             /* RBM<complex<float|double>> */
 enum { YQ_HAM_TFI = 0, YQ_HAM_XXZ = 1, YQ_HAM_TFI2D = 2,       /* Hamiltonian kinds          */
        YQ_HAM_XXX = 3, YQ_HAM_J1J2 = 4, YQ_HAM_XYZNNN = 5, YQ_HAM_KITAEV_HEX = 6 };
-enum { YQ_MOVE_LOCAL = 0, YQ_MOVE_EXCHANGE_ANY = 1, YQ_MOVE_EXCHANGE_NN = 2 };
+enum { YQ_MOVE_LOCAL = 0, YQ_MOVE_EXCHANGE_ANY = 1, YQ_MOVE_EXCHANGE_NN = 2, YQ_MOVE_HAMILTONIAN = 3 };
 enum { YQ_SR_AUTO = 0, YQ_SR_S = 1, YQ_SR_T = 2 };             /* S = <O^H O>, T = O O^H dual */
 enum { YQ_PREC_FP64 = 0, YQ_PREC_MIXED = 1 };
 enum { YQ_SOLVE_LLT = 0, YQ_SOLVE_CG = 1 };
@@ -163,6 +163,16 @@ int yq_eloc(yq_ham H, yq_rbm q, int ns, const int8_t* sigma, const double* theta
  * otherwise randomSigma(n).  sweep_len 0 means n proposals per sweep. */
 int yq_sampler_create(yq_rbm q, int n_chains, int move, int nup, int sweep_len, yq_sampler* out);
 int yq_sampler_destroy(yq_sampler S);
+/* HamiltonianSweeper(n, ham) -- Samplers/HamiltonianSweeper.hpp:16-50, for a
+ * sampler created with move YQ_MOVE_HAMILTONIAN: every proposal picks one entry
+ * of offDiagonals(sigma) uniformly, flips it, and accepts with
+ * min(1, |psi(sigma')/psi(sigma)|^2 w1 / w2), w1 and w2 the list sizes in sigma
+ * and sigma' (no beta, as the reference's sweep ignores it).  offDiagonals is
+ * TFIsing's list of all n sites (Hamiltonians/TFIsing.hpp:41-50; the same for
+ * the 2D model); for the other kinds it is the state form's off-diagonal requests
+ * whose coefficient in sigma is non-zero.  A proposal slot with an empty list is
+ * skipped.  H must outlive the sampler's use of it. */
+int yq_sampler_set_hamiltonian(yq_sampler S, yq_ham H);
 /* Recompute theta from sigma in FP64 every k recorded/discarded sweeps (0 = never
  * inside one call, as the reference: States/RBMState.hpp:248-255). */
 int yq_sampler_set_resync(yq_sampler S, int every_sweeps);

@@ -215,6 +215,26 @@ struct SwapSweeperNN {
     uint32_t n;
     explicit SwapSweeperNN(uint32_t n_) : n(n_) {}
 };
+// Samplers/HamiltonianSweeper.hpp:16-19: proposals from ham's offDiagonals list
+template <class Ham>
+struct HamiltonianSweeper {
+    static constexpr int move = YQ_MOVE_HAMILTONIAN;
+    uint32_t n;
+    const Ham& ham;
+    HamiltonianSweeper(int n_, const Ham& h) : n(uint32_t(n_)), ham(h) {}
+    yq_ham proposals() const { return ham.handle(); }
+};
+
+namespace detail {
+template <class S>
+auto sweeper_ham(const S& s, int) -> decltype(s.proposals()) {
+    return s.proposals();
+}
+template <class S>
+yq_ham sweeper_ham(const S&, long) {
+    return nullptr;
+}
+}  // namespace detail
 
 // Samples of the last sample() call; they stay on the device.
 struct SampleSet {
@@ -238,6 +258,7 @@ public:
             throw std::invalid_argument("SamplerMT: nTmps must be 1 or even");  // SamplerMT.hpp:50
         if (sw.n != qs.getN()) throw std::invalid_argument("SamplerMT: sweeper size differs from the machine");
         check(yq_sampler_create(qs.handle(), int(nTmps * nChainsPer), Sweeper::move, nup, 0, &h_));
+        if (yq_ham hm = detail::sweeper_ham(sw, 0)) check(yq_sampler_set_hamiltonian(h_, hm));
         if (nTmps > 1) check(yq_sampler_set_tempering(h_, int(nTmps)));
     }
     ~SamplerMT() { yq_sampler_destroy(h_); }

@@ -252,6 +252,74 @@ void random_sigma(int n, int nup, uint64_t seed, uint32_t epoch, uint32_t chain,
     }
 }
 
+// offDiagonals(s) for the HamiltonianSweeper: TFIsing.hpp:41-50 lists every site
+// whatever the state (the 2D model likewise); for the other models, the state
+// form's off-diagonal requests whose coefficient in s is non-zero, in order.
+std::vector<std::array<int, 2>> off_diagonals(const Ham& H, const int8_t* s) {
+    std::vector<std::array<int, 2>> out;
+    if (H.kind == HAM_TFI || H.kind == HAM_TFI2D) {
+        for (int i = 0; i < H.n; ++i) out.push_back({i, -1});
+    } else if (H.kind == HAM_XXZ) {
+        for (int i = 0; i < H.n; ++i) {
+            int j = (i + 1) % H.n;
+            if (H.sign * H.J * (1 - s[i] * s[j]) != 0.0) out.push_back({i, j});
+        }
+    } else {
+        ModelStateForm(H, s, [](double) {}, [&](int a, int b, double c) {
+            if (c != 0.0) out.push_back({a, b});
+        });
+    }
+    return out;
+}
+
+// One proposal of LocalSweeper (LocalSweeper.hpp:42-52), SwapSweeper
+// (SwapSweeper.hpp:39-56, any pair, or its neighbour-pair variant) or
+// HamiltonianSweeper (HamiltonianSweeper.hpp:26-49, which takes no beta) from the
+// draw x.  Returns whether the move was accepted (and applied).
+static bool metropolis_step(const RBM& q, const SampleSpec& sp, int8_t* s, cd* th, const uint32_t x[4],
+                            double beta) {
+    const int n = q.n;
+    const double u = draw_u53(x[2], x[3]);
+    if (sp.move == MOVE_LOCAL) {
+        int k = int(draw_site(x[0], uint32_t(n)));
+        double pr = std::min(1.0, std::exp(beta * 2.0 * q.logRatio1(s, th, k).real()));
+        if (u < pr) {
+            q.flip1(s, th, k);
+            return true;
+        }
+        return false;
+    }
+    if (sp.move == MOVE_HAMILTONIAN) {
+        auto flips = off_diagonals(*sp.ham, s);
+        if (flips.empty()) return false;
+        auto f = flips[draw_site(x[0], uint32_t(flips.size()))];
+        std::vector<int8_t> sp2(s, s + n);
+        sp2[size_t(f[0])] = int8_t(-sp2[size_t(f[0])]);
+        if (f[1] >= 0) sp2[size_t(f[1])] = int8_t(-sp2[size_t(f[1])]);
+        const double w1 = double(flips.size());
+        const double w2 = double(off_diagonals(*sp.ham, sp2.data()).size());
+        const cd lr = f[1] < 0 ? q.logRatio1(s, th, f[0]) : q.logRatio2(s, th, f[0], f[1]);
+        double pr = std::min(1.0, std::exp(2.0 * lr.real()) * (w1 / w2));
+        if (u < pr) {
+            if (f[1] < 0)
+                q.flip1(s, th, f[0]);
+            else
+                q.flip2(s, th, f[0], f[1]);
+            return true;
+        }
+        return false;
+    }
+    int k = int(draw_site(x[0], uint32_t(n)));
+    int l = (sp.move == MOVE_EXCHANGE_ANY) ? int(draw_site(x[1], uint32_t(n))) : (k + 1) % n;
+    if (s[k] == s[l]) return false;
+    double pr = std::min(1.0, std::exp(beta * 2.0 * q.logRatio2(s, th, k, l).real()));
+    if (u < pr) {
+        q.flip2(s, th, k, l);
+        return true;
+    }
+    return false;
+}
+
 void sample(const RBM& q, const SampleSpec& sp, int8_t* chain_sigma, int8_t* out_sigma, cd* out_theta,
             uint64_t* acc, int nthreads) {
     const int n = q.n, m = q.m;
@@ -273,25 +341,7 @@ void sample(const RBM& q, const SampleSpec& sp, int8_t* chain_sigma, int8_t* out
             for (int p = 0; p < L; ++p) {
                 const uint32_t g = uint32_t(sw) * uint32_t(L) + uint32_t(p);
                 Philox4x32::draw(sp.seed, g, sp.epoch, uint32_t(c), TAG_SWEEP, x);
-                const double u = draw_u53(x[2], x[3]);
-                if (sp.move == MOVE_LOCAL) {  // LocalSweeper.hpp:42-52
-                    int k = int(draw_site(x[0], uint32_t(n)));
-                    double pr = std::min(1.0, std::exp(1.0 * 2.0 * q.logRatio1(s.data(), th.data(), k).real()));
-                    if (u < pr) {
-                        q.flip1(s.data(), th.data(), k);
-                        ++nacc;
-                    }
-                } else {  // SwapSweeper.hpp:39-56 (any pair) or its neighbour-pair variant
-                    int k = int(draw_site(x[0], uint32_t(n)));
-                    int l = (sp.move == MOVE_EXCHANGE_ANY) ? int(draw_site(x[1], uint32_t(n))) : (k + 1) % n;
-                    if (s[k] == s[l]) continue;
-                    double pr =
-                        std::min(1.0, std::exp(1.0 * 2.0 * q.logRatio2(s.data(), th.data(), k, l).real()));
-                    if (u < pr) {
-                        q.flip2(s.data(), th.data(), k, l);
-                        ++nacc;
-                    }
-                }
+                if (metropolis_step(q, sp, s.data(), th.data(), x, 1.0)) ++nacc;
             }
             if (sw >= sp.n_discard) {  // SamplerMT.hpp:165-173 (recorded in (sweep, chain) order)
                 size_t idx = size_t(sw - sp.n_discard) * sp.n_chains + c;
@@ -335,24 +385,7 @@ void sample_pt(const RBM& q, const SampleSpec& sp, int ntemps, int8_t* chain_sig
             for (int p = 0; p < L; ++p) {
                 const uint32_t g = uint32_t(sw) * uint32_t(L) + uint32_t(p);
                 Philox4x32::draw(sp.seed, g, sp.epoch, uint32_t(c), TAG_SWEEP, x);
-                const double u = draw_u53(x[2], x[3]);
-                if (sp.move == MOVE_LOCAL) {
-                    int k = int(draw_site(x[0], uint32_t(n)));
-                    double pr = std::min(1.0, std::exp(beta * 2.0 * q.logRatio1(sc, tc, k).real()));
-                    if (u < pr) {
-                        q.flip1(sc, tc, k);
-                        ++nacc[c];
-                    }
-                } else {
-                    int k = int(draw_site(x[0], uint32_t(n)));
-                    int l = (sp.move == MOVE_EXCHANGE_ANY) ? int(draw_site(x[1], uint32_t(n))) : (k + 1) % n;
-                    if (sc[k] == sc[l]) continue;
-                    double pr = std::min(1.0, std::exp(beta * 2.0 * q.logRatio2(sc, tc, k, l).real()));
-                    if (u < pr) {
-                        q.flip2(sc, tc, k, l);
-                        ++nacc[c];
-                    }
-                }
+                if (metropolis_step(q, sp, sc, tc, x, beta)) ++nacc[c];
             }
             lp[c] = q.logCoeff(sc, tc).real();
         }

@@ -20,6 +20,7 @@
 //   * complex numbers are interleaved (re, im) doubles at the C boundary.
 #pragma once
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -166,6 +167,8 @@ struct Ham {
 // KitaevHex link lists (KitaevHex.hpp:33-103), pairs of site indices in the
 // reference's order.
 std::vector<std::pair<int, int>> kitaev_links(const Ham& H, int axis);  // axis 0 = x, 1 = y, 2 = z
+// offDiagonals(s): the flips the HamiltonianSweeper proposes from ({a, -1} or {a, b})
+std::vector<std::array<int, 2>> off_diagonals(const Ham& H, const int8_t* s);
 
 // Off-diagonal flip enumeration of the state form (the "mock state" technique of
 // Tests/HamiltonianHelper.hpp:44-92): each requested ratio becomes a (mask, coeff)
@@ -183,10 +186,11 @@ cd ham_eloc(const Ham& H, const RBM& q, const int8_t* s, const cd* th);
 
 // ---------------------------------------------------------------------------
 // Samplers/LocalSweeper.hpp:32-53, Samplers/SwapSweeper.hpp:28-57, Samplers/SamplerMT.hpp:155-204
-enum Move { MOVE_LOCAL = 0, MOVE_EXCHANGE_ANY = 1, MOVE_EXCHANGE_NN = 2 };
+enum Move { MOVE_LOCAL = 0, MOVE_EXCHANGE_ANY = 1, MOVE_EXCHANGE_NN = 2, MOVE_HAMILTONIAN = 3 };
 struct SampleSpec {
     int n_chains = 1;
     int move = MOVE_LOCAL;
+    const Ham* ham = nullptr;  // MOVE_HAMILTONIAN: Samplers/HamiltonianSweeper.hpp:22-50
     int nup = -1;          // >=0: reinitialise with fixed magnetisation (randomSigma(n, nup))
     uint64_t seed = 0;
     uint32_t epoch = 0;

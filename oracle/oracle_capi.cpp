@@ -143,9 +143,13 @@ void orc_random_sigma(int n, int nup, uint64_t seed, uint32_t epoch, uint32_t ch
 
 void orc_sample(int n, int m, int use_bias, const double* params, int n_chains, int move, int nup, uint64_t seed,
                 uint32_t epoch, int reinit, int n_sweeps, int n_discard, int sweep_len, int8_t* chain_sigma,
-                int8_t* out_sigma, double* out_theta, uint64_t* acc, int nthreads) {
+                int8_t* out_sigma, double* out_theta, uint64_t* acc, int nthreads, int ham_kind, int ham_lx,
+                int ham_ly, const double* ham_hp) {
     RBM q = make_rbm(n, m, use_bias, params);
+    Ham H;
+    if (ham_hp) H = make_ham(ham_kind, n, ham_lx, ham_ly, ham_hp);
     SampleSpec sp;
+    sp.ham = ham_hp ? &H : nullptr;
     sp.n_chains = n_chains;
     sp.move = move;
     sp.nup = nup;
@@ -161,9 +165,12 @@ void orc_sample(int n, int m, int use_bias, const double* params, int n_chains, 
 void orc_sample_pt(int n, int m, int use_bias, const double* params, int n_chains, int ntemps, int move, int nup,
                    uint64_t seed, uint32_t epoch, int reinit, int n_sweeps, int n_discard, int sweep_len,
                    int8_t* chain_sigma, int* slot, int8_t* out_sigma, double* out_theta, uint64_t* acc,
-                   int nthreads) {
+                   int nthreads, int ham_kind, int ham_lx, int ham_ly, const double* ham_hp) {
     RBM q = make_rbm(n, m, use_bias, params);
+    Ham H;
+    if (ham_hp) H = make_ham(ham_kind, n, ham_lx, ham_ly, ham_hp);
     SampleSpec sp;
+    sp.ham = ham_hp ? &H : nullptr;
     sp.n_chains = n_chains;
     sp.move = move;
     sp.nup = nup;

@@ -17,7 +17,7 @@ _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
 # Hamiltonian kinds (oracle.hpp)
 TFI, XXZ, TFI2D, XXX, J1J2, XYZNNN, KITAEV_HEX = 0, 1, 2, 3, 4, 5, 6
-MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN = 0, 1, 2
+MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN, MOVE_HAMILTONIAN = 0, 1, 2, 3
 SR_S, SR_T = 0, 1
 SOLVE_LLT, SOLVE_CG = 0, 1
 
@@ -64,8 +64,8 @@ def _declare(L):
         "orc_ham_column": (i, [i, i, i, i, vp, u64, vp, vp, i]),
         "orc_eloc": (None, [i, i, i, i, vp, i, i, vp, i, vp, vp, vp, i]),
         "orc_random_sigma": (None, [i, i, u64, u32, u32, vp]),
-        "orc_sample": (None, [i, i, i, vp, i, i, i, u64, u32, i, i, i, i, vp, vp, vp, vp, i]),
-        "orc_sample_pt": (None, [i, i, i, vp, i, i, i, i, u64, u32, i, i, i, i, vp, vp, vp, vp, vp, i]),
+        "orc_sample": (None, [i, i, i, vp, i, i, i, u64, u32, i, i, i, i, vp, vp, vp, vp, i, i, i, i, vp]),
+        "orc_sample_pt": (None, [i, i, i, vp, i, i, i, i, u64, u32, i, i, i, i, vp, vp, vp, vp, vp, i, i, i, i, vp]),
         "orc_sr_step": (i, [i, i, i, i, vp, i, i, vp, i, vp, vp, d, i, i, d, vp, vp, vp, vp, vp, i]),
         "orc_cholesky_solve": (i, [i, vp, vp]),
         "orc_exact": (i, [i, i, i, i, vp, i, i, vp, i, i, vp, vp, vp, vp, i]),
@@ -232,21 +232,27 @@ def random_sigma(n, nup, seed, epoch, chain):
     return s
 
 
+def _ham_tail(ham):
+    return (ham.kind, ham.lx, ham.ly, _p(ham._hp)) if ham is not None else (0, 0, 0, None)
+
+
 def sample(n, m, params, n_chains, move=MOVE_LOCAL, nup=-1, seed=0, epoch=0, reinit=True, n_sweeps=1,
-           n_discard=0, sweep_len=0, chain_sigma=None, use_bias=True, nthreads=0):
-    """Restated SamplerMT (nTmps = 1).  Returns (sigma[Ns, n], theta[Ns, m], chain_sigma, acc)."""
+           n_discard=0, sweep_len=0, chain_sigma=None, use_bias=True, nthreads=0, ham=None):
+    """Restated SamplerMT (nTmps = 1).  Returns (sigma[Ns, n], theta[Ns, m], chain_sigma, acc).
+    move MOVE_HAMILTONIAN takes its proposals from `ham` (HamiltonianSweeper)."""
     cs = np.zeros((n_chains, n), dtype=np.int8) if chain_sigma is None else np.ascontiguousarray(chain_sigma, np.int8)
     ns = n_chains * n_sweeps
     osig = np.zeros((ns, n), dtype=np.int8)
     oth = np.zeros((ns, m), dtype=np.complex128)
     acc = np.zeros(n_chains, dtype=np.uint64)
     lib().orc_sample(n, m, int(use_bias), _p(params), n_chains, move, nup, seed, epoch, int(reinit), n_sweeps,
-                     n_discard, sweep_len, _p(cs), _p(osig), _p(oth), _p(acc), nthreads or os.cpu_count())
+                     n_discard, sweep_len, _p(cs), _p(osig), _p(oth), _p(acc), nthreads or os.cpu_count(),
+                     *_ham_tail(ham))
     return osig, oth, cs, acc
 
 
 def sample_pt(n, m, params, n_chains, ntemps, move=MOVE_LOCAL, nup=-1, seed=0, epoch=0, reinit=True, n_sweeps=1,
-              n_discard=0, sweep_len=0, chain_sigma=None, slot=None, use_bias=True, nthreads=0):
+              n_discard=0, sweep_len=0, chain_sigma=None, slot=None, use_bias=True, nthreads=0, ham=None):
     """Restated SamplerMT with nTmps = ntemps > 1 (temperature swaps between the
     chains of a group).  Returns (sigma[groups * n_sweeps, n], theta, chain_sigma, slot, acc)."""
     cs = np.zeros((n_chains, n), dtype=np.int8) if chain_sigma is None else np.ascontiguousarray(chain_sigma, np.int8)
@@ -257,7 +263,7 @@ def sample_pt(n, m, params, n_chains, ntemps, move=MOVE_LOCAL, nup=-1, seed=0, e
     acc = np.zeros(n_chains, dtype=np.uint64)
     lib().orc_sample_pt(n, m, int(use_bias), _p(params), n_chains, ntemps, move, nup, seed, epoch, int(reinit),
                         n_sweeps, n_discard, sweep_len, _p(cs), _p(sl), _p(osig), _p(oth), _p(acc),
-                        nthreads or os.cpu_count())
+                        nthreads or os.cpu_count(), *_ham_tail(ham))
     return osig, oth, cs, sl, acc
 
 

@@ -1,9 +1,10 @@
 // The further Hamiltonian adapters (XXX, J1J2, XYZNNN, KitaevHex) in the
 // reference's constructor forms, and a RunRBM-style run on the J1J2 chain
 // (Hamiltonians/J1J2.hpp:14-56, N = 12, J1 = 1, J2 = 0.2, sign rule) with
-// exchange moves at zero magnetisation.  Prints "TERMS <name> <n> <requests>"
-// for every model and a final "OK E/N first last" line; exits non-zero if the
-// energy does not go down.
+// exchange moves at zero magnetisation, then a HamiltonianSweeper sampler on the
+// trained machine.  Prints "TERMS <name> <n> <requests>" for every model,
+// "HAMSWEEP <samples>" and a final "OK E/N first last" line; exits non-zero if
+// the energy does not go down.
 #include <cstdio>
 #include <vector>
 
@@ -47,6 +48,11 @@ int main(int argc, char** argv) {
         es.push_back(e);
     };
     runner.run(sampler, callback, ham, 16, 16, 7);
+    // the same chain sampled with the HamiltonianSweeper (offDiagonals proposals)
+    HamiltonianSweeper<J1J2> hsw(int(N), ham);
+    SamplerMT<RBM<std::complex<double>>, HamiltonianSweeper<J1J2>> hsampler(runner.getQs(), 1, 16, hsw, int(N / 2));
+    hsampler.initializeRandomEngine(5);
+    std::printf("HAMSWEEP %zu\n", hsampler.sample(4, 8).size());
     double first = es.front(), last = 0.0;
     for (size_t i = es.size() - 5; i < es.size(); ++i) last += es[i] / 5.0;
     std::printf("OK %.8f %.8f\n", first / N, last / N);

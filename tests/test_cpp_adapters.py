@@ -48,6 +48,7 @@ def test_j1j2_driver_runs(tmp_path, orc):
              if l.startswith("TERMS")}
     assert terms == {"XXX": (10, 10), "XYZNNN": (10, 20), "KitaevHex": (16, 32), "KitaevHexAniso": (16, 32),
                      "J1J2": (12, 24)}
+    assert "HAMSWEEP 64" in out.stdout
     last = [l for l in out.stdout.splitlines() if l.startswith("OK")][0].split()
     e_first, e_last = float(last[1]), float(last[2])
     e0 = orc.ed_ground(orc.Ham.j1j2(12, 1.0, 0.2, True), 1, 6) / 12

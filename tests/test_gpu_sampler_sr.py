@@ -89,7 +89,7 @@ def test_sampler_c64_distribution(ctx, orc, move):
     counts = np.bincount([orc.index_of(x) for x in s], minlength=1 << n)
     N = len(s)
     sel = pr * N > 20
-    chi2 = (((counts - N * pr) ** 2) / (N * pr))[sel].sum()
+    chi2 = (((counts[sel] - N * pr[sel]) ** 2) / (N * pr[sel])).sum()
     dof = sel.sum() - 1
     assert chi2 < 4 * dof + 30, (chi2, dof)
 
@@ -287,3 +287,135 @@ def test_tempering_complex64_distribution(ctx, orc):
     assert pval > 1e-4, (chi2, pval)
     S.close()
     q.close()
+
+
+def _dev_ham(api, ctx, h):
+    """The device Hamiltonian of an oracle descriptor."""
+    if h.kind == 0:
+        return api.Hamiltonian.tfi(ctx, h.n, h.J, h.h)
+    if h.kind == 1:
+        return api.Hamiltonian.xxz(ctx, h.n, h.J, h.h, h.sign < 0)
+    if h.kind == 2:
+        return api.Hamiltonian.tfi2d(ctx, h.lx, h.ly, h.J, h.h)
+    if h.kind == 3:
+        return api.Hamiltonian.xxx(ctx, h.n)
+    if h.kind == 4:
+        return api.Hamiltonian.j1j2(ctx, h.n, h.J, h.h, h.sign < 0)
+    if h.kind == 5:
+        return api.Hamiltonian.xyznnn(ctx, h.n, h.J, h.h)
+    return api.Hamiltonian.kitaev_hex(ctx, h.lx, h.ly, h.J, h.jy, h.jz, h.h)
+
+
+HAM_SWEEPER = [
+    ("tfi10", lambda o: o.Ham.tfi(10, -1.0, -1.0), -1),
+    ("tfi2d_3x4", lambda o: o.Ham.tfi2d(3, 4, -1.0, -3.0), -1),
+    ("xxz10_sign", lambda o: o.Ham.xxz(10, 1.0, 1.0, True), 5),
+    ("xxx10", lambda o: o.Ham.xxx(10), 5),
+    ("j1j2_10_sign", lambda o: o.Ham.j1j2(10, 1.0, 0.5, True), 5),
+    ("xyznnn10", lambda o: o.Ham.xyznnn(10, 0.3, 0.7), -1),
+    ("kitaev4x2_field", lambda o: o.Ham.kitaev_hex(4, 2, 0.5, 0.7, 0.9, 0.3), -1),
+    ("kitaev4x4_nofield", lambda o: o.Ham.kitaev_hex(4, 4, 0.2, 0.4, 0.6), -1),
+]
+
+
+@pytest.mark.parametrize("name,mk,nup", HAM_SWEEPER, ids=[c[0] for c in HAM_SWEEPER])
+def test_hamiltonian_sweeper_fp64_draw_for_draw(ctx, orc, name, mk, nup):
+    """Samplers/HamiltonianSweeper.hpp:22-50 on the device (warp ballots over the
+    offDiagonals list) against the oracle's restatement, same Philox streams."""
+    from yannq_b200 import api
+
+    h = mk(orc)
+    n = h.n
+    m = 2 * n
+    q, p = _mk(api, ctx, orc, n, m, 27, 0.3, api.C128)
+    H = _dev_ham(api, ctx, h)
+    S = api.Sampler(q, 32, api.MOVE_HAMILTONIAN, nup)
+    S.set_hamiltonian(H)
+    S.sample(6, 4, seed=7, epoch=2, reinit=True)
+    s, th = S.get_samples()
+    os_, oth, ocs, oacc = orc.sample(n, m, p, 32, move=orc.MOVE_HAMILTONIAN, nup=nup, seed=7, epoch=2, reinit=True,
+                                     n_sweeps=6, n_discard=4, ham=h)
+    np.testing.assert_array_equal(s, os_)
+    assert np.max(np.abs(th - oth)) <= 1e-13 * max(1.0, np.max(np.abs(oth)))
+    np.testing.assert_array_equal(S.get_accepts(), oacc)
+    assert oacc.sum() > 0
+    S.sample(3, 0, seed=7, epoch=3, reinit=False)
+    s2, _ = S.get_samples()
+    os2, _, _, _ = orc.sample(n, m, p, 32, move=orc.MOVE_HAMILTONIAN, nup=nup, seed=7, epoch=3, reinit=False,
+                              n_sweeps=3, n_discard=0, chain_sigma=ocs, ham=h)
+    np.testing.assert_array_equal(s2, os2)
+    S.close()
+    H.close()
+    q.close()
+
+
+def test_hamiltonian_sweeper_tempering_draw_for_draw(ctx, orc):
+    from yannq_b200 import api
+
+    h = orc.Ham.j1j2(10, 1.0, 0.5, True)
+    n, m, nt = 10, 20, 4
+    q, p = _mk(api, ctx, orc, n, m, 28, 0.3, api.C128)
+    H = _dev_ham(api, ctx, h)
+    S = api.Sampler(q, 16 * nt, api.MOVE_HAMILTONIAN, 5)
+    S.set_hamiltonian(H)
+    S.set_tempering(nt)
+    S.sample(5, 3, seed=8, epoch=1, reinit=True)
+    s, _ = S.get_samples()
+    os_, _, _, osl, _ = orc.sample_pt(n, m, p, 16 * nt, nt, move=orc.MOVE_HAMILTONIAN, nup=5, seed=8, epoch=1,
+                                      n_sweeps=5, n_discard=3, ham=h)
+    np.testing.assert_array_equal(s, os_)
+    np.testing.assert_array_equal(S.get_slots(), osl)
+    S.close()
+    H.close()
+    q.close()
+
+
+@pytest.mark.parametrize("name,mk,nup,allowed", [
+    ("j1j2_6_sign", lambda o: o.Ham.j1j2(6, 1.0, 0.5, True), 3, lambda b: bin(b).count("1") == 3),
+    ("kitaev4x2_field", lambda o: o.Ham.kitaev_hex(4, 2, 0.5, 0.7, 0.9, 0.3), -1, lambda b: True),
+], ids=["j1j2_6_sign", "kitaev4x2_field"])
+def test_hamiltonian_sweeper_c64_distribution(ctx, orc, name, mk, nup, allowed):
+    from yannq_b200 import api
+
+    h = mk(orc)
+    n = m = h.n
+    q, p = _mk(api, ctx, orc, n, m, 41, 0.3, api.C64)
+    H = _dev_ham(api, ctx, h)
+    S = api.Sampler(q, 512, api.MOVE_HAMILTONIAN, nup)
+    S.set_hamiltonian(H)
+    S.sample(40, 100, seed=19, epoch=0, reinit=True)
+    s, _ = S.get_samples(theta=False)
+    basis = orc.basis(n)
+    pr = np.abs(np.array([orc.psi(n, m, p, orc.sigma_of(b, n)) for b in basis])) ** 2
+    mask = np.array([allowed(b) for b in range(1 << n)])
+    pr = np.where(mask, pr, 0)
+    pr /= pr.sum()
+    idx = np.array([orc.index_of(x) for x in s])
+    assert mask[idx].all()
+    counts = np.bincount(idx, minlength=1 << n)
+    N = len(s)
+    sel = pr * N > 20
+    chi2 = (((counts[sel] - N * pr[sel]) ** 2) / (N * pr[sel])).sum()
+    dof = sel.sum() - 1
+    assert chi2 < 4 * dof + 30, (chi2, dof)
+    S.close()
+    H.close()
+    q.close()
+
+
+def test_hamiltonian_sweeper_arguments(ctx, orc):
+    from yannq_b200 import api
+
+    q, _ = _mk(api, ctx, orc, 8, 8, 1, 0.1, api.C128)
+    S = api.Sampler(q, 8, api.MOVE_HAMILTONIAN)
+    with pytest.raises(api.YQError):
+        S.sample(1, 0, seed=1, epoch=0, reinit=True)  # no Hamiltonian attached
+    H10 = api.Hamiltonian.tfi(ctx, 10, -1.0, -1.0)
+    with pytest.raises(api.YQError):
+        S.set_hamiltonian(H10)  # size differs
+    L = api.Sampler(q, 8, api.MOVE_LOCAL)
+    H = api.Hamiltonian.tfi(ctx, 8, -1.0, -1.0)
+    with pytest.raises(api.YQError):
+        L.set_hamiltonian(H)  # not a HamiltonianSweeper sampler
+    for x in (S, L, H10, H, q):
+        x.close()

@@ -88,7 +88,7 @@ def test_sampler_distribution(orc, move):
     counts = np.bincount([_index(x) for x in s], minlength=1 << n)
     N = len(s)
     sel = pr * N > 20
-    chi2 = (((counts - N * pr) ** 2) / (N * pr))[sel].sum()
+    chi2 = (((counts[sel] - N * pr[sel]) ** 2) / (N * pr[sel])).sum()
     dof = sel.sum() - 1
     # samples within a chain are correlated; allow a generous factor over dof
     assert chi2 < 4 * dof + 30, (chi2, dof)
@@ -175,3 +175,57 @@ def test_oracle_tempering_samples_follow_psi2(orc):
     w /= w.sum()
     chi2, pval = stats.chisquare(np.bincount(idx, minlength=1 << n), len(idx) * w)
     assert pval > 1e-4, (chi2, pval)
+
+
+HAM_SWEEPER_CASES = [
+    # (name, Ham factory, n, nup, allowed(index) -> bool)
+    ("tfi6", lambda o: o.Ham.tfi(6, -1.0, -1.0), 6, -1, lambda b: True),
+    ("j1j2_6_sign", lambda o: o.Ham.j1j2(6, 1.0, 0.5, True), 6, 3, lambda b: bin(b).count("1") == 3),
+    ("xyznnn6", lambda o: o.Ham.xyznnn(6, 0.3, 0.7), 6, 3, lambda b: bin(b).count("1") % 2 == 1),
+    ("kitaev4x2_field", lambda o: o.Ham.kitaev_hex(4, 2, 0.5, 0.7, 0.9, 0.3), 8, -1, lambda b: True),
+]
+
+
+@pytest.mark.parametrize("name,mk,n,nup,allowed", HAM_SWEEPER_CASES, ids=[c[0] for c in HAM_SWEEPER_CASES])
+def test_hamiltonian_sweeper_distribution(orc, name, mk, n, nup, allowed):
+    """Samplers/HamiltonianSweeper.hpp:22-50: proposals drawn uniformly from
+    offDiagonals(sigma) with the w1 / w2 correction sample |psi|^2 on the sector
+    the moves connect (pair flips keep the magnetisation where only antiparallel
+    pairs flip, and its parity where parallel pairs flip too)."""
+    m = n
+    ham = mk(orc)
+    p = orc.init_params(n, m, 41, 0.3)
+    s, th, _, acc = orc.sample(n, m, p, 256, move=orc.MOVE_HAMILTONIAN, nup=nup, seed=23, n_sweeps=60,
+                               n_discard=100, ham=ham)
+    assert acc.sum() > 0
+    pr = _exact_probs(orc, n, m, p)
+    mask = np.array([allowed(b) for b in range(1 << n)])
+    pr = np.where(mask, pr, 0)
+    pr /= pr.sum()
+    idx = np.array([_index(x) for x in s])
+    assert mask[idx].all()
+    counts = np.bincount(idx, minlength=1 << n)
+    N = len(s)
+    sel = pr * N > 20
+    chi2 = (((counts[sel] - N * pr[sel]) ** 2) / (N * pr[sel])).sum()
+    dof = sel.sum() - 1
+    assert chi2 < 4 * dof + 30, (chi2, dof)
+    for k in range(0, N, 211):
+        assert np.allclose(th[k], orc.theta(n, m, p, s[k]), atol=1e-12)
+
+
+def test_hamiltonian_sweeper_list_sizes_vary(orc):
+    """The chi^2 case j1j2_6_sign exercises the w1 / w2 correction: its
+    offDiagonals list (antiparallel bonds) changes size with the state, while
+    XYZNNN's (a != b, every coefficient non-zero) and TFIsing's do not."""
+    n = 6
+
+    def sizes(ham):
+        out = set()
+        for b in range(1 << n):
+            d, masks, coeffs = orc.ham_enumerate(ham, orc.sigma_of(b, n))
+            out.add(int(np.count_nonzero(coeffs)))
+        return out
+
+    assert len(sizes(orc.Ham.j1j2(n, 1.0, 0.5, True))) > 1
+    assert sizes(orc.Ham.xyznnn(n, 0.3, 0.7)) == {2 * n}

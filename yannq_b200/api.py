@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(_HERE, "libyannq_b200.so")
 OK, E_ARG, E_CUDA, E_NOMEM, E_NOT_PD, E_NONFINITE, E_TIMEOUT, E_STATE, E_UNSUPPORTED = range(9)
 C64, C128 = 0, 1
 HAM_TFI, HAM_XXZ, HAM_TFI2D, HAM_XXX, HAM_J1J2, HAM_XYZNNN, HAM_KITAEV_HEX = 0, 1, 2, 3, 4, 5, 6
-MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN = 0, 1, 2
+MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN, MOVE_HAMILTONIAN = 0, 1, 2, 3
 SR_AUTO, SR_S, SR_T = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 SOLVE_LLT, SOLVE_CG = 0, 1
@@ -75,6 +75,7 @@ SIGNATURES = {
     "yq_eloc": [_vp, _vp, _i, _vp, _vp, _vp],
     "yq_sampler_create": [_vp, _i, _i, _i, _i, _vp],
     "yq_sampler_destroy": [_vp],
+    "yq_sampler_set_hamiltonian": [_vp, _vp],
     "yq_sampler_set_resync": [_vp, _i],
     "yq_sampler_set_chains": [_vp, _vp],
     "yq_sampler_get_chains": [_vp, _vp],
@@ -361,6 +362,12 @@ class Sampler:
         if self.h:
             check(lib().yq_sampler_destroy(self.h))
             self.h = None
+
+    def set_hamiltonian(self, ham):
+        """HamiltonianSweeper proposals (Samplers/HamiltonianSweeper.hpp) from `ham`,
+        which must stay open while the sampler uses it."""
+        check(lib().yq_sampler_set_hamiltonian(self.h, ham.h))
+        self._ham = ham
 
     def set_resync(self, every):
         check(lib().yq_sampler_set_resync(self.h, every))

@@ -428,6 +428,7 @@ int yq_ham_create(yq_ctx ctx, int kind, int n, int lx, int ly, double J, double 
         H->sign = sign_rule ? -1.0 : 1.0;
         H->conserves_sz = kind == YQ_HAM_XXZ;
         if (kind >= YQ_HAM_XXX) ham_build_terms(H.get(), 0.0, 0.0);
+        ham_build_moves(H.get());
         *out = H.release();
     });
 }
@@ -450,6 +451,7 @@ int yq_ham_create_kitaev_hex(yq_ctx ctx, int ncol, int nrow, double Jx, double J
         H->J = Jx;
         H->h = h;
         ham_build_terms(H.get(), Jy, Jz);
+        ham_build_moves(H.get());
         *out = H.release();
     });
 }
@@ -520,7 +522,8 @@ int yq_sampler_create(yq_rbm q, int n_chains, int move, int nup, int sweep_len, 
         need(out, "out");
         *out = nullptr;
         if (n_chains < 1) throw Error(YQ_E_ARG, "sampler: n_chains must be >= 1");
-        if (move != YQ_MOVE_LOCAL && move != YQ_MOVE_EXCHANGE_ANY && move != YQ_MOVE_EXCHANGE_NN)
+        if (move != YQ_MOVE_LOCAL && move != YQ_MOVE_EXCHANGE_ANY && move != YQ_MOVE_EXCHANGE_NN &&
+            move != YQ_MOVE_HAMILTONIAN)
             throw Error(YQ_E_ARG, "sampler: unknown move");
         if (nup > q->n) throw Error(YQ_E_ARG, "sampler: nup > n");
         if (sweep_len < 0) throw Error(YQ_E_ARG, "sampler: sweep_len < 0");
@@ -546,6 +549,17 @@ int yq_sampler_destroy(yq_sampler S) {
         if (!S) return;
         cudaStreamSynchronize(S->q->ctx->stream);
         delete S;
+    });
+}
+
+int yq_sampler_set_hamiltonian(yq_sampler S, yq_ham H) {
+    return guard([&] {
+        need(S, "sampler");
+        need(H, "ham");
+        if (S->move != YQ_MOVE_HAMILTONIAN) throw Error(YQ_E_ARG, "sampler: not a HamiltonianSweeper sampler");
+        if (H->n != S->q->n) throw Error(YQ_E_ARG, "sampler: Hamiltonian and RBM sizes differ");
+        if (H->ctx->device != S->q->ctx->device) throw Error(YQ_E_ARG, "sampler: Hamiltonian on another device");
+        S->ham = H;
     });
 }
 

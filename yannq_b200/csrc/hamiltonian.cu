@@ -220,6 +220,35 @@ void ham_build_terms(yq_ham_s* H, double jy, double jz) {
     YQ_CUDA(cudaMemcpy(H->terms.p, T.data(), T.size() * sizeof(HamTerm), cudaMemcpyHostToDevice));
 }
 
+// offDiagonals (Hamiltonians/TFIsing.hpp:41-50: every site, whatever the state;
+// the 2D model likewise).  Other kinds: the off-diagonal requests in order,
+// present where their coefficient for the state's zz is non-zero.
+void ham_build_moves(yq_ham_s* H) {
+    std::vector<HamMove> M;
+    const int n = H->n;
+    auto bits = [](double cp, double cm) { return (cp != 0.0 ? 1 : 0) | (cm != 0.0 ? 2 : 0); };
+    if (H->kind == YQ_HAM_TFI || H->kind == YQ_HAM_TFI2D) {
+        for (int i = 0; i < n; ++i) M.push_back(HamMove{i, -1, 3, 0});
+    } else if (H->kind == YQ_HAM_XXZ) {
+        // XXZ.hpp:40-47: sign J (1 - zz) ratio(i, i+1)
+        for (int i = 0; i < n; ++i)
+            M.push_back(HamMove{i, (i + 1) % n, bits(H->sign * H->J * (1 - 1), H->sign * H->J * (1 - (-1))), 0});
+    } else {
+        std::vector<HamTerm> T(size_t(H->nterms));
+        YQ_CUDA(cudaMemcpy(T.data(), H->terms.p, T.size() * sizeof(HamTerm), cudaMemcpyDeviceToHost));
+        for (const HamTerm& t : T) {
+            if (t.nflip == 0) continue;
+            if (t.nflip == 1)
+                M.push_back(HamMove{t.a, -1, t.cp != 0.0 ? 3 : 0, 0});
+            else
+                M.push_back(HamMove{t.a, t.b, bits(t.cp, t.cm), 0});
+        }
+    }
+    H->n_moves = int(M.size());
+    H->moves.ensure(M.size() * sizeof(HamMove));
+    YQ_CUDA(cudaMemcpy(H->moves.p, M.data(), M.size() * sizeof(HamMove), cudaMemcpyHostToDevice));
+}
+
 // ---------------------------------------------------------------------------
 template <typename R>
 struct ElocArgs {

@@ -58,6 +58,13 @@ struct HamTerm {
     double dp, dm, cp, cm;
 };
 
+// One entry of a Hamiltonian's offDiagonals list (the HamiltonianSweeper's
+// proposals): flip a (and b >= 0); present in state s when bit 0 (zz = s_a s_b
+// = +1, or a single flip) or bit 1 (zz = -1) of `on` is set.
+struct HamMove {
+    int a, b, on, pad;
+};
+
 struct yq_ham_s {
     yq_ctx_s* ctx = nullptr;
     int kind = 0, n = 0, lx = 0, ly = 0;
@@ -66,6 +73,8 @@ struct yq_ham_s {
     int nterms = 0, n_off = 0;  // n_off: off-diagonal requests per sample
     bool conserves_sz = false;  // every request keeps the number of down spins
     yq::DevBuf terms;           // nterms HamTerm
+    int n_moves = 0;
+    yq::DevBuf moves;           // n_moves HamMove (every kind)
 };
 
 struct yq_sampler_s {
@@ -80,6 +89,7 @@ struct yq_sampler_s {
     uint64_t proposals = 0;  // per chain, last call
     const uint32_t* epoch_dev = nullptr;  // device epoch offset added to the call's epoch (batched graphs)
     int chains_per_cta = 0;               // autotuned launch shape of the last sample call
+    const yq_ham_s* ham = nullptr;        // proposals of YQ_MOVE_HAMILTONIAN
     // parallel tempering (SamplerMT nTmps > 1): chains c = ntemps group + k
     int ntemps = 1;
     bool pt_ready = false;
@@ -167,6 +177,7 @@ void rbm_init_params_host(int n, int m, bool bias, uint64_t seed, double sd, c12
 void sampler_run(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, uint32_t epoch, int reinit);
 
 void ham_build_terms(yq_ham_s* H, double jy, double jz);  // term-table kinds
+void ham_build_moves(yq_ham_s* H);                        // offDiagonals list, every kind
 int ham_num_offdiag(const yq_ham_s* H);
 void ham_enumerate(yq_ham_s* H, int ns, const int8_t* d_sigma, int* d_a, int* d_b, double* d_c, double* d_diag);
 void ham_eloc(yq_ham_s* H, yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_theta, c128* d_out);

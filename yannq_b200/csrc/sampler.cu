@@ -1,8 +1,10 @@
 // Persistent Metropolis sampler: one warp per chain.
 //
 // Restates Samplers/SamplerMT.hpp (nTmps = 1) driving LocalSweeper
-// (Samplers/LocalSweeper.hpp:32-53) or SwapSweeper (Samplers/SwapSweeper.hpp:28-57,
-// plus a neighbour-pair variant).  Per chain the warp holds
+// (Samplers/LocalSweeper.hpp:32-53), SwapSweeper (Samplers/SwapSweeper.hpp:28-57,
+// plus a neighbour-pair variant) or HamiltonianSweeper
+// (Samplers/HamiltonianSweeper.hpp:22-50: proposals from the Hamiltonian's
+// offDiagonals list, counted and selected with warp ballots).  Per chain the warp holds
 //   sigma           int8 in shared memory (one row per warp),
 //   theta_j, t_j    = theta and tanh(theta) for j = lane + 32 r in registers,
 // and evaluates the reference's acceptance min(1, exp(2 beta Re logRatio)) with
@@ -49,7 +51,45 @@ struct SampArgs {
     int8_t* out_sigma;
     cplx<R>* out_theta;
     unsigned long long* acc;
+    const HamMove* moves;  // HamiltonianSweeper proposals
+    int n_moves;
 };
+
+// Is offDiagonals entry e present in s, with sites fa, fb (fb may be -1) flipped?
+__device__ __forceinline__ bool move_present(const HamMove& e, const int8_t* s, int fa, int fb) {
+    if (e.b < 0) return (e.on & 1) != 0;
+    int zz = s[e.a] * s[e.b];
+    const int flips = (e.a == fa || e.a == fb) + (e.b == fa || e.b == fb);
+    if (flips == 1) zz = -zz;
+    return ((e.on >> (zz > 0 ? 0 : 1)) & 1) != 0;
+}
+
+// Size of offDiagonals(s with fa, fb flipped), the same in every lane.
+__device__ __forceinline__ int count_moves(const HamMove* __restrict__ mv, int K, const int8_t* s, int fa, int fb,
+                                           int lane) {
+    int cnt = 0;
+    for (int e = lane; e < K; e += 32) cnt += move_present(mv[e], s, fa, fb) ? 1 : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    return cnt;
+}
+
+// Index of the r-th present entry of offDiagonals(s) (0 <= r < count), in list order.
+__device__ __forceinline__ int select_move(const HamMove* __restrict__ mv, int K, const int8_t* s, int r, int lane) {
+    for (int base = 0; base < K; base += 32) {
+        const int e = base + lane;
+        const bool on = e < K && move_present(mv[e], s, -1, -1);
+        const unsigned bal = __ballot_sync(0xffffffffu, on);
+        const int cnt = __popc(bal);
+        if (r < cnt) {
+            const bool mine = on && __popc(bal & ((1u << lane) - 1u)) == r;
+            const unsigned who = __ballot_sync(0xffffffffu, mine);
+            return base + (__ffs(who) - 1);
+        }
+        r -= cnt;
+    }
+    return -1;
+}
 
 __device__ __forceinline__ void prefetch_l1(const void* p) {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
@@ -158,6 +198,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     // into L1.
     // (register pipelining for complex64 only: complex128 would spill)
     constexpr bool REGPIPE = MOVE == YQ_MOVE_LOCAL && sizeof(R) == 4;
+    constexpr bool HAMMOVE = MOVE == YQ_MOVE_HAMILTONIAN;  // proposals depend on the state: nothing ahead
     U4 xcur = draw(A.seed, uint32_t(A.sw0) * L, epoch, uint32_t(c), TAG_SWEEP);
     cplx<R> tvn[JPL], wvn[JPL];
     double lkn = 0., abn = 0.;
@@ -173,7 +214,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     };
     if (REGPIPE) {
         load_cols(int(draw_site(xcur.x, uint32_t(n))));
-    } else {
+    } else if (!HAMMOVE) {
         const int k0 = int(draw_site(xcur.x, uint32_t(n)));
 #pragma unroll
         for (int r = 0; r < JPL; ++r) {
@@ -191,7 +232,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
             const U4 x = xcur;
             const U4 xn = draw(A.seed, g + 1u, epoch, uint32_t(c), TAG_SWEEP);
             xcur = xn;
-            if (!REGPIPE) {
+            if (!REGPIPE && !HAMMOVE) {
                 // prefetch the next proposal's columns into L1
                 int kn = int(draw_site(xn.x, uint32_t(n)));
                 int ln = (MOVE == YQ_MOVE_EXCHANGE_ANY) ? int(draw_site(xn.y, uint32_t(n))) : (kn + 1) % n;
@@ -209,8 +250,24 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 }
             }
             const R u = draw_uniform<R>(x);
-            const int k = int(draw_site(x.x, uint32_t(n)));
-            if (MOVE == YQ_MOVE_LOCAL) {
+            int k, l = -1;
+            R wfac = R(1);  // HamiltonianSweeper.hpp:39-42: w1 / w2
+            if (HAMMOVE) {
+                const int w1 = count_moves(A.moves, A.n_moves, s, -1, -1, lane);
+                if (w1 == 0) continue;  // empty list: the slot is consumed
+                const int e = select_move(A.moves, A.n_moves, s, int(draw_site(x.x, uint32_t(w1))), lane);
+                if (e < 0) continue;  // not reached: r < w1 entries are present
+                k = A.moves[e].a;
+                l = A.moves[e].b;
+                const int w2 = count_moves(A.moves, A.n_moves, s, k, l, lane);
+                wfac = R(w1) / R(w2);
+            } else {
+                k = int(draw_site(x.x, uint32_t(n)));
+                if (MOVE != YQ_MOVE_LOCAL) l = (MOVE == YQ_MOVE_EXCHANGE_ANY) ? int(draw_site(x.y, uint32_t(n))) : (k + 1) % n;
+            }
+            // HamiltonianSweeper.hpp:42 has no beta
+            const R bexp = HAMMOVE ? R(1) : beta;
+            if (MOVE == YQ_MOVE_LOCAL || (HAMMOVE && l < 0)) {
                 const R sk = R(s[k]);
                 const cplx<R>* wk = A.W + size_t(k) * m;
                 cplx<R> tv[JPL], wv[JPL], d[JPL];
@@ -259,7 +316,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 const double base = lk - 2.0 * double(sk) * ab;
                 const R logr = R(0.5) * ls + R(base);
                 // LocalSweeper.hpp:45-47: p = min(1, exp(beta * 2 * Re logRatio)); accept if u < p
-                if (u < exp(two * beta * logr)) {
+                if (u < exp(two * bexp * logr) * wfac) {
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
                         int j = lane + 32 * r;
@@ -275,9 +332,8 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                     ++nacc;
                 }
             } else {
-                const int l = (MOVE == YQ_MOVE_EXCHANGE_ANY) ? int(draw_site(x.y, uint32_t(n))) : (k + 1) % n;
                 const int8_t sk8 = s[k], sl8 = s[l];
-                if (sk8 == sl8) continue;  // SwapSweeper.hpp:43-46: the slot is consumed
+                if (!HAMMOVE && sk8 == sl8) continue;  // SwapSweeper.hpp:43-46: the slot is consumed
                 const R sk = R(sk8), sl = R(sl8);
                 const cplx<R>* tk = A.tau + size_t(k) * m;
                 const cplx<R>* tl = A.tau + size_t(l) * m;
@@ -316,7 +372,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                     base -= 2.0 * double(sk) * A.p64[size_t(n) * m + k].re +
                             2.0 * double(sl) * A.p64[size_t(n) * m + l].re;
                 const R logr = R(0.5) * ls + R(base);
-                if (u < exp(two * beta * logr)) {
+                if (u < exp(two * bexp * logr) * wfac) {
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
                         int j = lane + 32 * r;
@@ -543,6 +599,7 @@ static void launch_sweeps(yq_sampler_s* S, const SampArgs<R>& A, cudaStream_t st
     switch (S->move) {
         case YQ_MOVE_LOCAL: dispatch_jpl<R, YQ_MOVE_LOCAL>(A, st, &S->chains_per_cta); break;
         case YQ_MOVE_EXCHANGE_ANY: dispatch_jpl<R, YQ_MOVE_EXCHANGE_ANY>(A, st, &S->chains_per_cta); break;
+        case YQ_MOVE_HAMILTONIAN: dispatch_jpl<R, YQ_MOVE_HAMILTONIAN>(A, st, &S->chains_per_cta); break;
         default: dispatch_jpl<R, YQ_MOVE_EXCHANGE_NN>(A, st, &S->chains_per_cta); break;
     }
 }
@@ -583,6 +640,8 @@ static void run_t(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, u
     A.out_sigma = S->sigma.as<int8_t>();
     A.out_theta = S->theta.as<cplx<R>>();
     A.acc = S->acc.as<unsigned long long>();
+    A.moves = S->ham ? S->ham->moves.as<HamMove>() : nullptr;
+    A.n_moves = S->ham ? S->ham->n_moves : 0;
     cudaStream_t st = q->ctx->stream;
     if (S->ntemps <= 1) {
         launch_sweeps<R>(S, A, st);
@@ -625,6 +684,8 @@ void sampler_run(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, ui
     yq_rbm_s* q = S->q;
     YQ_CHECK_ARG(n_sweeps > 0 && n_discard >= 0, "sample: n_sweeps must be > 0 and n_discard >= 0");
     YQ_CHECK_ARG(reinit || S->have_chains, "sample: reinit = 0 needs chains (set_chains or an earlier sample)");
+    if (S->move == YQ_MOVE_HAMILTONIAN && !S->ham)
+        throw Error(YQ_E_STATE, "sample: a HamiltonianSweeper sampler needs yq_sampler_set_hamiltonian");
     const long long L = S->sweep_len > 0 ? S->sweep_len : q->n;
     YQ_CHECK_ARG((long long)(n_sweeps + n_discard) * L < (1LL << 32) - 1, "sample: too many proposals per call");
     rbm_prepare(q);
