@@ -37,6 +37,7 @@ enum {
 };
 
 enum { YQ_C64 = 0, YQ_C128 = 1 };                             /* RBM<complex<float|double>> */
+enum { YQ_ARCHIVE_C64 = 0, YQ_ARCHIVE_C128 = 1, YQ_ARCHIVE_F64 = 2, YQ_ARCHIVE_F32 = 3 }; /* archive element T */
 enum { YQ_HAM_TFI = 0, YQ_HAM_XXZ = 1, YQ_HAM_TFI2D = 2,       /* Hamiltonian kinds          */
        YQ_HAM_XXX = 3, YQ_HAM_J1J2 = 4, YQ_HAM_XYZNNN = 5, YQ_HAM_KITAEV_HEX = 6 };
 enum { YQ_MOVE_LOCAL = 0, YQ_MOVE_EXCHANGE_ANY = 1, YQ_MOVE_EXCHANGE_NN = 2, YQ_MOVE_HAMILTONIAN = 3 };
@@ -94,6 +95,26 @@ int yq_rbm_update_params(yq_rbm q, const double* delta);
  * columns, each entry (re, im) ~ N(0, sd^2); the normal draws are Philox4x32-10
  * keyed by seed (Box-Muller), identical to the oracle's. */
 int yq_rbm_init_random(yq_rbm q, uint64_t seed, double sd);
+/* Checkpoints in the reference's format: the cereal binary archive of
+ * std::unique_ptr<RBM<T>> that RunRBM writes to w%04d.dat (Runners/RunRBM.hpp:
+ * 155-164) and AbstractRunner::initializeFrom reads (Runners/AbstractRunner.hpp:
+ * 83-94); layout from Serializers/SerializeRBM.hpp:20-82 and SerializeEigen.hpp:
+ * 8-35 (u8 valid, u32 class version 1, u8 useBias, u32 N, u32 M, W as i32 rows,
+ * i32 cols and M x N column-major values, then a and b likewise when useBias).
+ * elem names T (the file does not record it): YQ_ARCHIVE_C128 std::complex<double>,
+ * YQ_ARCHIVE_C64 std::complex<float>, YQ_ARCHIVE_F64 double, YQ_ARCHIVE_F32 float
+ * (a real archive needs parameters with zero imaginary parts).  Saving converts
+ * the FP64 master parameters to T; loading needs a machine of the archive's N, M
+ * and useBias (the reference replaces the whole machine) and converts T to the
+ * masters.  Buffers are host memory. */
+int yq_rbm_archive_size(yq_rbm q, int elem, size_t* size);
+int yq_rbm_save_archive(yq_rbm q, int elem, void* buf, size_t cap, size_t* size);
+int yq_rbm_load_archive(yq_rbm q, int elem, const void* buf, size_t size);
+/* N, M and useBias of an archive (any element type). */
+int yq_rbm_archive_shape(const void* buf, size_t size, int* n, int* m, int* use_bias);
+int yq_rbm_save(yq_rbm q, int elem, const char* path);
+int yq_rbm_load(yq_rbm q, int elem, const char* path);
+int yq_rbm_file_shape(const char* path, int* n, int* m, int* use_bias);
 /* calcTheta over a batch -- Machines/RBM.hpp:137-141.  sigma: ns x n int8 (+-1). */
 int yq_rbm_theta(yq_rbm q, int ns, const int8_t* sigma, double* theta);
 /* logCoeff over a batch -- Machines/RBM.hpp:367-378 (ns complex). */

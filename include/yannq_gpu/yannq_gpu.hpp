@@ -21,6 +21,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdint>
+#include <cstdio>
 #include <functional>
 #include <stdexcept>
 #include <string>
@@ -115,6 +116,11 @@ public:
     }
     // RBM.hpp:325-349 (Philox-seeded normal draws in the reference's order)
     void initializeRandom(uint64_t seed, double sigma = 1e-3) { check(yq_rbm_init_random(h_, seed, sigma)); }
+
+    // cereal image of std::unique_ptr<RBM<T>> (Serializers/SerializeRBM.hpp), as RunRBM writes it
+    static constexpr int archiveElem = std::is_same<T, std::complex<double>>::value ? YQ_ARCHIVE_C128 : YQ_ARCHIVE_C64;
+    void save(const std::string& path) const { check(yq_rbm_save(h_, archiveElem, path.c_str())); }
+    void load(const std::string& path) { check(yq_rbm_load(h_, archiveElem, path.c_str())); }
 
     // logCoeff over configurations (ns x n, entries +-1), RBM.hpp:367-378
     std::vector<cd> logCoeff(const std::vector<int8_t>& sigma) const {
@@ -364,7 +370,7 @@ class RunRBM {
     Context& ctx_;
     RBM<T> qs_;
     double lambdaIni_ = 1e-3, lambdaDecay_ = 1.0, lambdaMin_ = 1e-4;
-    int maxIter_ = 2000;
+    int maxIter_ = 2000, saveWfPer_ = 0;
     bool useCG_ = false;
     double cgTol_ = 1e-4;
     double gradClip_ = 0.0;
@@ -383,7 +389,18 @@ public:
         lambdaDecay_ = decay;
         lambdaMin_ = mn;
     }
-    void setIterParams(int maxIter, int /*saveWfPer*/) { maxIter_ = maxIter; }
+    // AbstractRunner.hpp:83-94: start from a checkpoint written by RunRBM (the
+    // file's N, M and useBias must match this runner's machine)
+    void initializeFrom(const std::string& path) {
+        qs_.load(path);
+        initialized_ = true;
+    }
+    // saveWfPer != 0: the parameters are saved to w%04d.dat (working directory)
+    // before every epoch ll with ll % saveWfPer == 0 (RunRBM.hpp:155-164)
+    void setIterParams(int maxIter, int saveWfPer) {
+        maxIter_ = maxIter;
+        saveWfPer_ = saveWfPer;
+    }
     void setOptimizer(const SGD& opt) { opt_ = opt; }
     void setSolverParams(bool useCG, double cgTol = 1e-4) {
         useCG_ = useCG;
@@ -400,6 +417,11 @@ public:
         SRMat<RBM<T>, Ham> srm(qs_, ham, sampler);
         sampler.initializeRandomEngine(seed);
         for (int ll = 0; ll <= maxIter_; ++ll) {
+            if (saveWfPer_ != 0 && ll % saveWfPer_ == 0) {
+                char fileName[30];
+                std::snprintf(fileName, sizeof(fileName), "w%04d.dat", ll);
+                qs_.save(fileName);
+            }
             const double lambda = std::max(lambdaIni_ * std::pow(lambdaDecay_, ll), lambdaMin_);
             const double eta = opt_.eta();
             if (gradClip_ == 0.0) {

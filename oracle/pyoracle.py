@@ -358,3 +358,65 @@ def ff_batch(L, conv_out, conv_k, fc_out, params, sigma, want_der=True, nthreads
     der = np.zeros((B, ff_dim(L, conv_out, conv_k, fc_out))) if want_der else None
     lib().orc_ff_batch(L, conv_out, conv_k, fc_out, _p(p), B, _p(sigma), _p(lp), _p(der), nthreads or os.cpu_count())
     return lp, der
+
+
+# ---------------------------------------------------------------------------
+# RBM checkpoints: the cereal BinaryOutputArchive image of std::unique_ptr<RBM<T>>
+# (Runners/RunRBM.hpp:155-164, Runners/AbstractRunner.hpp:83-94).  cereal is not
+# vendored; the layout is restated from its published binary-archive rules
+# (little-endian raw values, no names, no header; a unique_ptr is one "valid" byte
+# and the pointee; a versioned class writes its u32 version before its first
+# instance) applied to Serializers/SerializeRBM.hpp:20-82 (useBias, N, M, W, then
+# a and b if useBias) and Serializers/SerializeEigen.hpp:8-35 (i32 rows, i32 cols,
+# raw column-major data).
+ARCHIVE_ELEM = {0: ("<f4", True), 1: ("<f8", True), 2: ("<f8", False), 3: ("<f4", False)}
+
+
+def rbm_archive(n, m, params, use_bias=True, elem=1, version=1):
+    """bytes of the archive; params in the reference layout [W (m x n col-major) | a | b]."""
+    import struct
+
+    fmt, cplx = ARCHIVE_ELEM[elem]
+    p = np.asarray(params, np.complex128)
+
+    def values(x):
+        x = np.asarray(x, np.complex128)
+        if cplx:
+            return np.stack([x.real, x.imag], axis=-1).astype(fmt).tobytes()
+        assert np.all(x.imag == 0)
+        return x.real.astype(fmt).tobytes()
+
+    nm = n * m
+    out = struct.pack("<BIBII", 1, version, int(bool(use_bias)), n, m)
+    out += struct.pack("<ii", m, n) + values(p[:nm])
+    if use_bias:
+        out += struct.pack("<ii", n, 1) + values(p[nm:nm + n])
+        out += struct.pack("<ii", m, 1) + values(p[nm + n:nm + n + m])
+    return out
+
+
+def rbm_unarchive(data, elem=1):
+    """(n, m, use_bias, params) from an archive."""
+    import struct
+
+    fmt, cplx = ARCHIVE_ELEM[elem]
+    valid, _version, bias, n, m = struct.unpack_from("<BIBII", data, 0)
+    assert valid == 1
+    at = struct.calcsize("<BIBII")
+    es = np.dtype(fmt).itemsize * (2 if cplx else 1)
+
+    def block(rows, cols):
+        nonlocal at
+        r, c = struct.unpack_from("<ii", data, at)
+        assert (r, c) == (rows, cols)
+        at += 8
+        raw = np.frombuffer(data, dtype=fmt, count=rows * cols * (2 if cplx else 1), offset=at)
+        at += rows * cols * es
+        raw = raw.astype(np.float64)
+        return raw[0::2] + 1j * raw[1::2] if cplx else raw + 0j
+
+    parts = [block(m, n)]
+    if bias:
+        parts += [block(n, 1), block(m, 1)]
+    assert at == len(data)
+    return n, m, bool(bias), np.concatenate(parts)

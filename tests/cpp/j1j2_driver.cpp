@@ -2,9 +2,10 @@
 // reference's constructor forms, and a RunRBM-style run on the J1J2 chain
 // (Hamiltonians/J1J2.hpp:14-56, N = 12, J1 = 1, J2 = 0.2, sign rule) with
 // exchange moves at zero magnetisation, then a HamiltonianSweeper sampler on the
-// trained machine.  Prints "TERMS <name> <n> <requests>" for every model,
-// "HAMSWEEP <samples>" and a final "OK E/N first last" line; exits non-zero if
-// the energy does not go down.
+// trained machine; checkpoints every 20 epochs (w%04d.dat in the working
+// directory) and a resumed runner.  Prints "TERMS <name> <n> <requests>" for
+// every model, "HAMSWEEP <samples>", "RESUME <dim>" and a final "OK E/N first
+// last" line; exits non-zero if the energy does not go down.
 #include <cstdio>
 #include <vector>
 
@@ -38,7 +39,7 @@ int main(int argc, char** argv) {
     RunRBM<std::complex<double>> runner(ctx, N, alpha, true);
     runner.initializeRandom(20261204, 0.01);
     runner.setLambda(1e-3, 1.0, 1e-3);
-    runner.setIterParams(epochs, 0);
+    runner.setIterParams(epochs, 20);  // w0000.dat, w0020.dat, ... in the working directory
     runner.setOptimizer(SGD{0.05, 0.0});
     SwapSweeper sweeper{N};
     SamplerMT<RBM<std::complex<double>>, SwapSweeper> sampler(runner.getQs(), 1, 64, sweeper, int(N / 2));
@@ -53,6 +54,10 @@ int main(int argc, char** argv) {
     SamplerMT<RBM<std::complex<double>>, HamiltonianSweeper<J1J2>> hsampler(runner.getQs(), 1, 16, hsw, int(N / 2));
     hsampler.initializeRandomEngine(5);
     std::printf("HAMSWEEP %zu\n", hsampler.sample(4, 8).size());
+    // resume from a checkpoint (AbstractRunner::initializeFrom)
+    RunRBM<std::complex<double>> resumed(ctx, N, alpha, true);
+    resumed.initializeFrom("w0020.dat");
+    std::printf("RESUME %u\n", resumed.getQs().getDim());
     double first = es.front(), last = 0.0;
     for (size_t i = es.size() - 5; i < es.size(); ++i) last += es[i] / 5.0;
     std::printf("OK %.8f %.8f\n", first / N, last / N);

@@ -6,6 +6,7 @@ constructs the XXX, XYZNNN and KitaevHex adapters)."""
 import os
 import subprocess
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -42,8 +43,15 @@ def test_adapter_driver_runs(tmp_path, orc):
 @pytest.mark.gpu
 def test_j1j2_driver_runs(tmp_path, orc):
     exe = _build(tmp_path, "j1j2_driver")
-    out = subprocess.run([exe, "40"], capture_output=True, text=True, timeout=600)
+    run_dir = tmp_path / "run"
+    run_dir.mkdir()
+    out = subprocess.run([exe, "40"], capture_output=True, text=True, timeout=600, cwd=run_dir)
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    # RunRBM.hpp:155-164 checkpoints at ll % saveWfPer == 0
+    assert sorted(p.name for p in run_dir.iterdir()) == ["w0000.dat", "w0020.dat", "w0040.dat"]
+    n, m, bias, p = orc.rbm_unarchive((run_dir / "w0020.dat").read_bytes(), 1)
+    assert (n, m, bias) == (12, 12, True) and np.all(np.isfinite(p))
+    assert "RESUME 168" in out.stdout
     terms = {l.split()[1]: (int(l.split()[2]), int(l.split()[3])) for l in out.stdout.splitlines()
              if l.startswith("TERMS")}
     assert terms == {"XXX": (10, 10), "XYZNNN": (10, 20), "KitaevHex": (16, 32), "KitaevHexAniso": (16, 32),

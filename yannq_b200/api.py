@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libyannq_b200.so")
 
 OK, E_ARG, E_CUDA, E_NOMEM, E_NOT_PD, E_NONFINITE, E_TIMEOUT, E_STATE, E_UNSUPPORTED = range(9)
 C64, C128 = 0, 1
+ARCHIVE_C64, ARCHIVE_C128, ARCHIVE_F64, ARCHIVE_F32 = 0, 1, 2, 3
 HAM_TFI, HAM_XXZ, HAM_TFI2D, HAM_XXX, HAM_J1J2, HAM_XYZNNN, HAM_KITAEV_HEX = 0, 1, 2, 3, 4, 5, 6
 MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN, MOVE_HAMILTONIAN = 0, 1, 2, 3
 SR_AUTO, SR_S, SR_T = 0, 1, 2
@@ -58,6 +59,13 @@ SIGNATURES = {
     "yq_rbm_create": [_vp, _i, _i, _i, _i, _vp],
     "yq_rbm_destroy": [_vp],
     "yq_rbm_dim": [_vp, _vp],
+    "yq_rbm_archive_size": [_vp, _i, _vp],
+    "yq_rbm_save_archive": [_vp, _i, _vp, C.c_size_t, _vp],
+    "yq_rbm_load_archive": [_vp, _i, _vp, C.c_size_t],
+    "yq_rbm_archive_shape": [_vp, C.c_size_t, _vp, _vp, _vp],
+    "yq_rbm_save": [_vp, _i, C.c_char_p],
+    "yq_rbm_load": [_vp, _i, C.c_char_p],
+    "yq_rbm_file_shape": [C.c_char_p, _vp, _vp, _vp],
     "yq_rbm_set_params": [_vp, _vp],
     "yq_rbm_get_params": [_vp, _vp],
     "yq_rbm_update_params": [_vp, _vp],
@@ -248,6 +256,28 @@ class RBM:
     def update_params(self, d):
         check(lib().yq_rbm_update_params(self.h, _p(_c128(d))))
 
+    def archive(self, elem=None):
+        """The cereal image of unique_ptr<RBM<T>> (Serializers/SerializeRBM.hpp) as bytes;
+        elem defaults to the machine's own type."""
+        elem = self.dtype if elem is None else elem
+        size = C.c_size_t()
+        check(lib().yq_rbm_archive_size(self.h, elem, C.byref(size)))
+        buf = (C.c_uint8 * size.value)()
+        got = C.c_size_t()
+        check(lib().yq_rbm_save_archive(self.h, elem, buf, size.value, C.byref(got)))
+        return bytes(buf[:got.value])
+
+    def load_archive(self, data, elem=None):
+        elem = self.dtype if elem is None else elem
+        buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+        check(lib().yq_rbm_load_archive(self.h, elem, buf, len(data)))
+
+    def save(self, path, elem=None):
+        check(lib().yq_rbm_save(self.h, self.dtype if elem is None else elem, os.fsencode(path)))
+
+    def load(self, path, elem=None):
+        check(lib().yq_rbm_load(self.h, self.dtype if elem is None else elem, os.fsencode(path)))
+
     def init_random(self, seed, sd):
         check(lib().yq_rbm_init_random(self.h, seed, sd))
 
@@ -349,6 +379,20 @@ class Hamiltonian:
         out = np.zeros(s.shape[0], np.complex128)
         check(lib().yq_eloc(self.h, rbm.h, s.shape[0], _p(s), _p(th), _p(out)))
         return out
+
+
+def archive_shape(data):
+    """(N, M, useBias) of an RBM archive."""
+    n, m, b = C.c_int(), C.c_int(), C.c_int()
+    buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+    check(lib().yq_rbm_archive_shape(buf, len(data), C.byref(n), C.byref(m), C.byref(b)))
+    return n.value, m.value, bool(b.value)
+
+
+def file_shape(path):
+    n, m, b = C.c_int(), C.c_int(), C.c_int()
+    check(lib().yq_rbm_file_shape(os.fsencode(path), C.byref(n), C.byref(m), C.byref(b)))
+    return n.value, m.value, bool(b.value)
 
 
 class Sampler:

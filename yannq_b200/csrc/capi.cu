@@ -291,6 +291,74 @@ int yq_rbm_set_params(yq_rbm q, const double* params) {
     });
 }
 
+int yq_rbm_archive_size(yq_rbm q, int elem, size_t* size) {
+    return guard([&] {
+        need(q, "rbm");
+        need(size, "size");
+        *size = rbm_archive_size(q->n, q->m, q->use_bias, elem);
+    });
+}
+
+int yq_rbm_save_archive(yq_rbm q, int elem, void* buf, size_t cap, size_t* size) {
+    return guard([&] {
+        need(q, "rbm");
+        need(buf, "buf");
+        std::vector<uint8_t> out;
+        rbm_archive_write(q, elem, out);
+        if (size) *size = out.size();
+        if (cap < out.size()) throw Error(YQ_E_ARG, "archive: buffer smaller than yq_rbm_archive_size");
+        std::memcpy(buf, out.data(), out.size());
+    });
+}
+
+int yq_rbm_load_archive(yq_rbm q, int elem, const void* buf, size_t size) {
+    return guard([&] {
+        need(q, "rbm");
+        need(buf, "buf");
+        rbm_archive_read(q, elem, static_cast<const uint8_t*>(buf), size);
+    });
+}
+
+int yq_rbm_archive_shape(const void* buf, size_t size, int* n, int* m, int* use_bias) {
+    return guard([&] {
+        need(buf, "buf");
+        need(n, "n");
+        need(m, "m");
+        need(use_bias, "use_bias");
+        rbm_archive_shape(static_cast<const uint8_t*>(buf), size, n, m, use_bias);
+    });
+}
+
+int yq_rbm_save(yq_rbm q, int elem, const char* path) {
+    return guard([&] {
+        need(q, "rbm");
+        need(path, "path");
+        std::vector<uint8_t> out;
+        rbm_archive_write(q, elem, out);
+        write_file(path, out);
+    });
+}
+
+int yq_rbm_load(yq_rbm q, int elem, const char* path) {
+    return guard([&] {
+        need(q, "rbm");
+        need(path, "path");
+        const std::vector<uint8_t> buf = read_file(path);
+        rbm_archive_read(q, elem, buf.data(), buf.size());
+    });
+}
+
+int yq_rbm_file_shape(const char* path, int* n, int* m, int* use_bias) {
+    return guard([&] {
+        need(path, "path");
+        need(n, "n");
+        need(m, "m");
+        need(use_bias, "use_bias");
+        const std::vector<uint8_t> buf = read_file(path);
+        rbm_archive_shape(buf.data(), buf.size(), n, m, use_bias);
+    });
+}
+
 int yq_rbm_get_params(yq_rbm q, double* params) {
     return guard([&] {
         need(q, "rbm");

@@ -176,6 +176,13 @@ void rbm_init_params_host(int n, int m, bool bias, uint64_t seed, double sd, c12
 
 void sampler_run(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, uint32_t epoch, int reinit);
 
+// RBM checkpoints (cereal binary image of unique_ptr<RBM<T>>)
+size_t rbm_archive_size(int n, int m, bool bias, int elem);
+void rbm_archive_shape(const uint8_t* buf, size_t size, int* n, int* m, int* use_bias);
+void rbm_archive_write(yq_rbm_s* q, int elem, std::vector<uint8_t>& out);
+void rbm_archive_read(yq_rbm_s* q, int elem, const uint8_t* buf, size_t size);
+std::vector<uint8_t> read_file(const char* path);
+void write_file(const char* path, const std::vector<uint8_t>& buf);
 void ham_build_terms(yq_ham_s* H, double jy, double jz);  // term-table kinds
 void ham_build_moves(yq_ham_s* H);                        // offDiagonals list, every kind
 int ham_num_offdiag(const yq_ham_s* H);
