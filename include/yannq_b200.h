@@ -51,6 +51,8 @@ typedef struct yq_rbm_s* yq_rbm;
 typedef struct yq_ham_s* yq_ham;
 typedef struct yq_sampler_s* yq_sampler;
 typedef struct yq_sr_s* yq_sr;
+typedef struct yq_ap_s* yq_ap;
+typedef struct yq_ngd_s* yq_ngd;
 
 /* Message of the last failed call on this thread (always NUL-terminated). */
 int yq_last_error(char* buf, size_t len);
@@ -334,6 +336,65 @@ typedef struct yq_batch_s* yq_batch;
 int yq_batch_create(yq_ctx ctx, int nprob, const yq_sr* srs, yq_batch* out);
 int yq_batch_iteration(yq_batch B, const yq_iter_params* p, yq_iter_result* results);
 int yq_batch_destroy(yq_batch B);
+
+/* ---- AmplitudePhase and NGDExact (Machines/AmplitudePhase.hpp, ----------
+ * ---- GroundState/NGDExact.hpp, Runners/RunAmplitudePhase.hpp) ----------- */
+/* Phase-network layers: 6 ints per layer {type, a, b, k, stride, use_bias} and one
+ * double x.  YQ_LAYER_CONV1D: Conv1D(a = inChannels, b = outChannels, k =
+ * kernelSize, stride, useBias) (layers/Conv1D.hpp:57-65, periodic); YQ_LAYER_FC:
+ * FullyConnected(a = inputDim, b = outputDim, useBias); the activation layers of
+ * layers/ActivationLayer.hpp with x = Tanh's constant, LeakyReLU's negative
+ * slope, LeakyHardTanh's outside slope or Cos's a (layers/activations.hpp; the
+ * Sigmoid forward exp(z) + 1 and Jacobian (1 - a) a are restated as written). */
+enum { YQ_LAYER_CONV1D = 0, YQ_LAYER_FC = 1, YQ_ACT_IDENTITY = 10, YQ_ACT_LNCOSH = 11, YQ_ACT_TANH = 12,
+       YQ_ACT_WEAKTANH = 13, YQ_ACT_SIGMOID = 14, YQ_ACT_RELU = 15, YQ_ACT_LEAKYRELU = 16, YQ_ACT_HARDTANH = 17,
+       YQ_ACT_SOFTSHRINK = 18, YQ_ACT_LEAKYHARDTANH = 19, YQ_ACT_SOFTSIGN = 20, YQ_ACT_COS = 21 };
+enum { YQ_INIT_LECUN = 0, YQ_INIT_XAVIER = 1, YQ_INIT_HE = 2 };  /* FeedForward.hpp InitializationMode */
+enum { YQ_NGD_GRAD = 0, YQ_NGD_OLOC_AMP = 1, YQ_NGD_OLOC_PHASE = 2, YQ_NGD_CORR_AMP = 3, YQ_NGD_CORR_PHASE = 4 };
+enum { YQ_NGD_AMP = 0, YQ_NGD_PHASE = 1, YQ_NGD_ALL = 2 };      /* RunAmplitudePhase.hpp Mode */
+/* AmplitudePhase(N = n, M = m, useBias, FeedForward<double>&& phase) --
+ * AmplitudePhase.hpp:37-40: psi = sqrt(A) exp(i pi phi), A = exp(a.s + sum_j
+ * logCosh(theta_j)) of a real RBM<double>, phi the network's single output.
+ * Parameters are real: [amplitude in the RBM layout W (m x n col-major) | a | b,
+ * then each layer's parameters in order (Conv1D kernel (in k) x out col-major then
+ * bias, FullyConnected weight in x out col-major then bias)]. */
+int yq_ap_create(yq_ctx ctx, int n, int m, int use_bias, int nlayers, const int* layers, const double* layer_x,
+                 yq_ap* out);
+int yq_ap_destroy(yq_ap q);
+/* getDimAmp(), getDimPhase() -- AmplitudePhase.hpp:61-74 */
+int yq_ap_dims(yq_ap q, size_t* dim_amp, size_t* dim_phase);
+int yq_ap_set_params(yq_ap q, const double* params);
+int yq_ap_get_params(yq_ap q, double* params);
+/* updateParams -- AmplitudePhase.hpp:156-161 */
+int yq_ap_update_params(yq_ap q, const double* delta);
+/* initializeRandom(re, sigma) -- AmplitudePhase.hpp:92-97: amplitude N(0, sigma^2)
+ * in the RBM draw order, then every parameterised layer N(0, s^2) with s from
+ * FeedForward.hpp initializeRandom(re, mode) (LeCun sqrt(1/fanIn), Xavier
+ * sqrt(2/(fanIn + fanOut)), He sqrt(2/fanIn)); the reference initializes the
+ * phase with Xavier.  Normals: the first Box-Muller value of Philox4x32-10 draw
+ * (seed; counter e, 0, 0, parameter tag), e counting through both blocks. */
+int yq_ap_init_random(yq_ap q, uint64_t seed, double sigma_amp, int phase_mode);
+/* log psi = log(A) / 2 + i pi phi over a batch (AmplitudePhase::coeff, :132-143). out: ns complex. */
+int yq_ap_log_psi(yq_ap q, int ns, const int8_t* sigma, double* out);
+/* logDeriv -- AmplitudePhase.hpp:42-59: rows [RBM logDeriv / 2 | i pi backward]; out ns x dim complex. */
+int yq_ap_log_deriv(yq_ap q, int ns, const int8_t* sigma, double* out);
+/* NGDExact(qs, basis, col) -- NGDExact.hpp:196-208: the full basis or the Jz basis
+ * (nup spins down; needs a Hamiltonian that conserves Sz) and the Hamiltonian's
+ * column form, applied matrix-free.  The machine and H must outlive the object. */
+int yq_ngd_create(yq_ap q, yq_ham H, int basis_kind, int nup, yq_ngd* out);
+int yq_ngd_destroy(yq_ngd g);
+int yq_ngd_basis_size(yq_ngd g, uint64_t* dim);
+/* constructExact -- NGDExact.hpp:123-150; energy = eloc() (may be null). */
+int yq_ngd_construct(yq_ngd g, double* energy);
+/* energyGrad (dim), olocAmp (Pa), olocPhase (Pp), corrMatAmp (Pa x Pa), corrMatPhase
+ * (Pp x Pp, row-major) of the last construct -- NGDExact.hpp:152-194. */
+int yq_ngd_get(yq_ngd g, int what, double* out);
+/* One epoch of RunAmplitudePhaseExact::run (Runners/RunAmplitudePhase.hpp:92-119):
+ * constructExact, v = (corrMat + lambda I)^{-1} grad by LLT for the amplitude and/or
+ * phase block (mode), params += -lr v (SGD.hpp:48-54 with a caller-given rate).
+ * Returns E before the update, |grad| and |v|.  A non-positive pivot returns
+ * YQ_E_NOT_PD (the reference ignores it). */
+int yq_ngd_iteration(yq_ngd g, double lambda, double lr, int mode, double* energy, double* grad_norm, double* v_norm);
 
 #ifdef __cplusplus
 }

@@ -889,4 +889,290 @@ void ff_backward(const FFNet& f, const int8_t* s, double* der) {
                 der[ki + size_t(K) * oc] += A.in[(r + ki - K / 2 + L) % L] * dz1[r + oc * L];
 }
 
+
+// ---------------------------------------------------------------------------
+// AmplitudePhase machine and NGDExact.
+
+void ap_layout(APNet& q) {
+    q.Pa = size_t(q.n) * q.m + (q.bias ? size_t(q.n + q.m) : 0);
+    int size = q.n;
+    size_t off = q.Pa;
+    for (Layer& L : q.layers) {
+        L.in_size = size;
+        L.off = off;
+        if (L.type == L_CONV1D) {  // layers/Conv1D.hpp:57-65, :104-106
+            if (L.a < 1 || L.b < 1 || L.k < 1 || L.stride < 1 || size % L.a) throw std::runtime_error("conv1d shape");
+            const int in_len = size / L.a;
+            if (L.k / 2 > in_len) throw std::runtime_error("conv1d kernel");
+            L.out_size = (in_len / L.stride) * L.b;
+            L.npar = size_t(L.a) * L.b * L.k + (L.bias ? size_t(L.b) : 0);
+        } else if (L.type == L_FC) {  // layers/FullyConnected.hpp
+            if (L.a != size || L.b < 1) throw std::runtime_error("fc shape");
+            L.out_size = L.b;
+            L.npar = size_t(L.a) * L.b + (L.bias ? size_t(L.b) : 0);
+        } else {
+            L.out_size = size;
+            L.npar = 0;
+        }
+        off += L.npar;
+        size = L.out_size;
+    }
+    if (size != 1) throw std::runtime_error("the phase network must end in one output");
+    q.Pp = off - q.Pa;
+}
+
+// activations.hpp forward and ApplyJacobian, as written there
+static double act_fwd(const Layer& L, double z) {
+    switch (L.type) {
+        case A_IDENTITY: return z;
+        case A_LNCOSH: return logCosh(z);
+        case A_TANH: return L.x * std::tanh(z / L.x);
+        case A_WEAKTANH: return z - std::tanh(z) / 2.0;
+        case A_SIGMOID: return std::exp(z) + 1.;  // activations.hpp:215-220 (the inverse() results are discarded)
+        case A_RELU: return std::max(z, 0.0);
+        case A_LEAKYRELU: return z > 0 ? z : L.x * z;
+        case A_HARDTANH: return std::abs(z) > 1.0 ? std::copysign(1.0, z) : z;
+        case A_SOFTSHRINK: return std::abs(z) < 1.0 ? 0.0 : (z - std::copysign(1.0, z));
+        case A_LEAKYHARDTANH: {
+            double v = std::abs(z) > 1.0 ? std::copysign(1.0, z) : z;
+            v += std::abs(z) < 1.0 ? 0.0 : L.x * (z - std::copysign(1.0, z));
+            return v;
+        }
+        case A_SOFTSIGN: return z / (std::abs(z) + 1.0);
+        case A_COS: return L.x * std::cos(z * M_PI / L.x);
+        default: throw std::runtime_error("unknown activation");
+    }
+}
+static double act_jac(const Layer& L, double z, double a, double f) {
+    switch (L.type) {
+        case A_IDENTITY: return f;
+        case A_LNCOSH: return f * std::tanh(z);
+        case A_TANH: return f * (1. - a * a / (L.x * L.x));
+        case A_WEAKTANH: {
+            const double t = std::tanh(z);
+            return f * (1.0 + t * t) / 2.0;
+        }
+        case A_SIGMOID: return (1. - a) * a;  // activations.hpp:226-229 (F unused)
+        case A_RELU: return z > 0 ? f : 0.0;
+        case A_LEAKYRELU: return z > 0 ? f : L.x * f;
+        case A_HARDTANH: return std::abs(z) > 1.0 ? 0.0 : f;
+        case A_SOFTSHRINK: return std::abs(z) < 1.0 ? 0.0 : f;
+        case A_LEAKYHARDTANH: return std::abs(z) > 1.0 ? L.x * f : f;
+        case A_SOFTSIGN: {
+            const double d = 1.0 + std::abs(z);
+            return (1.0 / (d * d)) * f;
+        }
+        case A_COS: return -M_PI * std::sin(M_PI * z / L.x) * f;
+        default: throw std::runtime_error("unknown activation");
+    }
+}
+
+std::vector<std::vector<double>> ap_phase_data(const APNet& q, const int8_t* s) {
+    std::vector<std::vector<double>> data;
+    data.emplace_back(s, s + q.n);
+    for (const Layer& L : q.layers) {
+        const std::vector<double>& in = data.back();
+        std::vector<double> out(size_t(L.out_size), 0.0);
+        const double* w = q.p + L.off;
+        if (L.type == L_CONV1D) {  // Conv1D.hpp:144-171
+            const int in_len = L.in_size / L.a, out_len = in_len / L.stride, K = L.k;
+            for (int oc = 0; oc < L.b; ++oc)
+                for (int r = 0; r < out_len; ++r)
+                    for (int ic = 0; ic < L.a; ++ic)
+                        for (int ki = 0; ki < K; ++ki)
+                            out[size_t(r + oc * out_len)] +=
+                                w[size_t(ki + ic * K) + size_t(oc) * L.a * K] *
+                                in[size_t((r * L.stride + ki - K / 2 + in_len) % in_len + ic * in_len)];
+            if (L.bias) {
+                const double* b = w + size_t(L.a) * L.b * K;
+                for (int oc = 0; oc < L.b; ++oc)
+                    for (int r = 0; r < out_len; ++r) out[size_t(r + oc * out_len)] += b[oc];
+            }
+        } else if (L.type == L_FC) {  // FullyConnected.hpp forward: bias + W^T in
+            for (int o = 0; o < L.b; ++o) {
+                double acc = L.bias ? w[size_t(L.a) * L.b + o] : 0.0;
+                double t = 0.;
+                for (int i = 0; i < L.a; ++i) t += w[size_t(i) + size_t(o) * L.a] * in[size_t(i)];
+                out[size_t(o)] = acc + t;
+            }
+        } else {
+            for (int i = 0; i < L.in_size; ++i) out[size_t(i)] = act_fwd(L, in[size_t(i)]);
+        }
+        data.push_back(std::move(out));
+    }
+    return data;
+}
+
+// FeedForward::backward (FeedForward.hpp:186-205) with dout = 1
+void ap_phase_backward(const APNet& q, const std::vector<std::vector<double>>& data, double* der) {
+    std::vector<double> dout(1, 1.0);
+    for (int idx = int(q.layers.size()) - 1; idx >= 0; --idx) {
+        const Layer& L = q.layers[size_t(idx)];
+        const std::vector<double>& prev = data[size_t(idx)];
+        const std::vector<double>& cur = data[size_t(idx) + 1];
+        std::vector<double> din(size_t(L.in_size), 0.0);
+        const double* w = q.p + L.off;
+        double* d = der + (L.off - q.Pa);
+        if (L.type == L_CONV1D) {  // Conv1D.hpp:173-225
+            const int in_len = L.in_size / L.a, out_len = in_len / L.stride, K = L.k;
+            for (size_t e = 0; e < L.npar; ++e) d[e] = 0.0;
+            for (int oc = 0; oc < L.b; ++oc)
+                for (int r = 0; r < out_len; ++r)
+                    for (int ic = 0; ic < L.a; ++ic)
+                        for (int ki = 0; ki < K; ++ki) {
+                            const size_t src = size_t((r * L.stride + ki - K / 2 + in_len) % in_len + ic * in_len);
+                            const size_t wi = size_t(ki + ic * K) + size_t(oc) * L.a * K;
+                            din[src] += w[wi] * dout[size_t(r + oc * out_len)];
+                            d[wi] += prev[src] * dout[size_t(r + oc * out_len)];
+                        }
+            if (L.bias)
+                for (int oc = 0; oc < L.b; ++oc)
+                    for (int r = 0; r < out_len; ++r) d[size_t(L.a) * L.b * K + oc] += dout[size_t(r + oc * out_len)];
+        } else if (L.type == L_FC) {  // FullyConnected.hpp backprop
+            for (int o = 0; o < L.b; ++o)
+                for (int i = 0; i < L.a; ++i) d[size_t(i) + size_t(o) * L.a] = prev[size_t(i)] * dout[size_t(o)];
+            if (L.bias)
+                for (int o = 0; o < L.b; ++o) d[size_t(L.a) * L.b + o] = dout[size_t(o)];
+            for (int i = 0; i < L.a; ++i) {
+                double t = 0.;
+                for (int o = 0; o < L.b; ++o) t += w[size_t(i) + size_t(o) * L.a] * dout[size_t(o)];
+                din[size_t(i)] = t;
+            }
+        } else {
+            for (int i = 0; i < L.in_size; ++i)
+                din[size_t(i)] = act_jac(L, prev[size_t(i)], cur[size_t(i)], dout[size_t(i)]);
+        }
+        dout = std::move(din);
+    }
+}
+
+static void amp_theta(const APNet& q, const int8_t* s, std::vector<double>& th) {
+    th.assign(size_t(q.m), 0.0);
+    const size_t nm = size_t(q.n) * q.m;
+    for (int j = 0; j < q.m; ++j) {
+        double t = q.bias ? q.p[nm + q.n + j] : 0.0;
+        for (int i = 0; i < q.n; ++i) t += q.p[size_t(j) + size_t(i) * q.m] * s[i];
+        th[size_t(j)] = t;
+    }
+}
+
+// Machines/RBM.hpp:367-378 for real T
+double ap_log_amp(const APNet& q, const int8_t* s) {
+    std::vector<double> th;
+    amp_theta(q, s, th);
+    const size_t nm = size_t(q.n) * q.m;
+    double acc = 0.;
+    if (q.bias)
+        for (int i = 0; i < q.n; ++i) acc += q.p[nm + i] * s[i];
+    for (int j = 0; j < q.m; ++j) acc += logCosh(th[size_t(j)]);
+    return acc;
+}
+
+// AmplitudePhase::logDerivAmp = RBM::logDeriv / 2 (RBM.hpp:390-406)
+void ap_log_deriv_amp(const APNet& q, const int8_t* s, double* out) {
+    std::vector<double> th;
+    amp_theta(q, s, th);
+    const size_t nm = size_t(q.n) * q.m;
+    for (int i = 0; i < q.n; ++i)
+        for (int j = 0; j < q.m; ++j) out[size_t(i) * q.m + j] = s[i] * std::tanh(th[size_t(j)]) / 2.0;
+    if (!q.bias) return;
+    for (int i = 0; i < q.n; ++i) out[nm + i] = s[i] / 2.0;
+    for (int j = 0; j < q.m; ++j) out[nm + q.n + j] = std::tanh(th[size_t(j)]) / 2.0;
+}
+
+// Real draws: entry e of the amplitude (order a, b, W by columns) and of the
+// phase (layer by layer, FeedForward.hpp initializeRandom) uses the first normal
+// of normal_pair(seed, e); the phase continues the counter after the amplitude.
+void ap_init(const APNet& q, uint64_t seed, double sigma_amp, int mode, double* p) {
+    uint32_t e = 0;
+    const size_t nm = size_t(q.n) * q.m;
+    if (q.bias) {
+        for (int i = 0; i < q.n; ++i) p[nm + i] = sigma_amp * normal_pair(seed, e++, nullptr);
+        for (int j = 0; j < q.m; ++j) p[nm + q.n + j] = sigma_amp * normal_pair(seed, e++, nullptr);
+    }
+    for (int i = 0; i < q.n; ++i)
+        for (int j = 0; j < q.m; ++j) p[size_t(i) * q.m + j] = sigma_amp * normal_pair(seed, e++, nullptr);
+    for (const Layer& L : q.layers) {
+        if (L.npar == 0) continue;
+        // fanIn / fanOut: Conv1D.hpp:227-234, FullyConnected.hpp
+        const double fin = L.type == L_CONV1D ? double(L.a) * L.k : double(L.a);
+        const double fout = L.type == L_CONV1D ? double(L.b) * L.k : double(L.b);
+        const double sd = mode == 0 ? std::sqrt(1.0 / fin) : mode == 1 ? std::sqrt(2.0 / (fin + fout)) : std::sqrt(2.0 / fin);
+        for (size_t k = 0; k < L.npar; ++k) p[L.off + k] = sd * normal_pair(seed, e++, nullptr);
+    }
+}
+
+// GroundState/NGDExact.hpp:123-150 (constructExact), :177-189 (corrMat*)
+NGDResult ngd_exact(const APNet& q, const Ham& H, const std::vector<uint64_t>& basis, bool with_corr, int nthreads) {
+    const size_t dim = basis.size(), Pa = q.Pa, Pp = q.Pp;
+    const int nt = nthreads_or_default(nthreads);
+    std::vector<cd> psi(dim);
+    std::vector<double> Da(dim * Pa), Dp(dim * Pp);
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nt)
+    for (size_t k = 0; k < dim; ++k) {
+        std::vector<int8_t> s(size_t(q.n));
+        for (int i = 0; i < q.n; ++i) s[size_t(i)] = ((basis[k] >> i) & 1u) ? int8_t(-1) : int8_t(1);
+        auto data = ap_phase_data(q, s.data());
+        const double phi = data.back()[0];
+        // AmplitudePhase::coeff: sqrt(A) exp(i pi phi)
+        psi[k] = std::sqrt(std::exp(ap_log_amp(q, s.data()))) * std::exp(cd(0., M_PI * phi));
+        ap_log_deriv_amp(q, s.data(), Da.data() + k * Pa);
+        ap_phase_backward(q, data, Dp.data() + k * Pp);
+        for (size_t c = 0; c < Pp; ++c) Dp[k * Pp + c] *= M_PI;  // logDerivPhase = pi * backward
+    }
+    double nrm = 0.;
+    for (auto& z : psi) nrm += std::norm(z);
+    nrm = std::sqrt(nrm);
+    for (auto& z : psi) z /= nrm;
+    // k = H_sub psi, H_sub(idx, j) = col(basis[idx])[basis[j]] (ED/ConstructSparseMat.hpp:31-56)
+    std::vector<cd> kv(dim);
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (size_t idx = 0; idx < dim; ++idx) {
+        auto col = ham_column(H, basis[idx]);
+        cd acc = 0.;
+        for (auto& e : col) {
+            auto it = std::lower_bound(basis.begin(), basis.end(), e.first);
+            if (it == basis.end() || *it != e.first) continue;
+            acc += e.second * psi[size_t(it - basis.begin())];
+        }
+        kv[idx] = acc;
+    }
+    NGDResult R;
+    cd e = 0.;
+    for (size_t k = 0; k < dim; ++k) e += std::conj(psi[k]) * kv[k];
+    R.energy = e.real();
+    R.oloc_amp.assign(Pa, 0.);
+    R.oloc_phase.assign(Pp, 0.);
+    R.grad.assign(Pa + Pp, 0.);
+    for (size_t k = 0; k < dim; ++k) {
+        const double w = std::norm(psi[k]);
+        const cd g = std::conj(psi[k]) * kv[k];
+        for (size_t c = 0; c < Pa; ++c) {
+            R.oloc_amp[c] += w * Da[k * Pa + c];
+            R.grad[c] += 2.0 * Da[k * Pa + c] * g.real();
+        }
+        for (size_t c = 0; c < Pp; ++c) {
+            R.oloc_phase[c] += w * Dp[k * Pp + c];
+            R.grad[Pa + c] += 2.0 * Dp[k * Pp + c] * g.imag();
+        }
+    }
+    for (size_t c = 0; c < Pa; ++c) R.grad[c] -= 2.0 * R.energy * R.oloc_amp[c];
+    if (!with_corr) return R;
+    auto corr = [&](const std::vector<double>& D, size_t P, const std::vector<double>& o, std::vector<double>& C) {
+        C.assign(P * P, 0.);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+        for (size_t r = 0; r < P; ++r)
+            for (size_t c = 0; c <= r; ++c) {
+                double t = 0.;
+                for (size_t k = 0; k < dim; ++k) t += D[k * P + r] * std::norm(psi[k]) * D[k * P + c];
+                t -= o[r] * o[c];
+                C[r * P + c] = t;
+                C[c * P + r] = t;
+            }
+    };
+    corr(Da, Pa, R.oloc_amp, R.corr_amp);
+    corr(Dp, Pp, R.oloc_phase, R.corr_phase);
+    return R;
+}
+
 }  // namespace orc

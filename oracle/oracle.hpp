@@ -278,4 +278,43 @@ struct FFNet {
 double ff_forward(const FFNet& f, const int8_t* s);
 void ff_backward(const FFNet& f, const int8_t* s, double* der);
 
+// ---------------------------------------------------------------------------
+// AmplitudePhase (Machines/AmplitudePhase.hpp:9-178): a real RBM<double> amplitude
+// and a FeedForward<double> phase (Machines/FeedForward.hpp) of layers
+// Conv1D (layers/Conv1D.hpp), FullyConnected (layers/FullyConnected.hpp) and the
+// activation layers of layers/ActivationLayer.hpp / activations.hpp.
+// psi(s) = sqrt(A(s)) exp(i pi phi(s)), A = exp(a.s + sum_j logCosh(theta_j)).
+enum LayerType {
+    L_CONV1D = 0, L_FC = 1,
+    A_IDENTITY = 10, A_LNCOSH = 11, A_TANH = 12, A_WEAKTANH = 13, A_SIGMOID = 14, A_RELU = 15, A_LEAKYRELU = 16,
+    A_HARDTANH = 17, A_SOFTSHRINK = 18, A_LEAKYHARDTANH = 19, A_SOFTSIGN = 20, A_COS = 21
+};
+struct Layer {
+    int type = 0;
+    int a = 0, b = 0, k = 0, stride = 1, bias = 0;  // Conv1D: in, out channels, kernel; FC: in, out
+    double x = 0.;                                   // activation constant / slope
+    int in_size = 0, out_size = 0;                   // set by ap_layout
+    size_t npar = 0, off = 0;                        // parameters of the layer and their offset
+};
+struct APNet {
+    int n = 0, m = 0;
+    bool bias = true;
+    std::vector<Layer> layers;
+    size_t Pa = 0, Pp = 0;
+    const double* p = nullptr;  // [amplitude RBM (reference layout) | phase layers in order]
+};
+void ap_layout(APNet& q);  // sizes and offsets; throws on a bad stack
+std::vector<std::vector<double>> ap_phase_data(const APNet& q, const int8_t* s);   // FeedForward::makeData
+void ap_phase_backward(const APNet& q, const std::vector<std::vector<double>>& data, double* der);
+double ap_log_amp(const APNet& q, const int8_t* s);  // log A(s) = RBM<double>::logCoeff
+void ap_log_deriv_amp(const APNet& q, const int8_t* s, double* out);  // RBM logDeriv / 2
+void ap_init(const APNet& q, uint64_t seed, double sigma_amp, int mode, double* p);  // LeCun 0, Xavier 1, He 2
+// GroundState/NGDExact.hpp:123-189 over a basis: energy, grad (Pa + Pp), oloc of
+// both blocks, the two correlation matrices (row-major) when requested.
+struct NGDResult {
+    double energy = 0.;
+    std::vector<double> grad, oloc_amp, oloc_phase, corr_amp, corr_phase;
+};
+NGDResult ngd_exact(const APNet& q, const Ham& H, const std::vector<uint64_t>& basis, bool with_corr, int nthreads);
+
 }  // namespace orc

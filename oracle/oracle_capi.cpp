@@ -29,6 +29,28 @@ Ham make_ham(int kind, int n, int lx, int ly, const double* hp) {
     H.jz = hp[4];
     return H;
 }
+// Phase layers: desc holds 6 ints per layer (type, a, b, k, stride, bias), xs one
+// double (activation constant / slope).
+APNet make_ap(int n, int m, int use_bias, int nl, const int* desc, const double* xs, const double* p) {
+    APNet q;
+    q.n = n;
+    q.m = m;
+    q.bias = use_bias != 0;
+    for (int l = 0; l < nl; ++l) {
+        Layer L;
+        L.type = desc[6 * l];
+        L.a = desc[6 * l + 1];
+        L.b = desc[6 * l + 2];
+        L.k = desc[6 * l + 3];
+        L.stride = desc[6 * l + 4];
+        L.bias = desc[6 * l + 5];
+        L.x = xs[l];
+        q.layers.push_back(L);
+    }
+    ap_layout(q);
+    q.p = p;
+    return q;
+}
 }  // namespace
 
 extern "C" {
@@ -280,4 +302,73 @@ void orc_ff_batch(int L, int conv_out, int conv_k, int fc_out, const double* par
     }
 }
 
+
+// ---- AmplitudePhase / NGDExact ---------------------------------------------
+int orc_ap_dims(int n, int m, int use_bias, int nl, const int* desc, const double* xs, uint64_t* dims) {
+    try {
+        APNet q = make_ap(n, m, use_bias, nl, desc, xs, nullptr);
+        dims[0] = q.Pa;
+        dims[1] = q.Pp;
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+void orc_ap_init(int n, int m, int use_bias, int nl, const int* desc, const double* xs, uint64_t seed,
+                 double sigma_amp, int mode, double* p) {
+    APNet q = make_ap(n, m, use_bias, nl, desc, xs, p);
+    ap_init(q, seed, sigma_amp, mode, p);
+}
+
+// out: ns complex log psi = log A / 2 + i pi phi
+void orc_ap_log_psi(int n, int m, int use_bias, int nl, const int* desc, const double* xs, const double* p, int ns,
+                    const int8_t* s, double* out) {
+    APNet q = make_ap(n, m, use_bias, nl, desc, xs, p);
+    for (int k = 0; k < ns; ++k) {
+        const int8_t* sk = s + size_t(k) * n;
+        auto data = ap_phase_data(q, sk);
+        out[2 * k] = 0.5 * ap_log_amp(q, sk);
+        out[2 * k + 1] = M_PI * data.back()[0];
+    }
+}
+
+// out: ns x (Pa + Pp) complex rows [logDerivAmp | i logDerivPhase] (AmplitudePhase.hpp:52-59)
+void orc_ap_log_deriv(int n, int m, int use_bias, int nl, const int* desc, const double* xs, const double* p, int ns,
+                      const int8_t* s, double* out) {
+    APNet q = make_ap(n, m, use_bias, nl, desc, xs, p);
+    const size_t P = q.Pa + q.Pp;
+    std::vector<double> da(q.Pa), dp(q.Pp);
+    for (int k = 0; k < ns; ++k) {
+        const int8_t* sk = s + size_t(k) * n;
+        ap_log_deriv_amp(q, sk, da.data());
+        ap_phase_backward(q, ap_phase_data(q, sk), dp.data());
+        double* row = out + 2 * size_t(k) * P;
+        for (size_t c = 0; c < q.Pa; ++c) {
+            row[2 * c] = da[c];
+            row[2 * c + 1] = 0.0;
+        }
+        for (size_t c = 0; c < q.Pp; ++c) {
+            row[2 * (q.Pa + c)] = 0.0;
+            row[2 * (q.Pa + c) + 1] = M_PI * dp[c];
+        }
+    }
+}
+
+int orc_ngd_exact(int kind, int n, int lx, int ly, const double* hp, int m, int use_bias, int nl, const int* desc,
+                  const double* xs, const double* p, int basis_kind, int nup, int with_corr, double* energy,
+                  double* grad, double* oloc_amp, double* oloc_phase, double* corr_amp, double* corr_phase,
+                  int nthreads) {
+    Ham H = make_ham(kind, n, lx, ly, hp);
+    APNet q = make_ap(n, m, use_bias, nl, desc, xs, p);
+    auto basis = basis_kind == 0 ? basis_full(n) : basis_jz(n, nup);
+    NGDResult R = ngd_exact(q, H, basis, with_corr != 0, nthreads);
+    *energy = R.energy;
+    std::memcpy(grad, R.grad.data(), R.grad.size() * sizeof(double));
+    if (oloc_amp) std::memcpy(oloc_amp, R.oloc_amp.data(), R.oloc_amp.size() * sizeof(double));
+    if (oloc_phase) std::memcpy(oloc_phase, R.oloc_phase.data(), R.oloc_phase.size() * sizeof(double));
+    if (with_corr && corr_amp) std::memcpy(corr_amp, R.corr_amp.data(), R.corr_amp.size() * sizeof(double));
+    if (with_corr && corr_phase) std::memcpy(corr_phase, R.corr_phase.data(), R.corr_phase.size() * sizeof(double));
+    return int(basis.size());
+}
 }  // extern "C"

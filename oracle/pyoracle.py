@@ -72,6 +72,11 @@ def _declare(L):
         "orc_exact_sample": (i, [i, i, i, vp, i, i, i, u64, u32, vp, vp, i]),
         "orc_basis": (i, [i, i, i, vp, i]),
         "orc_ed_ground": (d, [i, i, i, i, vp, i, i, i, i]),
+        "orc_ap_dims": (i, [i, i, i, i, vp, vp, vp]),
+        "orc_ap_init": (None, [i, i, i, i, vp, vp, u64, d, i, vp]),
+        "orc_ap_log_psi": (None, [i, i, i, i, vp, vp, vp, i, vp, vp]),
+        "orc_ap_log_deriv": (None, [i, i, i, i, vp, vp, vp, i, vp, vp]),
+        "orc_ngd_exact": (i, [i, i, i, i, vp, i, i, i, vp, vp, vp, i, i, i, vp, vp, vp, vp, vp, vp, i]),
         "orc_ff_forward": (d, [i, i, i, i, vp, vp]),
         "orc_ff_backward": (None, [i, i, i, i, vp, vp, vp]),
         "orc_ff_batch": (None, [i, i, i, i, vp, i, vp, vp, vp, i]),
@@ -420,3 +425,58 @@ def rbm_unarchive(data, elem=1):
         parts += [block(n, 1), block(m, 1)]
     assert at == len(data)
     return n, m, bool(bias), np.concatenate(parts)
+
+
+# ---------------------------------------------------------------------------
+# AmplitudePhase (Machines/AmplitudePhase.hpp) and NGDExact (GroundState/NGDExact.hpp).
+class AP:
+    """Shape of an AmplitudePhase machine: RBM<double>(n, m, use_bias) amplitude and
+    a phase network given as desc (L x 6 ints: type, a, b, k, stride, bias) and xs
+    (L doubles) in the oracle's LayerType numbering."""
+
+    def __init__(self, n, m, use_bias, desc, xs):
+        self.n, self.m, self.use_bias = n, m, bool(use_bias)
+        self.desc = np.ascontiguousarray(desc, np.int32).reshape(-1, 6)
+        self.xs = np.ascontiguousarray(xs, np.float64).reshape(-1)
+        dims = np.zeros(2, np.uint64)
+        if lib().orc_ap_dims(n, m, int(use_bias), len(self.xs), _p(self.desc), _p(self.xs), _p(dims)) != 0:
+            raise ValueError("bad phase network")
+        self.Pa, self.Pp = int(dims[0]), int(dims[1])
+        self.dim = self.Pa + self.Pp
+
+    def args(self):
+        return (self.n, self.m, int(self.use_bias), len(self.xs), _p(self.desc), _p(self.xs))
+
+
+def ap_init(ap, seed, sigma_amp, mode=1):
+    p = np.zeros(ap.dim)
+    lib().orc_ap_init(*ap.args(), seed, sigma_amp, mode, _p(p))
+    return p
+
+
+def ap_log_psi(ap, params, sigma):
+    s = _s8(sigma).reshape(-1, ap.n)
+    out = np.zeros(s.shape[0], np.complex128)
+    lib().orc_ap_log_psi(*ap.args(), _p(np.ascontiguousarray(params, np.float64)), s.shape[0], _p(s), _p(out))
+    return out
+
+
+def ap_log_deriv(ap, params, sigma):
+    s = _s8(sigma).reshape(-1, ap.n)
+    out = np.zeros((s.shape[0], ap.dim), np.complex128)
+    lib().orc_ap_log_deriv(*ap.args(), _p(np.ascontiguousarray(params, np.float64)), s.shape[0], _p(s), _p(out))
+    return out
+
+
+def ngd_exact(ham, ap, params, basis_kind=0, nup=0, with_corr=True, nthreads=0):
+    """NGDExact::constructExact: dict of energy, grad, oloc_amp, oloc_phase, corr_amp, corr_phase."""
+    g = np.zeros(ap.dim)
+    oa, op = np.zeros(ap.Pa), np.zeros(ap.Pp)
+    ca = np.zeros((ap.Pa, ap.Pa)) if with_corr else None
+    cp = np.zeros((ap.Pp, ap.Pp)) if with_corr else None
+    e = C.c_double()
+    k, lx, ly, hp = ham.kind, ham.lx, ham.ly, _p(ham._hp)
+    lib().orc_ngd_exact(k, ham.n, lx, ly, hp, ap.m, int(ap.use_bias), len(ap.xs), _p(ap.desc), _p(ap.xs),
+                        _p(np.ascontiguousarray(params, np.float64)), basis_kind, nup, int(with_corr), C.byref(e),
+                        _p(g), _p(oa), _p(op), _p(ca), _p(cp), nthreads or os.cpu_count())
+    return {"energy": e.value, "grad": g, "oloc_amp": oa, "oloc_phase": op, "corr_amp": ca, "corr_phase": cp}

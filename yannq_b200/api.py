@@ -17,6 +17,12 @@ LIB_PATH = os.path.join(_HERE, "libyannq_b200.so")
 OK, E_ARG, E_CUDA, E_NOMEM, E_NOT_PD, E_NONFINITE, E_TIMEOUT, E_STATE, E_UNSUPPORTED = range(9)
 C64, C128 = 0, 1
 ARCHIVE_C64, ARCHIVE_C128, ARCHIVE_F64, ARCHIVE_F32 = 0, 1, 2, 3
+LAYER_TYPES = {"conv1d": 0, "fc": 1, "identity": 10, "lncosh": 11, "tanh": 12, "weaktanh": 13, "sigmoid": 14,
+               "relu": 15, "leakyrelu": 16, "hardtanh": 17, "softshrink": 18, "leakyhardtanh": 19, "softsign": 20,
+               "cos": 21}
+INIT_LECUN, INIT_XAVIER, INIT_HE = 0, 1, 2
+NGD_GRAD, NGD_OLOC_AMP, NGD_OLOC_PHASE, NGD_CORR_AMP, NGD_CORR_PHASE = 0, 1, 2, 3, 4
+NGD_AMP, NGD_PHASE, NGD_ALL = 0, 1, 2
 HAM_TFI, HAM_XXZ, HAM_TFI2D, HAM_XXX, HAM_J1J2, HAM_XYZNNN, HAM_KITAEV_HEX = 0, 1, 2, 3, 4, 5, 6
 MOVE_LOCAL, MOVE_EXCHANGE_ANY, MOVE_EXCHANGE_NN, MOVE_HAMILTONIAN = 0, 1, 2, 3
 SR_AUTO, SR_S, SR_T = 0, 1, 2
@@ -66,6 +72,21 @@ SIGNATURES = {
     "yq_rbm_save": [_vp, _i, C.c_char_p],
     "yq_rbm_load": [_vp, _i, C.c_char_p],
     "yq_rbm_file_shape": [C.c_char_p, _vp, _vp, _vp],
+    "yq_ap_create": [_vp, _i, _i, _i, _i, _vp, _vp, _vp],
+    "yq_ap_destroy": [_vp],
+    "yq_ap_dims": [_vp, _vp, _vp],
+    "yq_ap_set_params": [_vp, _vp],
+    "yq_ap_get_params": [_vp, _vp],
+    "yq_ap_update_params": [_vp, _vp],
+    "yq_ap_init_random": [_vp, C.c_uint64, _d, _i],
+    "yq_ap_log_psi": [_vp, _i, _vp, _vp],
+    "yq_ap_log_deriv": [_vp, _i, _vp, _vp],
+    "yq_ngd_create": [_vp, _vp, _i, _i, _vp],
+    "yq_ngd_destroy": [_vp],
+    "yq_ngd_basis_size": [_vp, _vp],
+    "yq_ngd_construct": [_vp, _vp],
+    "yq_ngd_get": [_vp, _i, _vp],
+    "yq_ngd_iteration": [_vp, _d, _d, _i, _vp, _vp, _vp],
     "yq_rbm_set_params": [_vp, _vp],
     "yq_rbm_get_params": [_vp, _vp],
     "yq_rbm_update_params": [_vp, _vp],
@@ -593,3 +614,120 @@ class FeedForward:
         out = np.zeros(self.batch, np.complex128) if copy else None
         check(lib().yq_ff_eloc_tfi(self.h, J, h, _p(out)))
         return out
+
+
+# ---------------------------------------------------------------------------
+def encode_layers(spec):
+    """Phase-network layers in the C ABI's encoding from a list such as
+    [("conv1d", in_ch, out_ch, kernel[, stride[, bias]]), ("leakyhardtanh", 0.01),
+     ("fc", in_dim, out_dim[, bias]), ("softsign",)].  Returns (desc, xs)."""
+    desc, xs = [], []
+    for layer in spec:
+        kind, args = layer[0], list(layer[1:])
+        t = LAYER_TYPES[kind]
+        if kind == "conv1d":
+            a, b, k = args[:3]
+            stride = args[3] if len(args) > 3 else 1
+            bias = args[4] if len(args) > 4 else False
+            desc.append([t, a, b, k, stride, int(bool(bias))])
+            xs.append(0.0)
+        elif kind == "fc":
+            a, b = args[:2]
+            bias = args[2] if len(args) > 2 else True
+            desc.append([t, a, b, 0, 1, int(bool(bias))])
+            xs.append(0.0)
+        else:
+            default = {"tanh": 1.0, "leakyrelu": 0.1, "leakyhardtanh": 0.01, "cos": 1.0}.get(kind, 0.0)
+            desc.append([t, 0, 0, 0, 1, 0])
+            xs.append(float(args[0]) if args else default)
+    return np.ascontiguousarray(desc, np.int32), np.ascontiguousarray(xs, np.float64)
+
+
+class AmplitudePhase:
+    """Machines/AmplitudePhase.hpp on the device: real RBM amplitude, FeedForward phase."""
+
+    def __init__(self, ctx, n, m, use_bias, layers):
+        self.ctx, self.n, self.m, self.use_bias = ctx, n, m, bool(use_bias)
+        self.desc, self.xs = encode_layers(layers) if not isinstance(layers, tuple) else layers
+        h = C.c_void_p()
+        check(lib().yq_ap_create(ctx.h, n, m, int(use_bias), len(self.xs), _p(self.desc), _p(self.xs), C.byref(h)))
+        self.h = h
+        a, b = C.c_size_t(), C.c_size_t()
+        check(lib().yq_ap_dims(h, C.byref(a), C.byref(b)))
+        self.dim_amp, self.dim_phase = a.value, b.value
+        self.dim = self.dim_amp + self.dim_phase
+
+    def close(self):
+        if self.h:
+            check(lib().yq_ap_destroy(self.h))
+            self.h = None
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float64)
+        assert p.size == self.dim
+        check(lib().yq_ap_set_params(self.h, _p(p)))
+
+    def get_params(self):
+        p = np.zeros(self.dim)
+        check(lib().yq_ap_get_params(self.h, _p(p)))
+        return p
+
+    def update_params(self, d):
+        d = np.ascontiguousarray(d, np.float64)
+        check(lib().yq_ap_update_params(self.h, _p(d)))
+
+    def init_random(self, seed, sigma_amp, mode=INIT_XAVIER):
+        check(lib().yq_ap_init_random(self.h, seed, sigma_amp, mode))
+
+    def log_psi(self, sigma):
+        s = _s8(sigma).reshape(-1, self.n)
+        out = np.zeros(s.shape[0], np.complex128)
+        check(lib().yq_ap_log_psi(self.h, s.shape[0], _p(s), _p(out)))
+        return out
+
+    def log_deriv(self, sigma):
+        s = _s8(sigma).reshape(-1, self.n)
+        out = np.zeros((s.shape[0], self.dim), np.complex128)
+        check(lib().yq_ap_log_deriv(self.h, s.shape[0], _p(s), _p(out)))
+        return out
+
+
+class NGDExact:
+    """GroundState/NGDExact.hpp on the device; iteration() is one epoch of
+    RunAmplitudePhaseExact (Runners/RunAmplitudePhase.hpp)."""
+
+    def __init__(self, ap, ham, basis_kind=BASIS_FULL, nup=0):
+        self.ap, self.ham = ap, ham
+        h = C.c_void_p()
+        check(lib().yq_ngd_create(ap.h, ham.h, basis_kind, nup, C.byref(h)))
+        self.h = h
+        d = C.c_uint64()
+        check(lib().yq_ngd_basis_size(h, C.byref(d)))
+        self.basis_size = d.value
+
+    def close(self):
+        if self.h:
+            check(lib().yq_ngd_destroy(self.h))
+            self.h = None
+
+    def construct(self):
+        e = C.c_double()
+        check(lib().yq_ngd_construct(self.h, C.byref(e)))
+        return e.value
+
+    def get(self, what):
+        a = self.ap
+        size = {NGD_GRAD: a.dim, NGD_OLOC_AMP: a.dim_amp, NGD_OLOC_PHASE: a.dim_phase,
+                NGD_CORR_AMP: a.dim_amp ** 2, NGD_CORR_PHASE: a.dim_phase ** 2}[what]
+        out = np.zeros(size)
+        check(lib().yq_ngd_get(self.h, what, _p(out)))
+        if what == NGD_CORR_AMP:
+            return out.reshape(a.dim_amp, a.dim_amp)
+        if what == NGD_CORR_PHASE:
+            return out.reshape(a.dim_phase, a.dim_phase)
+        return out
+
+    def iteration(self, lam, lr, mode=NGD_ALL):
+        e, g, v = C.c_double(), C.c_double(), C.c_double()
+        check(lib().yq_ngd_iteration(self.h, lam, lr, mode, C.byref(e), C.byref(g), C.byref(v)))
+        return e.value, g.value, v.value

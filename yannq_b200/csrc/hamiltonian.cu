@@ -7,8 +7,11 @@
 // XYZNNN and KitaevHex are term tables (HamTerm) built on the host in the
 // reference's evaluation order (XXX.hpp:11-22, J1J2.hpp:35-56,
 // XYZNNN.hpp:33-53, KitaevHex.hpp:119-146); the kernels walk the table.
+#include <algorithm>
 #include <vector>
 
+#include "ap.hpp"
+#include "basis.cuh"
 #include "internal.hpp"
 #include "ratio.cuh"
 
@@ -133,6 +136,53 @@ void ham_enumerate(yq_ham_s* H, int ns, const int8_t* d_sigma, int* d_a, int* d_
                                                                             d_c, d_diag);
     else
         enumerate_kernel<<<cdiv_u(ns, 128), 128, 0, H->ctx->stream>>>(desc(H), ns, d_sigma, d_a, d_b, d_c, d_diag);
+    YQ_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// H psi over a basis (NGDExact's sparse product, matrix-free): one thread per
+// configuration walks the state form and gathers psi at the flipped
+// configurations by their basis rank.
+__global__ void apply_basis_kernel(HamDesc H, uint64_t dim, int kind, int nup, const uint64_t* __restrict__ binom,
+                                   const uint64_t* __restrict__ index, const int8_t* __restrict__ sigma,
+                                   const c128* __restrict__ psi, c128* __restrict__ out) {
+    for (uint64_t k = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < dim; k += uint64_t(gridDim.x) * blockDim.x) {
+        const int8_t* s = sigma + k * H.n;
+        const uint64_t v = index[k];
+        double diag = 0.;
+        c128 acc = mk(0., 0.);
+        const bool table = H.nterms > 0;
+        const int nterm = table ? H.nterms : H.n;
+        for (int t = 0; t < nterm; ++t) {
+            int a, b;
+            double c;
+            if (table) {
+                double d;
+                table_term(H.terms[t], s, d, a, b, c);
+                diag += d;
+                if (a < 0) continue;
+            } else {
+                diag += diag_term(H, s, t);
+                offdiag_term(H, s, t, a, b, c);
+            }
+            if (c == 0.0) continue;
+            const uint64_t w = v ^ (uint64_t(1) << a) ^ (b >= 0 ? uint64_t(1) << b : uint64_t(0));
+            const long long j = basis_rank(w, H.n, kind, nup, binom);
+            if (j < 0) continue;
+            const c128 pj = psi[j];
+            acc.re += c * pj.re;
+            acc.im += c * pj.im;
+        }
+        const c128 pk = psi[k];
+        out[k] = mk(acc.re + diag * pk.re, acc.im + diag * pk.im);
+    }
+}
+
+void ham_apply_basis(yq_ham_s* H, uint64_t dim, int kind, int nup, const uint64_t* d_binom, const uint64_t* d_index,
+                     const int8_t* d_sigma, const c128* d_psi, c128* d_out, cudaStream_t st) {
+    if (dim == 0) return;
+    apply_basis_kernel<<<std::max(1u, std::min(148u * 16, cdiv_u(dim, 128))), 128, 0, st>>>(
+        desc(H), dim, kind, nup, d_binom, d_index, d_sigma, d_psi, d_out);
     YQ_LAUNCH_CHECK();
 }
 
