@@ -294,7 +294,71 @@ def suite(api, ctx, hbm_gbs):
     f.close()
     out["ff40"] = ff
     out["batch64"] = batch64(api)
+    out["j1j2_64"] = j1j2_64(api, ctx)
+    out["ngd_ap_j1j2_20"] = ngd_ap(api, ctx)
     return out
+
+
+def j1j2_64(api, ctx):
+    """J1J2 chain N = 64 (J2 = 0.5, sign rule), RBM alpha = 4, complex64, Sz = 0:
+    4096 chains x 32 recorded sweeps (+32 thermalisation) with the HamiltonianSweeper
+    (proposals from the antiparallel NN / NNN bonds, w1 / w2 correction) against
+    neighbour-pair exchanges; E_loc over the 131,072 samples (term table)."""
+    n, m, chains, sweeps = 64, 256, 4096, 32
+    res = {}
+    q = api.RBM(ctx, n, m, True, api.C64)
+    q.init_random(W["seed"], 0.01)
+    H = api.Hamiltonian.j1j2(ctx, n, 1.0, 0.5, True)
+    for name, move in (("hamiltonian_sweeper", api.MOVE_HAMILTONIAN), ("exchange_nn", api.MOVE_EXCHANGE_NN)):
+        S = api.Sampler(q, chains, move, n // 2)
+        if move == api.MOVE_HAMILTONIAN:
+            S.set_hamiltonian(H)
+        S.sample(sweeps, 32, W["seed"], 0, True)
+        S.sample(sweeps, 32, W["seed"], 1, True)
+        t_s = ctx.stage_ms("sample")
+        row = {"sample_ms": t_s, "proposals_per_s": chains * (sweeps + 32) * n / (t_s * 1e-3),
+               "accept_rate": float(S.get_accepts().sum()) / (chains * (sweeps + 32) * n)}
+        if move == api.MOVE_HAMILTONIAN:
+            sr = api.SR(q, H, S, api.SR_S, api.PREC_MIXED)
+            sr.construct()
+            sr.construct()
+            row["eloc_ms"] = ctx.stage_ms("eloc")
+            row["eloc_samples_per_s"] = chains * sweeps / (row["eloc_ms"] * 1e-3)
+            sr.close()
+        res[name] = row
+        S.close()
+    H.close()
+    q.close()
+    return res
+
+
+def ngd_ap(api, ctx, iters=3):
+    """Examples/AmplitudePhase.cpp at N = 20: J1J2(20, 1, 0.44, sign rule), Jz basis
+    (184,756 configurations), RBM alpha = 2 without bias (P_amp = 800) and the
+    example's phase network Conv1D 1->12->10->8->6->4->2 (kernel 5, LeakyHardTanh
+    0.01), FullyConnected(40 -> 1), SoftSign (P_phase = 1,500); one NGDExact epoch
+    (construct, both LLT solves, SGD) per iteration, host wall time around the
+    synchronous call."""
+    n = 20
+    layers = []
+    for a, b in [(1, 12), (12, 10), (10, 8), (8, 6), (6, 4), (4, 2)]:
+        layers += [("conv1d", a, b, 5), ("leakyhardtanh", 0.01)]
+    layers += [("fc", 2 * n, 1, False), ("softsign",)]
+    q = api.AmplitudePhase(ctx, n, 2 * n, False, layers)
+    q.init_random(W["seed"], 0.01, api.INIT_XAVIER)
+    H = api.Hamiltonian.j1j2(ctx, n, 1.0, 0.44, True)
+    g = api.NGDExact(q, H, api.BASIS_JZ, n // 2)
+    g.iteration(10.0, 0.05)  # warm-up
+    t0 = time.perf_counter()
+    for ll in range(iters):
+        e, gn, vn = g.iteration(max(10.0 * 0.9 ** (ll + 1), 1e-3), 0.05)
+    dt = (time.perf_counter() - t0) / iters
+    res = {"basis": g.basis_size, "P_amp": q.dim_amp, "P_phase": q.dim_phase, "ms_per_epoch": dt * 1e3,
+           "epochs_per_s": 1.0 / dt, "energy_per_site": e / n,
+           "gram_flop_per_epoch": 2.0 * g.basis_size * (q.dim_amp ** 2 + q.dim_phase ** 2)}
+    for x in (g, H, q):
+        x.close()
+    return res
 
 
 # DRAM bytes (read + write) of the Ns = 8192, P = 41,904 Gram launch, from one

@@ -448,5 +448,183 @@ public:
     }
 };
 
+// ---------------------------------------------------------------------------
+// Machines/FeedForward.hpp with the layer names of Machines/layers: phase networks
+// are built as in the reference, ff.addLayer<Conv1D>(1, 12, 5, 1, false) or
+// ff.addLayer<LeakyHardTanh>(0.01), and handed to AmplitudePhase.
+struct Conv1D {
+    static void encode(std::vector<int>& d, std::vector<double>& x, int in, int out, int kernel, int stride = 1,
+                       bool useBias = false) {
+        d.insert(d.end(), {YQ_LAYER_CONV1D, in, out, kernel, stride, useBias ? 1 : 0});
+        x.push_back(0.0);
+    }
+};
+struct FullyConnected {
+    static void encode(std::vector<int>& d, std::vector<double>& x, int in, int out, bool useBias = true) {
+        d.insert(d.end(), {YQ_LAYER_FC, in, out, 0, 1, useBias ? 1 : 0});
+        x.push_back(0.0);
+    }
+};
+template <int Type>
+struct Activation {
+    static void encode(std::vector<int>& d, std::vector<double>& x, double c = Type == YQ_ACT_TANH || Type == YQ_ACT_COS ? 1.0
+                                                                              : Type == YQ_ACT_LEAKYRELU     ? 0.1
+                                                                              : Type == YQ_ACT_LEAKYHARDTANH ? 0.01
+                                                                                                             : 0.0) {
+        d.insert(d.end(), {Type, 0, 0, 0, 1, 0});
+        x.push_back(c);
+    }
+};
+using Identity = Activation<YQ_ACT_IDENTITY>;
+using LnCosh = Activation<YQ_ACT_LNCOSH>;
+using Tanh = Activation<YQ_ACT_TANH>;
+using WeakTanh = Activation<YQ_ACT_WEAKTANH>;
+using Sigmoid = Activation<YQ_ACT_SIGMOID>;
+using ReLU = Activation<YQ_ACT_RELU>;
+using LeakyReLU = Activation<YQ_ACT_LEAKYRELU>;
+using HardTanh = Activation<YQ_ACT_HARDTANH>;
+using SoftShrink = Activation<YQ_ACT_SOFTSHRINK>;
+using LeakyHardTanh = Activation<YQ_ACT_LEAKYHARDTANH>;
+using SoftSign = Activation<YQ_ACT_SOFTSIGN>;
+using Cos = Activation<YQ_ACT_COS>;
+
+class FeedForward {
+    std::vector<int> desc_;
+    std::vector<double> x_;
+
+public:
+    template <class Layer, typename... Ts>
+    void addLayer(Ts&&... args) {
+        Layer::encode(desc_, x_, std::forward<Ts>(args)...);
+    }
+    int numLayers() const { return int(x_.size()); }
+    const std::vector<int>& desc() const { return desc_; }
+    const std::vector<double>& x() const { return x_; }
+};
+
+enum class InitializationMode { LeCun = YQ_INIT_LECUN, Xavier = YQ_INIT_XAVIER, He = YQ_INIT_HE };
+
+// Machines/AmplitudePhase.hpp:9-178: psi = sqrt(A) exp(i pi phi); real parameters
+class AmplitudePhase {
+    yq_ap h_ = nullptr;
+    uint32_t n_;
+    size_t dimAmp_ = 0, dimPhase_ = 0;
+
+public:
+    using RealVector = std::vector<double>;
+    AmplitudePhase(Context& ctx, uint32_t N, uint32_t M, bool useBias, FeedForward&& phase) : n_(N) {
+        check(yq_ap_create(ctx.handle(), int(N), int(M), useBias ? 1 : 0, phase.numLayers(), phase.desc().data(),
+                           phase.x().data(), &h_));
+        check(yq_ap_dims(h_, &dimAmp_, &dimPhase_));
+    }
+    ~AmplitudePhase() { yq_ap_destroy(h_); }
+    AmplitudePhase(const AmplitudePhase&) = delete;
+    AmplitudePhase& operator=(const AmplitudePhase&) = delete;
+    yq_ap handle() const { return h_; }
+    uint32_t getN() const { return n_; }
+    uint32_t getDimAmp() const { return uint32_t(dimAmp_); }
+    uint32_t getDimPhase() const { return uint32_t(dimPhase_); }
+    uint32_t getDim() const { return uint32_t(dimAmp_ + dimPhase_); }
+    // AmplitudePhase.hpp:92-97 (amplitude N(0, sigma^2), phase by mode; Xavier in the reference)
+    void initializeRandom(uint64_t seed, double sigma, InitializationMode mode = InitializationMode::Xavier) {
+        check(yq_ap_init_random(h_, seed, sigma, int(mode)));
+    }
+    RealVector getParams() const {
+        RealVector p(getDim());
+        check(yq_ap_get_params(h_, p.data()));
+        return p;
+    }
+    void setParams(const RealVector& p) {
+        if (p.size() != getDim()) throw std::invalid_argument("setParams: size != getDim()");
+        check(yq_ap_set_params(h_, p.data()));
+    }
+    void updateParams(const RealVector& d) {
+        if (d.size() != getDim()) throw std::invalid_argument("updateParams: size != getDim()");
+        check(yq_ap_update_params(h_, d.data()));
+    }
+};
+
+// Basis/BasisFull.hpp, Basis/BasisJz.hpp
+struct BasisFull {
+    uint32_t n;
+    static constexpr int kind = YQ_BASIS_FULL;
+    int nup() const { return 0; }
+};
+struct BasisJz {
+    uint32_t n, nup_;
+    static constexpr int kind = YQ_BASIS_JZ;
+    BasisJz(uint32_t n_, uint32_t nup) : n(n_), nup_(nup) {}
+    int nup() const { return int(nup_); }
+};
+
+// GroundState/NGDExact.hpp:18-211 (the Hamiltonian's column form is applied on the device)
+class NGDExact {
+    yq_ngd h_ = nullptr;
+    const AmplitudePhase& qs_;
+    double energy_ = 0.;
+
+    std::vector<double> get(int what, size_t count) const {
+        std::vector<double> out(count);
+        check(yq_ngd_get(h_, what, out.data()));
+        return out;
+    }
+
+public:
+    template <class Basis, class Ham>
+    NGDExact(const AmplitudePhase& qs, const Basis& basis, const Ham& ham) : qs_(qs) {
+        check(yq_ngd_create(qs.handle(), ham.handle(), Basis::kind, basis.nup(), &h_));
+    }
+    ~NGDExact() { yq_ngd_destroy(h_); }
+    NGDExact(const NGDExact&) = delete;
+    NGDExact& operator=(const NGDExact&) = delete;
+    yq_ngd handle() const { return h_; }
+    void constructExact() { check(yq_ngd_construct(h_, &energy_)); }
+    double eloc() const { return energy_; }
+    double getEnergy() const { return energy_; }
+    std::vector<double> energyGrad() const { return get(YQ_NGD_GRAD, qs_.getDim()); }
+    std::vector<double> olocAmp() const { return get(YQ_NGD_OLOC_AMP, qs_.getDimAmp()); }
+    std::vector<double> olocPhase() const { return get(YQ_NGD_OLOC_PHASE, qs_.getDimPhase()); }
+    std::vector<double> corrMatAmp() const { return get(YQ_NGD_CORR_AMP, size_t(qs_.getDimAmp()) * qs_.getDimAmp()); }
+    std::vector<double> corrMatPhase() const {
+        return get(YQ_NGD_CORR_PHASE, size_t(qs_.getDimPhase()) * qs_.getDimPhase());
+    }
+};
+
+enum class Mode { AMP = YQ_NGD_AMP, PHASE = YQ_NGD_PHASE, ALL = YQ_NGD_ALL };
+
+// Runners/RunAmplitudePhase.hpp:12-122
+class RunAmplitudePhaseExact {
+    AmplitudePhase qs_;
+    double lambdaIni_ = 1e-3, lambdaDecay_ = 1.0, lambdaMin_ = 1e-4;
+    int maxIter_ = 2000;
+    SGD opt_;
+
+public:
+    RunAmplitudePhaseExact(Context& ctx, uint32_t N, uint32_t alpha, bool useBias, FeedForward&& phase)
+        : qs_(ctx, N, N * alpha, useBias, std::move(phase)) {}
+    AmplitudePhase& getQs() { return qs_; }
+    void initializeRandom(uint64_t seed, double sigma) { qs_.initializeRandom(seed, sigma); }
+    void setLambda(double ini, double decay = 1.0, double mn = 0.0) {
+        lambdaIni_ = ini;
+        lambdaDecay_ = decay;
+        lambdaMin_ = mn;
+    }
+    // saveWfPer: the reference archives the whole machine; not built for AmplitudePhase
+    void setIterParams(int maxIter, int /*saveWfPer*/) { maxIter_ = maxIter; }
+    void setOptimizer(const SGD& opt) { opt_ = opt; }
+
+    // callback(ll, currE, |grad|, |v|) as RunAmplitudePhase.hpp:119
+    template <class Callback, class Basis, class Ham>
+    void run(Callback&& callback, const Basis& basis, const Ham& ham, Mode mode = Mode::ALL) {
+        NGDExact ngd(qs_, basis, ham);
+        for (int ll = 0; ll <= maxIter_; ++ll) {
+            const double lambda = std::max(lambdaIni_ * std::pow(lambdaDecay_, ll), lambdaMin_);
+            double e = 0., gn = 0., vn = 0.;
+            check(yq_ngd_iteration(ngd.handle(), lambda, opt_.eta(), int(mode), &e, &gn, &vn));
+            callback(ll, e, gn, vn);
+        }
+    }
+};
+
 }  // namespace gpu
 }  // namespace yannq

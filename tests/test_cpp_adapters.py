@@ -1,8 +1,9 @@
 """The header-only C++ adapters (include/yannq_gpu/yannq_gpu.hpp): RunRBM-style
 drivers in the reference example's call pattern compile against them (CPU), and
 on a GPU they run and the energy goes down towards the exact ground energy: the
-TFI chain with local moves, and the J1J2 chain with exchange moves (which also
-constructs the XXX, XYZNNN and KitaevHex adapters)."""
+TFI chain with local moves, the J1J2 chain with exchange moves (which also
+constructs the XXX, XYZNNN and KitaevHex adapters), and the AmplitudePhase
+example's RunAmplitudePhaseExact loop."""
 import os
 import subprocess
 
@@ -23,7 +24,7 @@ def _build(tmp_path, name="rbm_tfi_driver"):
     return exe
 
 
-@pytest.mark.parametrize("name", ["rbm_tfi_driver", "j1j2_driver"])
+@pytest.mark.parametrize("name", ["rbm_tfi_driver", "j1j2_driver", "amplitude_phase_driver"])
 def test_adapters_compile(tmp_path, name):
     _build(tmp_path, name)
 
@@ -62,3 +63,17 @@ def test_j1j2_driver_runs(tmp_path, orc):
     e0 = orc.ed_ground(orc.Ham.j1j2(12, 1.0, 0.2, True), 1, 6) / 12
     assert e_last < e_first
     assert e_last >= e0 - 1e-3
+
+
+@pytest.mark.gpu
+def test_amplitude_phase_driver_runs(tmp_path, orc):
+    exe = _build(tmp_path, "amplitude_phase_driver")
+    out = subprocess.run([exe, "60"], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    g = [l for l in out.stdout.splitlines() if l.startswith("GETTERS")][0].split()
+    assert int(g[1]) == (12 * 12) ** 2 and int(g[2]) == 144 + 30 + 120 + 40 + 24
+    last = [l for l in out.stdout.splitlines() if l.startswith("OK")][0].split()
+    e_first, e_last = float(last[1]), float(last[2])
+    e0 = orc.ed_ground(orc.Ham.j1j2(12, 1.0, 0.2, True), 1, 6) / 12
+    assert e_last < e_first
+    assert e_last >= e0 - 1e-9
