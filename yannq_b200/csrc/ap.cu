@@ -82,7 +82,7 @@ struct yq_ngd_s {
     yq::DevBuf part, scal;                       // reductions
     yq::DevBuf grad, oloc;                       // Pa + Pp doubles each
     yq::DevBuf Ca, Cp;                           // c128 dim_pad x dim_pad (lower, real part used)
-    yq::DevBuf La, LaH, Lp, LpH, rhs, sol, chol_work;
+    yq::DevBuf La, LaH, Lp, LpH, Ga, Gp, rhs, chol_work, cpart, va, vp;
     int pad_a = 0, pad_p = 0;
     double energy = 0.;
     bool constructed = false;
@@ -639,9 +639,9 @@ void ngd_construct(yq_ngd_s* g) {
     YQ_LAUNCH_CHECK();
     double* grad = g->grad.as<double>();
     double* oloc = g->oloc.as<double>();
-    DevBuf cpart;
-    packed_colsums(g->Da.as<c128>(), Pa, dim, g->p.as<double>(), g->ya.as<double>(), cpart, oloc, grad, st);
-    packed_colsums(g->Dp.as<c128>(), Pp, dim, g->p.as<double>(), g->yb.as<double>(), cpart, oloc + Pa, grad + Pa, st);
+    packed_colsums(g->Da.as<c128>(), Pa, dim, g->p.as<double>(), g->ya.as<double>(), g->cpart, oloc, grad, st);
+    packed_colsums(g->Dp.as<c128>(), Pp, dim, g->p.as<double>(), g->yb.as<double>(), g->cpart, oloc + Pa, grad + Pa,
+                   st);
     grad_kernel<<<grid_for(Pa, 256, 1u << 20), 256, 0, st>>>(Pa, scal, oloc, grad, 1);
     grad_kernel<<<grid_for(Pp, 256, 1u << 20), 256, 0, st>>>(Pp, scal, oloc + Pa, grad + Pa, 0);
     // centred, sqrt(p)-scaled rows and their real Gram matrices (lower triangles)
@@ -660,11 +660,10 @@ void ngd_construct(yq_ngd_s* g) {
 }
 
 // LLT of (C + lambda I) for one block: solution into g->sol (c128, pad entries)
-void solve_block(yq_ngd_s* g, DevBuf& C, int P, int pad, DevBuf& L, DevBuf& LH, const double* rhs_dev, double lambda,
-                 c128* out) {
+void solve_block(yq_ngd_s* g, DevBuf& C, DevBuf& G, int P, int pad, DevBuf& L, DevBuf& LH, const double* rhs_dev,
+                 double lambda, c128* out) {
     yq_ctx_s* ctx = g->q->ctx;
     cudaStream_t st = ctx->stream;
-    DevBuf G;
     G.ensure(size_t(pad) * pad * sizeof(c128));
     shift_pad_kernel<<<grid_for(size_t(pad) * pad, 256, 148 * 32), 256, 0, st>>>(P, pad, C.as<c128>(), G.as<c128>(),
                                                                                lambda);
@@ -1045,12 +1044,15 @@ int yq_ngd_iteration(yq_ngd g, double lambda, double lr, int mode, double* energ
         YQ_CUDA(cudaStreamSynchronize(st));
         const bool use_a = mode == YQ_NGD_AMP || mode == YQ_NGD_ALL;
         const bool use_p = (mode == YQ_NGD_PHASE || mode == YQ_NGD_ALL) && q->Pp > 0;
-        DevBuf va, vp;
+        DevBuf& va = g->va;
+        DevBuf& vp = g->vp;
         va.ensure(size_t(g->pad_a) * sizeof(c128));
         vp.ensure(size_t(g->pad_p) * sizeof(c128));
-        if (use_a) solve_block(g, g->Ca, int(q->Pa), g->pad_a, g->La, g->LaH, g->grad.as<double>(), lambda, va.as<c128>());
+        if (use_a)
+            solve_block(g, g->Ca, g->Ga, int(q->Pa), g->pad_a, g->La, g->LaH, g->grad.as<double>(), lambda,
+                        va.as<c128>());
         if (use_p)
-            solve_block(g, g->Cp, int(q->Pp), g->pad_p, g->Lp, g->LpH, g->grad.as<double>() + q->Pa, lambda,
+            solve_block(g, g->Cp, g->Gp, int(q->Pp), g->pad_p, g->Lp, g->LpH, g->grad.as<double>() + q->Pa, lambda,
                         vp.as<c128>());
         const int stt = ctx->read_status_and_clear();
         if (stt & DS_TIMEOUT) throw Error(YQ_E_TIMEOUT, "ngd: a bounded device wait gave up");
