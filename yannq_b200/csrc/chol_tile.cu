@@ -129,70 +129,83 @@ __device__ __forceinline__ void warp_mma(const c128* A, int lda, const c128* B, 
 //   chol(A11) -> L11, X11;   L21 = A21 X11^H;   A22 -= L21 L21^H;
 //   chol(A22) -> L22, X22;   X21 = -X22 (L21 X11),
 // with the products on DMMA (m8n8k4, one 8 x 8 output tile per warp at a time)
-// and 8 x 8 leaves factored and inverted by one warp in registers (lane r holds
-// row r; pivots and columns move by shuffles).  Levels of size 16 and below run
+// and 8 x 8 leaves factored and inverted by one warp in registers (two elements
+// per lane; pivots and columns move by shuffles).  Levels of size 16 and below run
 // in warp 0 alone (warp barriers), the levels above use all four warps.  T is
 // scratch.  On exit F holds L in its lower triangle (the caller reads only that)
 // and X holds L^{-1} with zeros above the diagonal.
 
-// Lane r < 8 of warp 0: rows o + r of the 8 x 8 diagonal block.
+// Warp 0: the 8 x 8 diagonal block at o, element-parallel.  Lane l holds row
+// r = l >> 2 and columns q0 = l & 3, q1 = q0 + 4.  Right-looking factorisation:
+// per column one pivot broadcast and three complex shuffles (the column entries of
+// this lane's row and of its two columns), then the rank-1 update of the lane's
+// elements; the inverse by right-looking substitution from the identity (row k
+// is final after its scaling by 1 / L_kk, then rows below subtract L_rk X_k).
 __device__ __forceinline__ void leaf8(c128* F, c128* X, int o, int* status) {
-    const int lane = threadIdx.x & 31, r = lane & 7;
-    c128 v[8];
+    const int lane = threadIdx.x & 31, r = lane >> 2, q0 = lane & 3;
+    const int qq[2] = {q0, q0 + 4};
+    c128 e[2];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = q <= r ? F[(o + r) * FLS + o + q] : mk(0., 0.);
-    double diag = 1.0;
+    for (int h = 0; h < 2; ++h) e[h] = qq[h] <= r ? F[(o + r) * FLS + o + qq[h]] : mk(0., 0.);
+    double sc[8];  // 1 / L_cc
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        double d = __shfl_sync(0xffffffffu, v[c].re, c);
+        const int hc = c >> 2, lc = c & 3;
+        double d = __shfl_sync(0xffffffffu, e[hc].re, 4 * c + lc);
         if (!(d > 0.0)) {
             if (lane == 0) atomicOr(status, DS_NOT_PD);
             d = 1.0;  // unit pivot keeps the launch well defined
         }
-        const double is = rsqrt(d);
-        const c128 lc = r > c ? is * v[c] : mk(0., 0.);  // L_rc
-        if (r == c) {
-            diag = d * is;
-            v[c] = mk(diag, 0.0);
-        } else if (r > c) {
-            v[c] = lc;
+        const double s = rsqrt(d);
+        sc[c] = s;
+        c128 arc, aqc[2];
+        arc.re = __shfl_sync(0xffffffffu, e[hc].re, 4 * r + lc);
+        arc.im = __shfl_sync(0xffffffffu, e[hc].im, 4 * r + lc);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            aqc[h].re = __shfl_sync(0xffffffffu, e[hc].re, 4 * qq[h] + lc);
+            aqc[h].im = __shfl_sync(0xffffffffu, e[hc].im, 4 * qq[h] + lc);
         }
+        const c128 Lrc = s * arc;
 #pragma unroll
-        for (int q = c + 1; q < 8; ++q) {
-            c128 lq;  // L_qc
-            lq.re = __shfl_sync(0xffffffffu, lc.re, q);
-            lq.im = __shfl_sync(0xffffffffu, lc.im, q);
-            if (r >= q) v[q] = v[q] - lc * conj(lq);
-        }
-    }
-    // X row r: X_rr = 1 / L_rr, X_rj = -(1 / L_rr) sum_{j <= k < r} L_rk X_kj
-    const double idg = 1.0 / diag;
-    c128 x[8], acc[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) x[j] = acc[j] = mk(0., 0.);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        if (r == k) {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                if (j < k) x[j] = (-idg) * acc[j];
-                else if (j == k) x[j] = mk(idg, 0.0);
+        for (int h = 0; h < 2; ++h) {
+            const int q = qq[h];
+            if (q == c) {
+                if (r == c) e[h] = mk(d * s, 0.0);
+                else if (r > c) e[h] = Lrc;
+            } else if (q > c && r >= q) {
+                e[h] = e[h] - Lrc * conj(s * aqc[h]);
             }
         }
+    }
+    c128 y[2];
 #pragma unroll
-        for (int j = 0; j <= k; ++j) {
-            c128 xk;  // X_kj
-            xk.re = __shfl_sync(0xffffffffu, x[j].re, k);
-            xk.im = __shfl_sync(0xffffffffu, x[j].im, k);
-            if (r > k) acc[j] = acc[j] + v[k] * xk;
+    for (int h = 0; h < 2; ++h) y[h] = mk(qq[h] == r ? 1.0 : 0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int hk = k >> 2, lk = k & 3;
+        if (r == k) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) y[h] = sc[k] * y[h];
+        }
+        c128 lrk, xk[2];
+        lrk.re = __shfl_sync(0xffffffffu, e[hk].re, 4 * r + lk);
+        lrk.im = __shfl_sync(0xffffffffu, e[hk].im, 4 * r + lk);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            xk[h].re = __shfl_sync(0xffffffffu, y[h].re, 4 * k + q0);
+            xk[h].im = __shfl_sync(0xffffffffu, y[h].im, 4 * k + q0);
+        }
+        if (r > k) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) y[h] = y[h] - lrk * xk[h];
         }
     }
-    if (lane < 8) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            F[(o + r) * FLS + o + q] = v[q];
-            X[(o + r) * FLS + o + q] = x[q];
-        }
+    for (int h = 0; h < 2; ++h) {
+        const bool low = qq[h] <= r;
+        F[(o + r) * FLS + o + qq[h]] = low ? e[h] : mk(0., 0.);
+        X[(o + r) * FLS + o + qq[h]] = low ? y[h] : mk(0., 0.);
     }
 }
 
