@@ -108,6 +108,31 @@ def test_ngd_construct(ctx, orc, name):
     q.close()
 
 
+def test_ngd_construct_split_gram(ctx, orc):
+    """A basis of 2^14 configurations (8,192 row pairs): the correlation matrices
+    are computed in K-chunks on side streams and summed."""
+    from yannq_b200 import api
+
+    n = 14
+    ho = orc.Ham.tfi(n, -1.0, -0.9)
+    hd = api.Hamiltonian.tfi(ctx, n, -1.0, -0.9)
+    layers = [("conv1d", 1, 2, 3, 1, True), ("lncosh",), ("fc", 2 * n, 2, True), ("tanh", 1.0), ("fc", 2, 1, False)]
+    q, o = _pair(api, orc, ctx, n, n, True, layers)
+    q.init_random(29, 0.1, api.INIT_XAVIER)
+    p = q.get_params()
+    ref = orc.ngd_exact(ho, o, p, api.BASIS_FULL, 0)
+    g = api.NGDExact(q, hd, api.BASIS_FULL, 0)
+    for _ in range(2):  # partials are rewritten, not accumulated, on every construct
+        e = g.construct()
+        assert e == pytest.approx(ref["energy"], rel=1e-11)
+        assert _rel(g.get(api.NGD_GRAD), ref["grad"]) < 1e-10
+        assert _rel(g.get(api.NGD_CORR_AMP), ref["corr_amp"]) < 1e-10
+        assert _rel(g.get(api.NGD_CORR_PHASE), ref["corr_phase"]) < 1e-10
+    g.close()
+    hd.close()
+    q.close()
+
+
 def test_ngd_iteration_matches_oracle_step(ctx, orc):
     from yannq_b200 import api
 

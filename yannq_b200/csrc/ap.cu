@@ -86,6 +86,19 @@ struct yq_ngd_s {
     int pad_a = 0, pad_p = 0;
     double energy = 0.;
     bool constructed = false;
+    // K-split of the two Gram matrices: side streams, fork / join events, partials
+    static constexpr int NSIDE = 8;
+    cudaStream_t side[NSIDE] = {};
+    cudaEvent_t fork = nullptr, join[NSIDE] = {};
+    int split_a = 1, split_p = 1;
+    yq::DevBuf Cpart;
+    ~yq_ngd_s() {
+        for (int i = 0; i < NSIDE; ++i) {
+            if (join[i]) cudaEventDestroy(join[i]);
+            if (side[i]) cudaStreamDestroy(side[i]);
+        }
+        if (fork) cudaEventDestroy(fork);
+    }
 };
 
 namespace yq {
@@ -616,6 +629,61 @@ void check_sigma_pm1(const int8_t* s, size_t count) {
         if (s[i] != 1 && s[i] != -1) throw Error(YQ_E_ARG, "sigma entries must be +1 or -1");
 }
 
+// C = sum of the split partials (every element; only the lower triangle is read)
+__global__ void sum_partials_kernel(size_t count, int nparts, const c128* __restrict__ parts, c128* __restrict__ C) {
+    for (size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < count; e += size_t(gridDim.x) * blockDim.x) {
+        c128 acc = parts[e];
+        for (int k = 1; k < nparts; ++k) acc = acc + parts[size_t(k) * count + e];
+        C[e] = acc;
+    }
+}
+
+// The real correlation matrices as the real parts of Z^H Z over the packed rows.
+// One DMMA CTA computes one 64 x 64 tile of the lower triangle over all K = dim2
+// rows, and P of a few hundred to a few thousand gives fewer tiles than the GPU
+// has SMs, so K is split into chunks computed on side streams into partial
+// matrices that are then summed in a fixed order.
+void grams(yq_ngd_s* g, cudaStream_t st) {
+    yq_ap_s* q = g->q;
+    const size_t Pa = q->Pa, Pp = q->Pp;
+    const uint64_t K = g->dim2;
+    if (g->split_a * g->split_p == 1) {
+        gram_fp64<double>(g->Da.as<c128>(), Pa, 1, int(Pa), int(K), g->Ca.as<c128>(), size_t(g->pad_a), 1.0, 0, 0.0, st);
+        if (Pp)
+            gram_fp64<double>(g->Dp.as<c128>(), Pp, 1, int(Pp), int(K), g->Cp.as<c128>(), size_t(g->pad_p), 1.0, 0, 0.0,
+                              st);
+        return;
+    }
+    const size_t na = size_t(g->pad_a) * g->pad_a, np = size_t(g->pad_p) * g->pad_p;
+    c128* pa = g->Cpart.as<c128>();
+    c128* pp = pa + size_t(g->split_a) * na;
+    YQ_CUDA(cudaEventRecord(g->fork, st));
+    int job = 0;
+    auto run = [&](const c128* Z, size_t P, int split, c128* parts, size_t cnt, int pad) {
+        const uint64_t chunk = (K + split - 1) / split;
+        for (int k = 0; k < split; ++k) {
+            const uint64_t k0 = std::min<uint64_t>(K, uint64_t(k) * chunk), kc = std::min<uint64_t>(chunk, K - k0);
+            cudaStream_t ss = g->side[job % yq_ngd_s::NSIDE];
+            if (job < yq_ngd_s::NSIDE) YQ_CUDA(cudaStreamWaitEvent(ss, g->fork, 0));
+            if (kc > 0)
+                gram_fp64<double>(Z + k0 * P, P, 1, int(P), int(kc), parts + size_t(k) * cnt, size_t(pad), 1.0, 0, 0.0,
+                                  ss);
+            else
+                YQ_CUDA(cudaMemsetAsync(parts + size_t(k) * cnt, 0, cnt * sizeof(c128), ss));
+            ++job;
+        }
+    };
+    run(g->Da.as<c128>(), Pa, g->split_a, pa, na, g->pad_a);
+    if (Pp) run(g->Dp.as<c128>(), Pp, g->split_p, pp, np, g->pad_p);
+    for (int i = 0; i < std::min(job, int(yq_ngd_s::NSIDE)); ++i) {
+        YQ_CUDA(cudaEventRecord(g->join[i], g->side[i]));
+        YQ_CUDA(cudaStreamWaitEvent(st, g->join[i], 0));
+    }
+    sum_partials_kernel<<<grid_for(na, 256, 148 * 16), 256, 0, st>>>(na, g->split_a, pa, g->Ca.as<c128>());
+    if (Pp) sum_partials_kernel<<<grid_for(np, 256, 148 * 16), 256, 0, st>>>(np, g->split_p, pp, g->Cp.as<c128>());
+    YQ_LAUNCH_CHECK();
+}
+
 // NGDExact::constructExact on the device
 void ngd_construct(yq_ngd_s* g) {
     yq_ap_s* q = g->q;
@@ -650,10 +718,7 @@ void ngd_construct(yq_ngd_s* g) {
     centre_scale_kernel<<<grid_for(g->dim2 * Pp, 256, 148 * 32), 256, 0, st>>>(Pp, dim, g->p.as<double>(), oloc + Pa,
                                                                              g->Dp.as<c128>());
     YQ_LAUNCH_CHECK();
-    gram_fp64<double>(g->Da.as<c128>(), Pa, 1, int(Pa), int(g->dim2), g->Ca.as<c128>(), size_t(g->pad_a), 1.0, 0, 0.0,
-                      st);
-    gram_fp64<double>(g->Dp.as<c128>(), Pp, 1, int(Pp), int(g->dim2), g->Cp.as<c128>(), size_t(g->pad_p), 1.0, 0, 0.0,
-                      st);
+    grams(g, st);
     YQ_CUDA(cudaMemcpyAsync(&g->energy, scal, sizeof(double), cudaMemcpyDeviceToHost, st));
     YQ_CUDA(cudaStreamSynchronize(st));
     g->constructed = true;
@@ -976,6 +1041,27 @@ int yq_ngd_create(yq_ap q, yq_ham H, int basis_kind, int nup, yq_ngd* out) {
         g->Cp.ensure(size_t(g->pad_p) * g->pad_p * sizeof(c128));
         YQ_CUDA(cudaMemsetAsync(g->Ca.p, 0, size_t(g->pad_a) * g->pad_a * sizeof(c128), st));
         YQ_CUDA(cudaMemsetAsync(g->Cp.p, 0, size_t(g->pad_p) * g->pad_p * sizeof(c128), st));
+        // K-split: enough chunks that both Grams together give about eight tiles per SM
+        // (at most 8 chunks each, and chunks of at least 4096 rows)
+        {
+            const int sms = std::max(1, q->ctx->sm_count);
+            auto tiles = [](size_t P) { const size_t t = (P + 63) / 64; return t * (t + 1) / 2; };
+            const size_t ta = tiles(q->Pa), tp = q->Pp ? tiles(q->Pp) : 0;
+            const size_t want = size_t(8) * sms;
+            const int by_rows = int(std::max<uint64_t>(1, g->dim2 / 4096));
+            const int split = int(std::min<size_t>(8, std::max<size_t>(1, (want + ta + tp - 1) / (ta + tp))));
+            g->split_a = g->split_p = std::min(split, by_rows);
+            if (g->split_a > 1) {
+                YQ_CUDA(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming));
+                for (int i = 0; i < yq_ngd_s::NSIDE; ++i) {
+                    YQ_CUDA(cudaStreamCreateWithFlags(&g->side[i], cudaStreamNonBlocking));
+                    YQ_CUDA(cudaEventCreateWithFlags(&g->join[i], cudaEventDisableTiming));
+                }
+                const size_t cnt = size_t(g->split_a) * g->pad_a * g->pad_a + size_t(g->split_p) * g->pad_p * g->pad_p;
+                g->Cpart.ensure(cnt * sizeof(c128));
+                YQ_CUDA(cudaMemsetAsync(g->Cpart.p, 0, cnt * sizeof(c128), st));
+            }
+        }
         YQ_CUDA(cudaStreamSynchronize(st));
         *out = g.release();
     });
