@@ -36,40 +36,66 @@ __device__ __forceinline__ void split_bf16(float v, uint16_t& hi, uint16_t& lo) 
     lo = __bfloat16_as_ushort(l);
 }
 
-__global__ void split_operands_kernel(const c64* __restrict__ O, int ns, size_t P, size_t rows_pad, size_t kpad,
-                                      uint16_t* __restrict__ xh, uint16_t* __restrict__ xl, uint16_t* __restrict__ yh,
+// Row s of O~ (the O writer's centred value, complex64) and its four planes:
+// k = p holds (Re, Im), k = P + p holds (Im, -Re); rows >= ns and k >= 2P are zero.
+__global__ void o_and_operands_kernel(int n, int m, bool bias, size_t P, int ns, size_t rows_pad, size_t kpad,
+                                      const int8_t* __restrict__ sigma, const c64* __restrict__ t,
+                                      const c128* __restrict__ oloc, c64* __restrict__ O, uint16_t* __restrict__ xh,
+                                      uint16_t* __restrict__ xl, uint16_t* __restrict__ yh,
                                       uint16_t* __restrict__ yl) {
+    const size_t nm = size_t(n) * m;
     for (size_t row = blockIdx.y; row < rows_pad; row += gridDim.y) {
-        for (size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x; k < kpad; k += size_t(gridDim.x) * blockDim.x) {
-            float xv = 0.f, yv = 0.f;
+        const int8_t* sg = sigma + row * n;
+        const c64* ts = t + row * m;
+        const size_t base = row * kpad;
+        for (size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += size_t(gridDim.x) * blockDim.x) {
+            float re = 0.f, im = 0.f;
             if (row < size_t(ns)) {
-                if (k < P) {
-                    c64 o = O[row * P + k];
-                    xv = o.re;
-                    yv = o.im;
-                } else if (k < 2 * P) {
-                    c64 o = O[row * P + (k - P)];
-                    xv = o.im;
-                    yv = -o.re;
+                c64 v;
+                if (p < nm) {
+                    const int i = int(p / m), j = int(p - size_t(i) * m);
+                    const float sv = float(sg[i]);
+                    v = mk(sv * ts[j].re, sv * ts[j].im);
+                } else if (p < nm + n) {
+                    v = mk(float(sg[p - nm]), 0.f);
+                } else {
+                    v = ts[p - nm - n];
                 }
+                const c128 o = oloc[p];
+                re = v.re - float(o.re);
+                im = v.im - float(o.im);
+                O[row * P + p] = mk(re, im);
             }
             uint16_t a, b;
-            const size_t q = row * kpad + k;
-            split_bf16(xv, a, b);
-            xh[q] = a;
-            xl[q] = b;
-            split_bf16(yv, a, b);
-            yh[q] = a;
-            yl[q] = b;
+            split_bf16(re, a, b);
+            xh[base + p] = a;
+            xl[base + p] = b;
+            split_bf16(im, a, b);
+            yh[base + p] = a;
+            yl[base + p] = b;
+            split_bf16(im, a, b);
+            xh[base + P + p] = a;
+            xl[base + P + p] = b;
+            split_bf16(-re, a, b);
+            yh[base + P + p] = a;
+            yl[base + P + p] = b;
+        }
+        for (size_t k = 2 * P + size_t(blockIdx.x) * blockDim.x + threadIdx.x; k < kpad;
+             k += size_t(gridDim.x) * blockDim.x) {
+            xh[base + k] = 0;
+            xl[base + k] = 0;
+            yh[base + k] = 0;
+            yl[base + k] = 0;
         }
     }
 }
 
-void gram_tc_prepare_operands(const c64* O, int ns, size_t P, uint16_t* xh, uint16_t* xl, uint16_t* yh, uint16_t* yl,
-                              cudaStream_t st) {
+void gram_tc_write_o_and_operands(int n, int m, bool bias, size_t P, int ns, const int8_t* sigma, const c64* t,
+                                  const c128* oloc, c64* O, uint16_t* xh, uint16_t* xl, uint16_t* yh, uint16_t* yl,
+                                  cudaStream_t st) {
     const size_t kpad = gram_tc_kpad(P), rows = gram_tc_rows(ns);
-    dim3 g(std::min<unsigned>(64u, cdiv_u(kpad, 256)), unsigned(std::min<size_t>(rows, 65535)));
-    split_operands_kernel<<<g, 256, 0, st>>>(O, ns, P, rows, kpad, xh, xl, yh, yl);
+    dim3 g(std::min<unsigned>(64u, cdiv_u(P, 256)), unsigned(std::min<size_t>(rows, 65535)));
+    o_and_operands_kernel<<<g, 256, 0, st>>>(n, m, bias, P, ns, rows, kpad, sigma, t, oloc, O, xh, xl, yh, yl);
     YQ_LAUNCH_CHECK();
 }
 

@@ -21,10 +21,13 @@ constexpr int TC_BK = 64;   // K per stage: 64 BF16 = one 128-byte swizzle atom 
 inline size_t gram_tc_kpad(size_t P) { return ((2 * P + TC_BK - 1) / TC_BK) * TC_BK; }
 inline size_t gram_tc_rows(int ns) { return ((size_t(ns) + TC_BM - 1) / TC_BM) * TC_BM; }
 
-// Split O~ into the four BF16 planes (rows padded with zeros to gram_tc_rows(ns),
-// K padded with zeros to gram_tc_kpad(P)).
-void gram_tc_prepare_operands(const c64* O, int ns, size_t P, uint16_t* xh, uint16_t* xl, uint16_t* yh, uint16_t* yl,
-                              cudaStream_t st);
+// The centred complex64 rows O~[s, p] = [s_i t_j | s | t] - oloc (row-major, P per
+// row) of the mixed T path and, from the same stored values, the four BF16 planes
+// X = [Re | Im], Y = [Im | -Re] split into hi and lo (rows padded with zeros to
+// gram_tc_rows(ns), K padded with zeros to gram_tc_kpad(P)), in one pass.
+void gram_tc_write_o_and_operands(int n, int m, bool bias, size_t P, int ns, const int8_t* sigma, const c64* t,
+                                  const c128* oloc, c64* O, uint16_t* xh, uint16_t* xl, uint16_t* yh, uint16_t* yl,
+                                  cudaStream_t st);
 
 // G[r, c] (r >= c, r, c < ns) = alpha * T_(r,c) + shift * [r == c], complex FP64, row stride ldg.
 void gram_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int ns, size_t P,

@@ -316,15 +316,22 @@ static void construct_t(yq_sr_s* sr) {
     ctx->stage_end(ST_MEAN);
 
     ctx->stage_begin(ST_O);
-    {
+    bool fused = false;
+    if constexpr (sizeof(R) == 4) {
+        if (sr->precision == YQ_PREC_MIXED && sr->mode == YQ_SR_T) {
+            // centred rows and their BF16 planes in one pass
+            gram_tc_write_o_and_operands(n, m, q->use_bias, P, ns, sigma, sr->tanhs.as<c64>(), sr->oloc.as<c128>(),
+                                         sr->O.as<c64>(), sr->xh.as<uint16_t>(), sr->xl.as<uint16_t>(),
+                                         sr->yh.as<uint16_t>(), sr->yl.as<uint16_t>(), st);
+            fused = true;
+        }
+    }
+    if (!fused) {
         dim3 g(std::max(1u, std::min(64u, cdiv_u(P, 512))), unsigned(std::min(ns, 65535)));
         o_writer_kernel<R><<<g, 256, 0, st>>>(n, m, q->use_bias, P, ns, sigma, sr->tanhs.as<cplx<R>>(),
                                               sr->oloc.as<c128>(), sr->O.as<cplx<R>>());
         YQ_LAUNCH_CHECK();
     }
-    if (sr->precision == YQ_PREC_MIXED && sr->mode == YQ_SR_T)
-        gram_tc_prepare_operands(sr->O.as<c64>(), ns, P, sr->xh.as<uint16_t>(), sr->xl.as<uint16_t>(),
-                                 sr->yh.as<uint16_t>(), sr->yl.as<uint16_t>(), st);
     ctx->stage_end(ST_O);
 
     // F = O~^H (E - <E>) / Ns (SRMat.hpp:101-102; equal to O~^H E / Ns since O~^H 1 = 0)
