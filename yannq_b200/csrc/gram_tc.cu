@@ -43,17 +43,18 @@ __global__ void o_and_operands_kernel(int n, int m, bool bias, size_t P, int ns,
                                       const c128* __restrict__ oloc, c64* __restrict__ O, uint16_t* __restrict__ xh,
                                       uint16_t* __restrict__ xl, uint16_t* __restrict__ yh,
                                       uint16_t* __restrict__ yl) {
-    const size_t nm = size_t(n) * m;
+    // column indices fit 32 bits (P < 2^31, checked by the caller): 32-bit division
+    const unsigned nm = unsigned(n) * unsigned(m), um = unsigned(m), uP = unsigned(P);
     for (size_t row = blockIdx.y; row < rows_pad; row += gridDim.y) {
         const int8_t* sg = sigma + row * n;
         const c64* ts = t + row * m;
         const size_t base = row * kpad;
-        for (size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += size_t(gridDim.x) * blockDim.x) {
+        for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < uP; p += gridDim.x * blockDim.x) {
             float re = 0.f, im = 0.f;
             if (row < size_t(ns)) {
                 c64 v;
                 if (p < nm) {
-                    const int i = int(p / m), j = int(p - size_t(i) * m);
+                    const unsigned i = p / um, j = p - i * um;
                     const float sv = float(sg[i]);
                     v = mk(sv * ts[j].re, sv * ts[j].im);
                 } else if (p < nm + n) {
@@ -93,6 +94,7 @@ __global__ void o_and_operands_kernel(int n, int m, bool bias, size_t P, int ns,
 void gram_tc_write_o_and_operands(int n, int m, bool bias, size_t P, int ns, const int8_t* sigma, const c64* t,
                                   const c128* oloc, c64* O, uint16_t* xh, uint16_t* xl, uint16_t* yh, uint16_t* yl,
                                   cudaStream_t st) {
+    YQ_CHECK_ARG(P < (size_t(1) << 31), "O: more than 2^31 parameters");
     const size_t kpad = gram_tc_kpad(P), rows = gram_tc_rows(ns);
     dim3 g(std::min<unsigned>(64u, cdiv_u(P, 256)), unsigned(std::min<size_t>(rows, 65535)));
     o_and_operands_kernel<<<g, 256, 0, st>>>(n, m, bias, P, ns, rows, kpad, sigma, t, oloc, O, xh, xl, yh, yl);
