@@ -7,6 +7,12 @@ runs the precision workload's machine (12 x 12 TFI, RBM alpha = 2) for
 kernel (sampler, local energy, O writer, tcgen05 Gram, Cholesky) ends quickly
 while its inputs stay larger than L2 (O~ of 2048 x 41,904 complex64 = 0.69 GB,
 BF16 operand planes 1.4 GB).
+
+    python -m yannq_b200.profile_cases --case sampler_scaling
+
+times the complex64 sampler of the same lattice (1024 chains, 8 + 8 local sweeps
+per call, chains kept) at M = 288, 192, 144, 96, 64, 32 hidden units, i.e. 9 down
+to 1 hidden units per lane: device ms of the sample stage, best of three calls.
 """
 import argparse
 import os
@@ -19,7 +25,7 @@ def main():
     from yannq_b200 import api
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default="iteration", choices=["iteration"])
+    ap.add_argument("--case", default="iteration", choices=["iteration", "sampler_scaling"])
     ap.add_argument("--chains", type=int, default=1024)
     ap.add_argument("--sweeps", type=int, default=2)
     ap.add_argument("--discard", type=int, default=8)
@@ -28,6 +34,22 @@ def main():
     a = ap.parse_args()
     ctx = api.Context(0)
     n, m = 144, 288
+    if a.case == "sampler_scaling":
+        for mm in (288, 192, 144, 96, 64, 32):
+            q = api.RBM(ctx, n, mm, True, api.C64)
+            q.init_random(5, 0.01)
+            S = api.Sampler(q, a.chains, api.MOVE_LOCAL)
+            S.sample(8, 8, 1, 0, True)
+            ts = []
+            for e in range(1, 4):
+                S.sample(8, 8, 1, e, False)
+                ts.append(ctx.stage_ms("sample"))
+            print(f"M {mm:4d}  units per lane {(mm + 31) // 32:2d}  sample {min(ts):.3f} ms  "
+                  f"chains per CTA {S.chains_per_cta()}")
+            S.close()
+            q.close()
+        ctx.close()
+        return
     q = api.RBM(ctx, n, m, True, api.C64 if a.precision == "mixed" else api.C128)
     q.init_random(20261203, 0.01)
     H = api.Hamiltonian.tfi2d(ctx, 12, 12, -1.0, -3.0)
