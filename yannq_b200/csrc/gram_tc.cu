@@ -19,7 +19,9 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <cstdlib>
 #include <mutex>
+#include <string>
 
 #include "gram_tc.hpp"
 #include "internal.hpp"
@@ -156,6 +158,11 @@ struct TcParams {
     int accumulate;
     int* status;
     unsigned wait_cap;
+    // K-split of the tiles after the last full wave: CTA index >= full_tiles maps to
+    // tile full_tiles + u / split, K-chunk u % split of kb_chunk stages, whose FP32
+    // partial goes to ws (128 x 256 float2 per chunk) instead of C
+    int full_tiles, split, kb_chunk;
+    float2* ws;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -254,6 +261,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
     // tile of this CTA: 128-row block bi, 256-column block bj <= bi / 2
     int t = blockIdx.x;
+    int s_idx = -1;  // K-chunk of a split tile
+    if (t >= p.full_tiles) {
+        const int u = t - p.full_tiles;
+        t = p.full_tiles + u / p.split;
+        s_idx = u - (u / p.split) * p.split;
+    }
+    const int tile = t;
     int bi = 0;
     while (bi < p.nt && t >= (bi >> 1) + 1) {
         t -= (bi >> 1) + 1;
@@ -282,11 +296,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
     const int total_kb = 3 * p.kb_per_seg;
+    const int kb0 = s_idx < 0 ? 0 : s_idx * p.kb_chunk;
+    const int kb1 = s_idx < 0 ? total_kb : min(total_kb, kb0 + p.kb_chunk);
 
     if (warp == 0) {
         if (lane == 0) {
-            for (int kb = 0; kb < total_kb; ++kb) {
-                const int stage = kb % TC_STAGES, round = kb / TC_STAGES;
+            for (int kb = kb0; kb < kb1; ++kb) {
+                const int stage = (kb - kb0) % TC_STAGES, round = (kb - kb0) / TC_STAGES;
                 if (round > 0 && !mbar_wait(smem_u32(&empty[stage]), uint32_t((round - 1) & 1), abort_flag,
                                             p.wait_cap, p.status))
                     break;
@@ -302,15 +318,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            for (int kb = 0; kb < total_kb; ++kb) {
-                const int stage = kb % TC_STAGES, round = kb / TC_STAGES;
+            for (int kb = kb0; kb < kb1; ++kb) {
+                const int stage = (kb - kb0) % TC_STAGES, round = (kb - kb0) / TC_STAGES;
                 if (!mbar_wait(smem_u32(&full[stage]), uint32_t(round & 1), abort_flag, p.wait_cap, p.status)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t sx = smem_u32(gbase + size_t(stage) * TC_STAGE_BYTES);
                 const uint32_t sy = sx + TC_A_BYTES, sb = sx + 2 * TC_A_BYTES;
 #pragma unroll
                 for (int k = 0; k < TC_BK / 16; ++k) {
-                    const uint32_t acc = (kb | k) != 0 ? 1u : 0u;
+                    const uint32_t acc = ((kb - kb0) | k) != 0 ? 1u : 0u;
                     const uint64_t db = sw128_desc(sb + k * 32);
                     umma_bf16(tmem, sw128_desc(sx + k * 32), db, acc);
                     umma_bf16(tmem + TC_BNW, sw128_desc(sy + k * 32), db, acc);
@@ -354,6 +370,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
             for (int i = 0; i < 32; ++i) stg[lane * SLD + i] = make_float2(__uint_as_float(vr[i]), __uint_as_float(vi[i]));
             __syncwarp();
+            if (s_idx >= 0) {  // partial of a split tile: rows lg * 32 + rr, columns chunk * 32 + lane
+                float2* wt = p.ws + (size_t(tile - p.full_tiles) * p.split + s_idx) * (TC_BM * TC_BNW);
+#pragma unroll 4
+                for (int rr = 0; rr < 32; ++rr) wt[(lg * 32 + rr) * TC_BNW + chunk * 32 + lane] = stg[rr * SLD + lane];
+                __syncwarp();
+                continue;
+            }
             const int c = c0 + lane;
             if (p.accumulate) {
 #pragma unroll
@@ -400,6 +423,32 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
 }
 
+// C (lower part, r < n) of the split tiles: alpha * (sum of the K-chunk partials in
+// chunk order, in FP64) + shift on the diagonal.  blockIdx.y: split tile.
+__global__ void split_reduce_kernel(TcParams p) {
+    int t = p.full_tiles + int(blockIdx.y), bi = 0;
+    while (bi < p.nt && t >= (bi >> 1) + 1) {
+        t -= (bi >> 1) + 1;
+        ++bi;
+    }
+    const int bj = t;
+    const float2* w = p.ws + size_t(blockIdx.y) * p.split * (TC_BM * TC_BNW);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < TC_BM * TC_BNW; e += gridDim.x * blockDim.x) {
+        const int r = bi * TC_BM + e / TC_BNW, c = bj * TC_BNW + e % TC_BNW;
+        if (r >= p.n || c > r) continue;
+        double re = 0.0, im = 0.0;
+        for (int k = 0; k < p.split; ++k) {
+            const float2 v = w[size_t(k) * (TC_BM * TC_BNW) + e];
+            re += double(v.x);
+            im += double(v.y);
+        }
+        re *= p.alpha;
+        im *= p.alpha;
+        if (c == r) re += p.shift;
+        reinterpret_cast<double2*>(p.C + size_t(r) * p.ldc)[c] = make_double2(re, im);
+    }
+}
+
 // ---------------------------------------------------------------------------
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -428,9 +477,42 @@ static CUtensorMap make_map(const uint16_t* base, size_t rows, size_t kpad, uint
     return m;
 }
 
+namespace {
+// Tiles of the lower triangle of an n x n output, and the K-split of the tiles
+// after the last full wave of sm_count CTAs (split <= 1: none).
+struct TcSplit {
+    int tiles, full, split, kb_chunk;
+};
+TcSplit plan_split(int n, size_t kpad, int sm_count) {
+    TcSplit q{};
+    const int nt = int((size_t(n) + TC_BM - 1) / TC_BM);
+    for (int b = 0; b < nt; ++b) q.tiles += (b >> 1) + 1;
+    q.full = q.tiles;
+    q.split = 1;
+    q.kb_chunk = 0;
+    const int W = std::max(1, sm_count);
+    const int R = q.tiles % W;
+    const int total_kb = 3 * int(kpad / TC_BK);
+    if (R == 0) return q;
+    const int want = W / R;
+    if (want < 2 || total_kb < 2 * TC_STAGES) return q;
+    const int chunk = (total_kb + want - 1) / want;
+    q.kb_chunk = chunk;
+    q.split = (total_kb + chunk - 1) / chunk;  // every chunk non-empty
+    q.full = q.tiles - R;
+    return q;
+}
+}  // namespace
+
 void herk_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int n,
                  size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
                  int* d_status, cudaStream_t st) {
+    herk_tc_launch(xh, xl, yh, yl, n, rows_pad, kpad, C, ldc, alpha, shift, accumulate, d_status, 0, nullptr, st);
+}
+
+void herk_tc_launch(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int n,
+                    size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
+                    int* d_status, int sm_count, DevBuf* ws, cudaStream_t st) {
     YQ_CHECK_ARG(n > 0 && kpad % TC_BK == 0 && kpad > 0 && rows_pad % TC_BM == 0 && size_t(n) <= rows_pad,
                  "herk_tc: operand padding");
     YQ_CHECK_ARG(reinterpret_cast<uintptr_t>(xh) % 16 == 0 && reinterpret_cast<uintptr_t>(xl) % 16 == 0 &&
@@ -443,8 +525,18 @@ void herk_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, con
     TcParams p;
     p.n = n;
     p.nt = int((size_t(n) + TC_BM - 1) / TC_BM);
-    int tiles = 0;
-    for (int b = 0; b < p.nt; ++b) tiles += (b >> 1) + 1;
+    TcSplit sp = plan_split(n, kpad, sm_count);
+    if (!ws || accumulate) sp.full = sp.tiles, sp.split = 1;  // the trailing updates keep whole tiles
+    const int tiles = sp.tiles;
+    p.full_tiles = sp.full;
+    p.split = sp.split;
+    p.kb_chunk = sp.kb_chunk;
+    p.ws = nullptr;
+    const int R = tiles - sp.full;
+    if (R > 0) {
+        ws->ensure(size_t(R) * sp.split * TC_BM * TC_BNW * sizeof(float2));
+        p.ws = ws->as<float2>();
+    }
     p.kb_per_seg = int(kpad / TC_BK);
     p.C = C;
     p.ldc = ldc;
@@ -458,13 +550,24 @@ void herk_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, con
         YQ_CUDA(cudaFuncSetAttribute(herk_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TC_SMEM)));
         attr = true;
     }
-    herk_tc_kernel<<<tiles, TC_THREADS, TC_SMEM, st>>>(mXh, mXl, mYh, mYl, mBh, mBl, p);
+    herk_tc_kernel<<<sp.full + R * sp.split, TC_THREADS, TC_SMEM, st>>>(mXh, mXl, mYh, mYl, mBh, mBl, p);
     YQ_LAUNCH_CHECK();
+    if (R > 0) {
+        split_reduce_kernel<<<dim3(32, unsigned(R)), 256, 0, st>>>(p);
+        YQ_LAUNCH_CHECK();
+    }
 }
 
 void gram_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int ns, size_t P,
-                 c128* G, size_t ldg, double alpha, double shift, int* d_status, cudaStream_t st) {
-    herk_tc_run(xh, xl, yh, yl, ns, gram_tc_rows(ns), gram_tc_kpad(P), G, ldg, alpha, shift, false, d_status, st);
+                 c128* G, size_t ldg, double alpha, double shift, int* d_status, int sm_count, DevBuf& ws,
+                 cudaStream_t st) {
+    // YQ_GRAM_SPLIT=0 keeps whole tiles in the last wave as well
+    static const bool split_on = [] {
+        const char* e = std::getenv("YQ_GRAM_SPLIT");
+        return !(e && std::string(e) == "0");
+    }();
+    herk_tc_launch(xh, xl, yh, yl, ns, gram_tc_rows(ns), gram_tc_kpad(P), G, ldg, alpha, shift, false, d_status,
+                   sm_count, split_on ? &ws : nullptr, st);
 }
 
 }  // namespace yq

@@ -30,8 +30,12 @@ void gram_tc_write_o_and_operands(int n, int m, bool bias, size_t P, int ns, con
                                   cudaStream_t st);
 
 // G[r, c] (r >= c, r, c < ns) = alpha * T_(r,c) + shift * [r == c], complex FP64, row stride ldg.
+// The tiles left after the last full wave of sm_count CTAs (one CTA per SM) are
+// split along K into chunks whose FP32 partials go to `ws` (grown as needed, at
+// most sm_count x 256 KiB) and are summed in a fixed order in FP64.
 void gram_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int ns, size_t P,
-                 c128* G, size_t ldg, double alpha, double shift, int* d_status, cudaStream_t st);
+                 c128* G, size_t ldg, double alpha, double shift, int* d_status, int sm_count, DevBuf& ws,
+                 cudaStream_t st);
 
 // General form over planes of `rows_pad` rows (a multiple of 128) and `kpad` BF16
 // columns (a multiple of 64):  for r >= c, r, c < n
@@ -39,6 +43,11 @@ void gram_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, con
 void herk_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int n,
                  size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
                  int* d_status, cudaStream_t st);
+// The same with the K-split of gram_tc_run (writes only: accumulate = false; ws
+// null keeps whole tiles).
+void herk_tc_launch(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int n,
+                    size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
+                    int* d_status, int sm_count, DevBuf* ws, cudaStream_t st);
 
 // Split the complex FP64 block G[r0 .. r0 + n), [c0 .. c0 + w) (row stride ld) into
 // the four planes with K = 2 w; rows n .. rows_pad are written as zeros.

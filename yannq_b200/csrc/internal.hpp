@@ -137,6 +137,7 @@ struct yq_sr_s {
     yq::DevBuf chol_planes;  // BF16 split panels of the mixed-precision Cholesky
     // mixed precision operands (BF16 hi/lo planes of [Re|Im] and [Im|-Re])
     yq::DevBuf xh, xl, yh, yl;
+    yq::DevBuf gram_ws;  // FP32 partials of the Gram's K-split tiles
     double host_stats[8] = {};
 };
 

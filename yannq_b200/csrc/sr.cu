@@ -472,7 +472,8 @@ static void form_matrix_t(yq_sr_s* sr, double shift) {
     if (sr->mode == YQ_SR_T) {
         if (sr->precision == YQ_PREC_MIXED)
             gram_tc_run(sr->xh.as<uint16_t>(), sr->xl.as<uint16_t>(), sr->yh.as<uint16_t>(), sr->yl.as<uint16_t>(),
-                        ns, P, G, size_t(sr->dim_pad), 1.0 / ns, shift, sr->q->ctx->status.as<int>(), st);
+                        ns, P, G, size_t(sr->dim_pad), 1.0 / ns, shift, sr->q->ctx->status.as<int>(),
+                        sr->q->ctx->sm_count, sr->gram_ws, st);
         else
             gram_fp64<R>(sr->O.as<cplx<R>>(), P, 0, ns, int(P), G, size_t(sr->dim_pad), 1.0 / ns, 0, shift, st);
     } else {
