@@ -633,10 +633,15 @@ void chol_factor_tiled(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* 
     launch_tiles(a, nitems, sm_count, st);
 }
 
-size_t chol_panel_planes_bytes(int n) {
+// BF16 planes of one panel, then the K-split partials of the trailing updates'
+// last waves (up to 160 partial tiles of 128 x 256 float2)
+static size_t panel_operand_bytes(int n) {
     const size_t rows = ((size_t(n) + TC_BM - 1) / TC_BM) * TC_BM;
     return 4 * rows * size_t(2 * CHOL_PANEL) * sizeof(uint16_t);
 }
+constexpr size_t TRAIL_SPLIT_BYTES = size_t(160) * 128 * 256 * 8;
+
+size_t chol_panel_planes_bytes(int n) { return panel_operand_bytes(n) + TRAIL_SPLIT_BYTES; }
 
 void chol_factor_panels(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* status, void* scratch,
                         void* planes, int sm_count, cudaStream_t st) {
@@ -645,7 +650,8 @@ void chol_factor_panels(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int*
     Scratch sc(scratch, nt);
     write_items(sc, nt, st);
     YQ_CUDA(cudaMemsetAsync(sc.words, 0, reinterpret_cast<char*>(sc.sflags) - reinterpret_cast<char*>(sc.words), st));
-    const size_t plane_elems = chol_panel_planes_bytes(n) / (4 * sizeof(uint16_t));
+    const size_t plane_elems = panel_operand_bytes(n) / (4 * sizeof(uint16_t));
+    float2* split_ws = reinterpret_cast<float2*>(static_cast<char*>(planes) + panel_operand_bytes(n));
     uint16_t* xh = static_cast<uint16_t*>(planes);
     uint16_t *xl = xh + plane_elems, *yh = xl + plane_elems, *yl = yh + plane_elems;
     int first = 0;  // index of the panel's first tile in the column-major list
@@ -662,8 +668,8 @@ void chol_factor_panels(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int*
         const int r0 = j1 * TB, n2 = n - r0, w = (j1 - j0) * TB;
         const size_t rows_pad = ((size_t(n2) + TC_BM - 1) / TC_BM) * TC_BM;
         herk_tc_split_block(G, ld, r0, j0 * TB, n2, w, rows_pad, xh, xl, yh, yl, st);
-        herk_tc_run(xh, xl, yh, yl, n2, rows_pad, size_t(2 * w), G + size_t(r0) * ld + r0, ld, -1.0, 0.0, true, status,
-                    st);
+        herk_tc_launch(xh, xl, yh, yl, n2, rows_pad, size_t(2 * w), G + size_t(r0) * ld + r0, ld, -1.0, 0.0, true,
+                       status, sm_count, nullptr, tc_split_enabled() ? split_ws : nullptr, TRAIL_SPLIT_BYTES, st);
     }
 }
 

@@ -423,8 +423,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
 }
 
-// C (lower part, r < n) of the split tiles: alpha * (sum of the K-chunk partials in
-// chunk order, in FP64) + shift on the diagonal.  blockIdx.y: split tile.
+// C (lower part, r < n) of the split tiles: [C +] alpha * (sum of the K-chunk
+// partials in chunk order, in FP64) + shift on the diagonal.  blockIdx.y: split tile.
 __global__ void split_reduce_kernel(TcParams p) {
     int t = p.full_tiles + int(blockIdx.y), bi = 0;
     while (bi < p.nt && t >= (bi >> 1) + 1) {
@@ -445,7 +445,13 @@ __global__ void split_reduce_kernel(TcParams p) {
         re *= p.alpha;
         im *= p.alpha;
         if (c == r) re += p.shift;
-        reinterpret_cast<double2*>(p.C + size_t(r) * p.ldc)[c] = make_double2(re, im);
+        double2* out = reinterpret_cast<double2*>(p.C + size_t(r) * p.ldc) + c;
+        if (p.accumulate) {
+            const double2 o = *out;
+            re += o.x;
+            im += o.y;
+        }
+        *out = make_double2(re, im);
     }
 }
 
@@ -475,6 +481,15 @@ static CUtensorMap make_map(const uint16_t* base, size_t rows, size_t kpad, uint
                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw Error(YQ_E_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(int(r)));
     return m;
+}
+
+// YQ_TC_SPLIT=0 keeps whole tiles in the last partial wave (Gram and trailing updates)
+bool tc_split_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("YQ_TC_SPLIT");
+        return !(e && std::string(e) == "0");
+    }();
+    return on;
 }
 
 namespace {
@@ -507,12 +522,14 @@ TcSplit plan_split(int n, size_t kpad, int sm_count) {
 void herk_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int n,
                  size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
                  int* d_status, cudaStream_t st) {
-    herk_tc_launch(xh, xl, yh, yl, n, rows_pad, kpad, C, ldc, alpha, shift, accumulate, d_status, 0, nullptr, st);
+    herk_tc_launch(xh, xl, yh, yl, n, rows_pad, kpad, C, ldc, alpha, shift, accumulate, d_status, 0, nullptr, nullptr,
+                   0, st);
 }
 
 void herk_tc_launch(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int n,
                     size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
-                    int* d_status, int sm_count, DevBuf* ws, cudaStream_t st) {
+                    int* d_status, int sm_count, DevBuf* ws, float2* ws_fixed, size_t ws_fixed_bytes,
+                    cudaStream_t st) {
     YQ_CHECK_ARG(n > 0 && kpad % TC_BK == 0 && kpad > 0 && rows_pad % TC_BM == 0 && size_t(n) <= rows_pad,
                  "herk_tc: operand padding");
     YQ_CHECK_ARG(reinterpret_cast<uintptr_t>(xh) % 16 == 0 && reinterpret_cast<uintptr_t>(xl) % 16 == 0 &&
@@ -526,17 +543,24 @@ void herk_tc_launch(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, 
     p.n = n;
     p.nt = int((size_t(n) + TC_BM - 1) / TC_BM);
     TcSplit sp = plan_split(n, kpad, sm_count);
-    if (!ws || accumulate) sp.full = sp.tiles, sp.split = 1;  // the trailing updates keep whole tiles
+    p.ws = nullptr;
+    if (sp.tiles > sp.full) {
+        const size_t need = size_t(sp.tiles - sp.full) * sp.split * TC_BM * TC_BNW * sizeof(float2);
+        if (ws) {
+            ws->ensure(need);
+            p.ws = ws->as<float2>();
+        } else if (ws_fixed && need <= ws_fixed_bytes) {
+            p.ws = ws_fixed;
+        } else {  // no workspace: whole tiles
+            sp.full = sp.tiles;
+            sp.split = 1;
+        }
+    }
     const int tiles = sp.tiles;
     p.full_tiles = sp.full;
     p.split = sp.split;
     p.kb_chunk = sp.kb_chunk;
-    p.ws = nullptr;
     const int R = tiles - sp.full;
-    if (R > 0) {
-        ws->ensure(size_t(R) * sp.split * TC_BM * TC_BNW * sizeof(float2));
-        p.ws = ws->as<float2>();
-    }
     p.kb_per_seg = int(kpad / TC_BK);
     p.C = C;
     p.ldc = ldc;
@@ -561,13 +585,8 @@ void herk_tc_launch(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, 
 void gram_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int ns, size_t P,
                  c128* G, size_t ldg, double alpha, double shift, int* d_status, int sm_count, DevBuf& ws,
                  cudaStream_t st) {
-    // YQ_GRAM_SPLIT=0 keeps whole tiles in the last wave as well
-    static const bool split_on = [] {
-        const char* e = std::getenv("YQ_GRAM_SPLIT");
-        return !(e && std::string(e) == "0");
-    }();
     herk_tc_launch(xh, xl, yh, yl, ns, gram_tc_rows(ns), gram_tc_kpad(P), G, ldg, alpha, shift, false, d_status,
-                   sm_count, split_on ? &ws : nullptr, st);
+                   sm_count, tc_split_enabled() ? &ws : nullptr, nullptr, 0, st);
 }
 
 }  // namespace yq

@@ -43,11 +43,16 @@ void gram_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, con
 void herk_tc_run(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int n,
                  size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
                  int* d_status, cudaStream_t st);
-// The same with the K-split of gram_tc_run (writes only: accumulate = false; ws
-// null keeps whole tiles).
+// False when YQ_TC_SPLIT=0: the K-splits below then keep whole tiles.
+bool tc_split_enabled();
+
+// The same with the K-split of the tiles after the last full wave of sm_count CTAs:
+// the partials go to `ws` (grown as needed) or, when ws is null, to `ws_fixed` if the
+// split fits in ws_fixed_bytes (at most sm_count x 256 KiB); otherwise whole tiles.
 void herk_tc_launch(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, const uint16_t* yl, int n,
                     size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
-                    int* d_status, int sm_count, DevBuf* ws, cudaStream_t st);
+                    int* d_status, int sm_count, DevBuf* ws, float2* ws_fixed, size_t ws_fixed_bytes,
+                    cudaStream_t st);
 
 // Split the complex FP64 block G[r0 .. r0 + n), [c0 .. c0 + w) (row stride ld) into
 // the four planes with K = 2 w; rows n .. rows_pad are written as zeros.
