@@ -222,7 +222,7 @@ int yq_sampler_get_slots(yq_sampler S, int* slots);
 /* No reference counterpart: chains per CTA (warps per block) that the sampler's
  * autotuner chose for the configuration of the last yq_sample (0 before any).  The
  * choice is timed once per configuration per process (1, 2 or 4); YQ_AUTOTUNE=0
- * in the environment fixes it at 4. */
+ * in the environment fixes it at 4, YQ_CHAINS_PER_CTA=1, 2 or 4 at that value. */
 int yq_sampler_chains_per_cta(yq_sampler S, int* out);
 /* Accepted proposals per chain in the last yq_sample (LocalSweeper::sweep's return). */
 int yq_sampler_get_accepts(yq_sampler S, uint64_t* acc);

@@ -494,12 +494,14 @@ static void launch_w(const SampArgs<R>& A, int warps, cudaStream_t st) {
 
 // Autotuned chains per CTA (warps per block).  On the first call of a
 // configuration (type, move, hidden units per lane, n, m, chains, sweep length) the
-// kernel runs two sweeps from a scratch copy of the chains into scratch outputs at
+// kernel runs four sweeps from a scratch copy of the chains into scratch outputs at
 // 1, 2 and 4 chains per CTA (the kernel's launch bound is 128 threads), timed with
-// CUDA events on the library stream; the
-// fastest is kept for the process.  The chains evolve identically whatever the
-// choice (each warp owns one chain and its own Philox counters).  Calls made while
-// the stream is being captured, and YQ_AUTOTUNE=0, use 4.
+// CUDA events on the library stream after one untimed launch, the candidates taken
+// in turn over three rounds so that a clock still ramping up weighs on all of them
+// alike; the fastest (least of its three times) is kept for the process.  The
+// chains evolve identically whatever the choice (each warp owns one chain and its
+// own Philox counters).  Calls made while the stream is being captured, and
+// YQ_AUTOTUNE=0, use 4; YQ_CHAINS_PER_CTA=1, 2 or 4 fixes the choice.
 constexpr int N_TUNE = 3;
 struct TuneEntry {
     int warps;
@@ -514,6 +516,12 @@ static int tuned_warps(const SampArgs<R>& A, cudaStream_t st) {
         const char* e = std::getenv("YQ_AUTOTUNE");
         return !(e && std::string(e) == "0");
     }();
+    static const int forced = [] {
+        const char* e = std::getenv("YQ_CHAINS_PER_CTA");
+        const int v = e ? std::atoi(e) : 0;
+        return (v == 1 || v == 2 || v == 4) ? v : 0;
+    }();
+    if (forced) return forced;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     YQ_CUDA(cudaStreamIsCapturing(st, &cap));
     const std::vector<long long> key = {static_cast<long long>(sizeof(R)), MOVE, JPL, A.n, A.m, A.n_chains, A.L};
@@ -523,18 +531,22 @@ static int tuned_warps(const SampArgs<R>& A, cudaStream_t st) {
         if (it != g_tune.end()) return it->second.warps;
     }
     if (!enabled || cap != cudaStreamCaptureStatusNone) return 4;
+    // Four sweeps, the last one recorded: the kernel writes recorded sweep sw to
+    // rows (sw - n_discard) * n_chains + chain, so the scratch outputs hold
+    // (n_total - n_discard) x n_chains rows.
+    constexpr int trial_sweeps = 4, trial_recorded = 1;
     DevBuf ch, sg, th, acc;
     ch.ensure(size_t(A.n_chains) * A.n);
-    sg.ensure(size_t(A.n_chains) * A.n);
-    th.ensure(size_t(A.n_chains) * A.m * sizeof(cplx<R>));
+    sg.ensure(size_t(trial_recorded) * A.n_chains * A.n);
+    th.ensure(size_t(trial_recorded) * A.n_chains * A.m * sizeof(cplx<R>));
     acc.ensure(size_t(A.n_chains) * sizeof(unsigned long long));
     SampArgs<R> T = A;
     T.chains = ch.as<int8_t>();
     T.out_sigma = sg.as<int8_t>();
     T.out_theta = th.as<cplx<R>>();
     T.acc = acc.as<unsigned long long>();
-    T.n_total = 2;
-    T.n_discard = 1;
+    T.n_total = trial_sweeps;
+    T.n_discard = trial_sweeps - trial_recorded;
     T.epoch_dev = nullptr;
     T.theta_in = nullptr;  // nothing of the real chain state is read or written
     T.theta_out = nullptr;
@@ -547,23 +559,24 @@ static int tuned_warps(const SampArgs<R>& A, cudaStream_t st) {
     cudaEvent_t e0, e1;
     YQ_CUDA(cudaEventCreate(&e0));
     YQ_CUDA(cudaEventCreate(&e1));
-    TuneEntry best{4, {0.f, 0.f, 0.f}};
-    float best_ms = 1e30f;
     const int cand[N_TUNE] = {1, 2, 4};
-    for (int c = 0; c < N_TUNE; ++c) {
-        float ms = 1e30f;
-        for (int rep = 0; rep < 2; ++rep) {  // the first run also warms the caches
+    TuneEntry best{4, {1e30f, 1e30f, 1e30f}};
+    launch_w<R, MOVE, JPL>(T, cand[0], st);  // untimed: caches and clocks
+    for (int round = 0; round < 3; ++round) {
+        for (int c = 0; c < N_TUNE; ++c) {
             YQ_CUDA(cudaEventRecord(e0, st));
             launch_w<R, MOVE, JPL>(T, cand[c], st);
             YQ_CUDA(cudaEventRecord(e1, st));
             YQ_CUDA(cudaEventSynchronize(e1));
             float t = 0.f;
             YQ_CUDA(cudaEventElapsedTime(&t, e0, e1));
-            ms = std::min(ms, t);
+            best.ms[c] = std::min(best.ms[c], t);
         }
-        best.ms[c] = ms;
-        if (ms < best_ms) {
-            best_ms = ms;
+    }
+    float best_ms = 1e30f;
+    for (int c = 0; c < N_TUNE; ++c) {
+        if (best.ms[c] < best_ms) {
+            best_ms = best.ms[c];
             best.warps = cand[c];
         }
     }
