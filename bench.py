@@ -488,7 +488,7 @@ def main():
                 "peak_source": src + (" (sustained)" if peaks.get("bf16_tflops_sustained") else ""),
                 "traffic": GRAM_TRAFFIC_BYTES if (Ns, P) == (8192, 41904) else None,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one Ns = 8192 Gram launch "
-                                  "(profiles/herk_tc_kernel_gram_tfi2d12x12_ns8192.md)"}
+                                  "(profiles/herk_tc_kernel_gram_tfi2d12x12.md)"}
     else:
         flops = 4.0 * Ns * Ns * P
         t_ms = head["stages_ms"]["gram"]

@@ -494,11 +494,11 @@ static void launch_w(const SampArgs<R>& A, int warps, cudaStream_t st) {
 
 // Autotuned chains per CTA (warps per block).  On the first call of a
 // configuration (type, move, hidden units per lane, n, m, chains, sweep length) the
-// kernel runs four sweeps from a scratch copy of the chains into scratch outputs at
+// kernel runs two sweeps from a scratch copy of the chains into scratch outputs at
 // 1, 2 and 4 chains per CTA (the kernel's launch bound is 128 threads), timed with
 // CUDA events on the library stream after one untimed launch, the candidates taken
-// in turn over three rounds so that a clock still ramping up weighs on all of them
-// alike; the fastest (least of its three times) is kept for the process.  The
+// in turn over two rounds so that a clock still ramping up weighs on all of them
+// alike; the fastest (least of its two times) is kept for the process.  The
 // chains evolve identically whatever the choice (each warp owns one chain and its
 // own Philox counters).  Calls made while the stream is being captured, and
 // YQ_AUTOTUNE=0, use 4; YQ_CHAINS_PER_CTA=1, 2 or 4 fixes the choice.
@@ -531,10 +531,10 @@ static int tuned_warps(const SampArgs<R>& A, cudaStream_t st) {
         if (it != g_tune.end()) return it->second.warps;
     }
     if (!enabled || cap != cudaStreamCaptureStatusNone) return 4;
-    // Four sweeps, the last one recorded: the kernel writes recorded sweep sw to
+    // Two sweeps, the last one recorded: the kernel writes recorded sweep sw to
     // rows (sw - n_discard) * n_chains + chain, so the scratch outputs hold
     // (n_total - n_discard) x n_chains rows.
-    constexpr int trial_sweeps = 4, trial_recorded = 1;
+    constexpr int trial_sweeps = 2, trial_recorded = 1, rounds = 2;
     DevBuf ch, sg, th, acc;
     ch.ensure(size_t(A.n_chains) * A.n);
     sg.ensure(size_t(trial_recorded) * A.n_chains * A.n);
@@ -562,7 +562,7 @@ static int tuned_warps(const SampArgs<R>& A, cudaStream_t st) {
     const int cand[N_TUNE] = {1, 2, 4};
     TuneEntry best{4, {1e30f, 1e30f, 1e30f}};
     launch_w<R, MOVE, JPL>(T, cand[0], st);  // untimed: caches and clocks
-    for (int round = 0; round < 3; ++round) {
+    for (int round = 0; round < rounds; ++round) {
         for (int c = 0; c < N_TUNE; ++c) {
             YQ_CUDA(cudaEventRecord(e0, st));
             launch_w<R, MOVE, JPL>(T, cand[c], st);
