@@ -231,6 +231,47 @@ def test_sampler_autotuned_launch_shape(ctx, orc):
     assert np.array_equal(out[0][1], out[1][1])
 
 
+_SHAPE_SCRIPT = r"""
+import hashlib, sys
+sys.path.insert(0, sys.argv[1])
+from yannq_b200 import api
+ctx = api.Context(0)
+h = hashlib.sha256()
+for dtype, move, nup, m in ((api.C64, 0, -1, 40), (api.C128, 1, 8, 20), (api.C64, 0, -1, 288)):
+    q = api.RBM(ctx, 16, m, True, dtype)
+    q.init_random(11, 0.1)
+    S = api.Sampler(q, 96, move, nup)
+    S.sample(3, 2, seed=5, epoch=0, reinit=True)
+    S.sample(3, 2, seed=5, epoch=1, reinit=False)
+    s, th = S.get_samples()
+    h.update(s.tobytes()); h.update(th.tobytes()); h.update(S.get_accepts().tobytes())
+    print("shape", S.chains_per_cta(), file=sys.stderr)
+    S.close(); q.close()
+ctx.close()
+print(h.hexdigest())
+"""
+
+
+def test_sampler_launch_shapes_give_identical_chains():
+    """YQ_CHAINS_PER_CTA = 1, 2 and 4 (read once per process, so one process each)
+    give bit-identical samples, theta and acceptance counts: each warp owns one chain
+    and its own Philox counters, whatever the block it runs in."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    digests = {}
+    for v in ("1", "2", "4"):
+        env = dict(os.environ, YQ_CHAINS_PER_CTA=v)
+        out = subprocess.run([sys.executable, "-c", _SHAPE_SCRIPT, root], env=env, capture_output=True, text=True,
+                             timeout=300)
+        assert out.returncode == 0, out.stderr
+        assert out.stderr.count(f"shape {v}") == 3, out.stderr
+        digests[v] = out.stdout.strip()
+    assert digests["1"] == digests["2"] == digests["4"], digests
+
+
 @pytest.mark.parametrize("move,nup,ntemps", [(0, -1, 4), (1, 5, 2), (0, -1, 8)])
 def test_tempering_fp64_matches_oracle_draw_for_draw(ctx, orc, move, nup, ntemps):
     """SamplerMT with nTmps > 1: every chain sweeps at its beta, temperatures swap
