@@ -181,8 +181,10 @@ __global__ void ohy_partial_kernel(size_t P, int ns, int chunk, const cplx<R>* _
 }
 
 // The same for complex64 O~ with an even P: two columns per thread, one 16-byte
-// load per row (eight rows in flight).
-__global__ void ohy_pair_kernel(size_t P, int ns, int chunk, const c64* __restrict__ O, const c128* __restrict__ yv,
+// load per row (eight rows in flight).  At most 40 registers, so that twelve
+// 128-thread blocks share an SM.
+constexpr int OHY_BLOCKS_PER_SM = 12;
+__global__ void __launch_bounds__(128, OHY_BLOCKS_PER_SM) ohy_pair_kernel(size_t P, int ns, int chunk, const c64* __restrict__ O, const c128* __restrict__ yv,
                                 c128* __restrict__ part) {
     const size_t p2 = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const int split = blockIdx.y;
@@ -218,13 +220,23 @@ __global__ void ohy_pair_kernel(size_t P, int ns, int chunk, const c64* __restri
 }
 
 // part[split][p] = sum over the split's sample chunk of conj(O~[s, p]) y_s; returns
-// the number of splits (at most 64; part holds 64 P entries).
+// the number of splits (at most 64; part holds 64 P entries).  The complex64 pair
+// kernel's blocks all do the same work, so its split count fills whole waves: as
+// many as fit in four waves of the resident blocks (a partial last wave cost ~20 %
+// at Ns = 8192, P = 41,904).
 template <typename R>
-static int launch_ohy(size_t P, int ns, const cplx<R>* O, const c128* y, c128* part, cudaStream_t st) {
+static int launch_ohy(size_t P, int ns, const cplx<R>* O, const c128* y, c128* part, int sm_count,
+                      cudaStream_t st) {
     if constexpr (sizeof(R) == 4) {
         if (P % 2 == 0) {
+            static const int per_sm = [] {
+                int b = 0;
+                YQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, ohy_pair_kernel, 128, 0));
+                return std::max(1, b);
+            }();
             const unsigned gx = cdiv_u(P / 2, 128);
-            const int nsplit = std::max(1, std::min(std::min(64, ns), int(32 * 148 / gx)));
+            const long long slots = 4LL * per_sm * sm_count;
+            const int nsplit = int(std::max(1LL, std::min<long long>(std::min(64, ns), slots / gx)));
             const int chunk = (ns + nsplit - 1) / nsplit;
             ohy_pair_kernel<<<dim3(gx, nsplit), 128, 0, st>>>(P, ns, chunk, O, y, part);
             YQ_LAUNCH_CHECK();
@@ -408,7 +420,8 @@ static void construct_t(yq_sr_s* sr) {
                                                           sr->y.as<c128>());
     YQ_LAUNCH_CHECK();
     {
-        const int nsplit = launch_ohy<R>(P, ns, sr->O.as<cplx<R>>(), sr->y.as<c128>(), sr->part.as<c128>(), st);
+        const int nsplit = launch_ohy<R>(P, ns, sr->O.as<cplx<R>>(), sr->y.as<c128>(), sr->part.as<c128>(),
+                                         sr->q->ctx->sm_count, st);
         reduce_parts_kernel<<<cdiv_u(P, 256), 256, 0, st>>>(P, nsplit, 1.0, sr->part.as<c128>(), nullptr, 0.0,
                                                             sr->grad.as<c128>());
         YQ_LAUNCH_CHECK();
@@ -503,7 +516,7 @@ static void op_ohy(yq_sr_s* sr, const c128* x, double alpha, c128* out, const c1
     cudaStream_t st = sr->q->ctx->stream;
     const size_t P = sr->q->P;
     const int ns = sr->ns;
-    const int nsplit = launch_ohy<R>(P, ns, sr->O.as<cplx<R>>(), x, sr->part.as<c128>(), st);
+    const int nsplit = launch_ohy<R>(P, ns, sr->O.as<cplx<R>>(), x, sr->part.as<c128>(), sr->q->ctx->sm_count, st);
     reduce_parts_kernel<<<cdiv_u(P, 256), 256, 0, st>>>(P, nsplit, alpha, sr->part.as<c128>(), addv, beta, out);
     YQ_LAUNCH_CHECK();
 }
