@@ -454,7 +454,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        v, cores, sample = cpu_sample(steps=args.steps, warmup=min(warmup, 1))
+        v, cores, sample = cpu_sample(steps=args.steps, warmup=warmup)
         print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": 0,
                           "steps": args.steps, "warmup": warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
                           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
