@@ -264,6 +264,71 @@ __global__ void reduce_parts_kernel(size_t P, int nsplit, double alpha, const c1
 
 // out_s = alpha * sum_p O~[s, p] x_p  (one block streams one sample row; four
 // loads of the row in flight per thread)
+// The same for complex64 O~ with an even P: two rows per block, so that each pair
+// of FP64 x entries read from L2 serves both, and two columns per 16-byte load
+// (two loads per row in flight).  The row index is clamped for the second row of
+// an odd last block, whose result is not written.
+__global__ void __launch_bounds__(256) ox_pair_kernel(size_t P, int ns, const float4* __restrict__ O4,
+                                                      const c128* __restrict__ x, double alpha,
+                                                      c128* __restrict__ out) {
+    constexpr int RB = 2, U = 2;
+    __shared__ c128 red[RB][8];
+    const int s0 = blockIdx.x * RB;
+    const size_t P2 = P / 2;
+    const float4* rows[RB];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) rows[r] = O4 + size_t(min(s0 + r, ns - 1)) * P2;
+    double ar[RB], ai[RB];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) ar[r] = ai[r] = 0.;
+    const size_t step = blockDim.x;
+    size_t q = threadIdx.x;
+    for (; q + (U - 1) * step < P2; q += U * step) {
+        float4 o[U][RB];
+        c128 x0[U], x1[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            x0[u] = x[2 * (q + u * step)];
+            x1[u] = x[2 * (q + u * step) + 1];
+#pragma unroll
+            for (int r = 0; r < RB; ++r) o[u][r] = rows[r][q + u * step];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int r = 0; r < RB; ++r) {
+                ar[r] += double(o[u][r].x) * x0[u].re - double(o[u][r].y) * x0[u].im + double(o[u][r].z) * x1[u].re -
+                         double(o[u][r].w) * x1[u].im;
+                ai[r] += double(o[u][r].x) * x0[u].im + double(o[u][r].y) * x0[u].re + double(o[u][r].z) * x1[u].im +
+                         double(o[u][r].w) * x1[u].re;
+            }
+    }
+    for (; q < P2; q += step) {
+        const c128 a = x[2 * q], b = x[2 * q + 1];
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            const float4 o = rows[r][q];
+            ar[r] += double(o.x) * a.re - double(o.y) * a.im + double(o.z) * b.re - double(o.w) * b.im;
+            ai[r] += double(o.x) * a.im + double(o.y) * a.re + double(o.z) * b.im + double(o.w) * b.re;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ar[r] += __shfl_xor_sync(0xffffffffu, ar[r], o);
+            ai[r] += __shfl_xor_sync(0xffffffffu, ai[r], o);
+        }
+        if ((threadIdx.x & 31) == 0) red[r][threadIdx.x >> 5] = mk(ar[r], ai[r]);
+    }
+    __syncthreads();
+    if (threadIdx.x < RB && s0 + int(threadIdx.x) < ns) {
+        c128 t = red[threadIdx.x][0];
+        for (int w = 1; w < int(blockDim.x >> 5); ++w) t = t + red[threadIdx.x][w];
+        out[s0 + threadIdx.x] = alpha * t;
+    }
+}
+
 template <typename R>
 __global__ void ox_kernel(size_t P, int ns, const cplx<R>* __restrict__ O, const c128* __restrict__ x, double alpha,
                           c128* __restrict__ out) {
@@ -522,6 +587,14 @@ static void op_ohy(yq_sr_s* sr, const c128* x, double alpha, c128* out, const c1
 }
 template <typename R>
 static void op_ox(yq_sr_s* sr, const c128* x, double alpha, c128* out) {
+    if constexpr (sizeof(R) == 4) {
+        if (sr->q->P % 2 == 0) {
+            ox_pair_kernel<<<cdiv_u(size_t(sr->ns), 2), 256, 0, sr->q->ctx->stream>>>(
+                sr->q->P, sr->ns, reinterpret_cast<const float4*>(sr->O.as<cplx<R>>()), x, alpha, out);
+            YQ_LAUNCH_CHECK();
+            return;
+        }
+    }
     ox_kernel<R><<<sr->ns, 256, 0, sr->q->ctx->stream>>>(sr->q->P, sr->ns, sr->O.as<cplx<R>>(), x, alpha, out);
     YQ_LAUNCH_CHECK();
 }
