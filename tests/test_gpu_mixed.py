@@ -43,7 +43,10 @@ def _t_ref(orc, n, m, p, s, th):
     return Oc @ Oc.conj().T / len(s)
 
 
-@pytest.mark.parametrize("n,m,chains,sweeps", [(8, 16, 16, 8), (16, 32, 64, 8), (12, 48, 40, 7)])
+# P = nm + n + m: 152, 560, 636 and 90 (even, not a multiple of 4) take the
+# two-column O writer, 175 (odd) the one-column writer.
+@pytest.mark.parametrize("n,m,chains,sweeps", [(8, 16, 16, 8), (16, 32, 64, 8), (12, 48, 40, 7), (10, 15, 24, 5),
+                                               (6, 12, 20, 6)])
 def test_tensor_core_gram(ctx, orc, n, m, chains, sweeps):
     from yannq_b200 import api
 
@@ -57,11 +60,13 @@ def test_tensor_core_gram(ctx, orc, n, m, chains, sweeps):
         x.close()
 
 
-def test_mixed_solve_matches_fp64(ctx, orc):
+# Ns < P: T-form.  P = 560 takes the pair kernels of O~^H y and O~ x, P = 175 the
+# one-column kernels.
+@pytest.mark.parametrize("n,m,chains", [(16, 32, 32), (10, 15, 12)])
+def test_mixed_solve_matches_fp64(ctx, orc, n, m, chains):
     from yannq_b200 import api
 
-    n, m = 16, 32
-    p, s, th, q, H, S, sr = _case(api, ctx, orc, n, m, 32, 8)  # Ns = 256 < P = 560
+    p, s, th, q, H, S, sr = _case(api, ctx, orc, n, m, chains, 8)
     ref = orc.sr_step(orc.Ham.tfi(n, -1.0, -1.0), m, p, s, th, 1e-3, orc.SR_T, orc.SOLVE_LLT)
     v, _, _ = sr.solve(1e-3, api.SOLVE_LLT)
     err = np.max(np.abs(v - ref["v"])) / np.max(np.abs(ref["v"]))
