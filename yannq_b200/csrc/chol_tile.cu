@@ -456,6 +456,22 @@ __device__ __forceinline__ void stage_tile(c128* dst, const c128* src, size_t ld
     }
 }
 
+// sum_{c < 32} op(A[c sa]) x[c] with four independent partial sums: each link of a
+// sweep's chain runs two of these, and one running sum would be a chain of 64
+// dependent FP64 FMAs.
+template <bool CONJ>
+__device__ __forceinline__ c128 dot32(const c128* A, int sa, const c128* x) {
+    c128 p[4] = {mk(0., 0.), mk(0., 0.), mk(0., 0.), mk(0., 0.)};
+#pragma unroll
+    for (int c = 0; c < 32; c += 4)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const c128 a = A[(c + u) * sa];
+            p[u] = p[u] + (CONJ ? conj(a) : a) * x[c + u];
+        }
+    return (p[0] + p[1]) + (p[2] + p[3]);
+}
+
 // Forward: x_r = L_rr^{-1} (b_r - sum_{k<r} L_rk x_k), block rows in increasing order.
 __global__ void __launch_bounds__(128, 1) chol_fwd_tile_kernel(SolveArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
@@ -483,9 +499,7 @@ __global__ void __launch_bounds__(128, 1) chol_fwd_tile_kernel(SolveArgs a) {
             cpa_wait_one();  // tile k (and everything before it) has landed
             __syncthreads();
             const c128* T = buf + (k & 1) * TB * SLD + row * SLD + half * 32;
-            c128 v = mk(0., 0.);
-#pragma unroll 8
-            for (int c = 0; c < 32; ++c) v = v + T[c] * xk[half * 32 + c];
+            c128 v = dot32<false>(T, 1, xk + half * 32);
             v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
             v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
             __syncthreads();
@@ -494,9 +508,7 @@ __global__ void __launch_bounds__(128, 1) chol_fwd_tile_kernel(SolveArgs a) {
         cpa_wait_all();
         __syncthreads();
         if (!ok) return;
-        c128 v = mk(0., 0.);
-#pragma unroll 8
-        for (int c = 0; c < 32; ++c) v = v + Li[row * SLD + half * 32 + c] * acc[half * 32 + c];
+        c128 v = dot32<false>(Li + row * SLD + half * 32, 1, acc + half * 32);
         v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
         v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
         if (half == 0) a.b[r * TB + row] = v;
@@ -533,12 +545,7 @@ __global__ void __launch_bounds__(128, 1) chol_bwd_tile_kernel(SolveArgs a) {
             __syncthreads();
             // acc[col] -= sum_row conj(L[k*64 + row][r*64 + col]) z_k[row]
             const c128* T = buf + (i & 1) * TB * SLD + col;
-            c128 v = mk(0., 0.);
-#pragma unroll 8
-            for (int q = 0; q < 32; ++q) {
-                const int rr = half * 32 + q;
-                v = v + conj(T[rr * SLD]) * zk[rr];
-            }
+            c128 v = dot32<true>(T + half * 32 * SLD, SLD, zk + half * 32);
             v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
             v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
             __syncthreads();
@@ -548,9 +555,7 @@ __global__ void __launch_bounds__(128, 1) chol_bwd_tile_kernel(SolveArgs a) {
         __syncthreads();
         if (!ok) return;
         const int rowo = col;
-        c128 v = mk(0., 0.);
-#pragma unroll 8
-        for (int c = 0; c < 32; ++c) v = v + Li[rowo * SLD + half * 32 + c] * acc[half * 32 + c];
+        c128 v = dot32<false>(Li + rowo * SLD + half * 32, 1, acc + half * 32);
         v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
         v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
         if (half == 0) a.b[r * TB + rowo] = v;
