@@ -30,10 +30,10 @@ LX, LY, ALPHA, J, H = 12, 12, 2, -1.0, -3.0
 CHAINS, SWEEPS, DISCARD, THERM, SHIFT, LR, SEED = 1024, 8, 8, 64, 1e-3, 0.01, 20261203
 
 
-def _problem(api, ctx, prec):
+def _problem(api, ctx, prec, seed):
     n = LX * LY
     q = api.RBM(ctx, n, ALPHA * n, True, api.C64 if prec == "mixed" else api.C128)
-    q.init_random(SEED, 0.01)
+    q.init_random(seed, 0.01)
     H_ = api.Hamiltonian.tfi2d(ctx, LX, LY, J, H)
     S = api.Sampler(q, CHAINS, api.MOVE_LOCAL)
     sr = api.SR(q, H_, S, api.SR_T, api.PREC_MIXED if prec == "mixed" else api.PREC_FP64)
@@ -73,22 +73,23 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--iters", type=int, default=300)
     ap.add_argument("--every", type=int, default=50)
+    ap.add_argument("--seed", type=int, default=SEED, help="parameter and Philox seed of both runs")
     a = ap.parse_args()
     ctx = api.Context(0)
     n = LX * LY
     runs = {}
     checks = []
     for prec in ("mixed", "fp64"):
-        q, H_, S, sr = _problem(api, ctx, prec)
+        q, H_, S, sr = _problem(api, ctx, prec, a.seed)
         ir = 2 if prec == "mixed" else 0
         e = []
         for it in range(a.iters):
             first = it == 0
-            r = sr.iteration(SWEEPS, THERM + DISCARD if first else DISCARD, SEED, it, SHIFT, LR, reinit=first,
+            r = sr.iteration(SWEEPS, THERM + DISCARD if first else DISCARD, a.seed, it, SHIFT, LR, reinit=first,
                              ir_steps=ir)
             e.append(r.energy / n)
             if prec == "mixed" and a.every and (it + 1) % a.every == 0:
-                S.sample(SWEEPS, DISCARD, SEED + 1, 1_000_000 + it, False)
+                S.sample(SWEEPS, DISCARD, a.seed + 1, 1_000_000 + it, False)
                 checks.append(dict(iteration=it + 1, **_same_samples(api, ctx, q, S, sr)))
         tail = np.array(e[-max(1, a.iters // 4):])
         runs[prec] = {"E_per_site": e, "tail_mean": float(tail.mean()),
@@ -98,7 +99,7 @@ def main():
     ctx.close()
     d = abs(runs["mixed"]["tail_mean"] - runs["fp64"]["tail_mean"])
     sem = float(np.hypot(runs["mixed"]["tail_sem"], runs["fp64"]["tail_sem"]))
-    print(json.dumps({"workload": "tfi2d_12x12_rbm_alpha2", "iterations": a.iters, "runs": runs,
+    print(json.dumps({"workload": "tfi2d_12x12_rbm_alpha2", "seed": a.seed, "iterations": a.iters, "runs": runs,
                       "tail_dE_per_site": d, "tail_combined_sem": sem, "same_sample_checks": checks}))
 
 
