@@ -61,6 +61,9 @@ const char* yq_version(void);
 /* Number of kernels this library has launched in the process so far (no
  * reference counterpart; used to report launches per VMC step). */
 int yq_launch_count(uint64_t* out);
+/* Number of device allocations (cudaMalloc calls) this library has made in the
+ * process so far (no reference counterpart; shows which calls allocate). */
+int yq_alloc_count(uint64_t* out);
 /* Page-locked host buffers for the host<->device copies of parameters and
  * samples (no reference counterpart: the reference is host-only). */
 int yq_host_alloc(size_t bytes, void** out);
@@ -126,6 +129,15 @@ int yq_rbm_log_psi(yq_rbm q, int ns, const int8_t* sigma, double* out);
  * log psi(sigma') - log psi(sigma) (defined modulo 2 pi i). */
 int yq_rbm_log_ratio(yq_rbm q, int ns, const int8_t* sigma, const double* theta, int nflip, const int* flips,
                      double* out);
+/* logRatio(const std::vector<int>&) -- States/RBMState.hpp:107-125: k distinct sites
+ * flips[s*k .. s*k+k) of each sample flipped together, in the reference's logCosh
+ * form (FP64 from the machine's weights); out: ns complex (modulo 2 pi i). */
+int yq_rbm_log_ratio_k(yq_rbm q, int ns, const int8_t* sigma, const double* theta, int k, const int* flips,
+                       double* out);
+/* logRatio(const RBMStateObj& other) -- States/RBMState.hpp:136-149: log psi of
+ * (sigma_other, theta_other) minus log psi of (sigma, theta), per sample; ns complex. */
+int yq_rbm_log_ratio_states(yq_rbm q, int ns, const int8_t* sigma, const double* theta, const int8_t* sigma_other,
+                            const double* theta_other, double* out);
 /* logDeriv over a batch -- Machines/RBM.hpp:390-406 / constructDelta
  * (GroundState/utils.hpp:12-51): out ns x getDim() complex, row per sample. */
 int yq_rbm_log_deriv(yq_rbm q, int ns, const int8_t* sigma, const double* theta, double* out);
@@ -141,9 +153,9 @@ int yq_rbm_log_deriv(yq_rbm q, int ns, const int8_t* sigma, const double* theta,
  * Allocates nothing: its partial sums live in a fixed 4 MiB array compiled into
  * the library (held by every GPU that loads it), so it rejects machines with
  * (n + 1) (m + 1) > 262144.  Every call shares that array: calls that overlap on
- * the GPU race and must be serialised by the caller.  The first call on a device
- * looks up the array's device address; make that first call before any stream
- * capture. */
+ * the GPU race and must be serialised by the caller.  The first call on a context
+ * looks up the array's device address (with the context's device current) and
+ * keeps it with the context; make that first call before any stream capture. */
 int yq_rbm_oloc_noalloc(yq_rbm q, int ns, const int8_t* d_sigma, const void* d_theta, double* d_oloc);
 
 /* ---- Hamiltonians (Hamiltonians/TFIsing.hpp, XXZ.hpp, XXX.hpp, J1J2.hpp, ------
@@ -236,6 +248,15 @@ int yq_sampler_put_samples(yq_sampler S, int ns, const int8_t* sigma, const doub
  * (optional, ns entries) receives the drawn basis positions. */
 int yq_sampler_sample_exact(yq_sampler S, int ns, uint64_t seed, uint32_t epoch, uint64_t* positions);
 
+/* Failure injection for the bounded device waits (no reference counterpart; for
+ * tests): runs the persistent tile Cholesky (which = 0) or the forward triangular
+ * solve (which = 1) on a 256 x 256 problem whose first work item is never
+ * claimed, so the flag it would publish is never set, with every wait limited to
+ * `cap` polls.  The first wait to run out records the timeout and raises the
+ * abort word; every CTA then returns.  Returns YQ_E_TIMEOUT (the context stays
+ * usable); *published receives the number of flags that were published (0). */
+int yq_debug_wait_timeout(yq_ctx ctx, int which, unsigned cap, int* published);
+
 /* ---- stochastic reconfiguration (GroundState/SRMat.hpp) ------------------- */
 /* SRMat<Machine, Hamiltonian>(qs, ham) -- SRMat.hpp:83-87, bound to a sampler.
  * mode: S = O~^H O~ / Ns (P x P), T = O~ O~^H / Ns (Ns x Ns, push-through dual),
@@ -267,6 +288,12 @@ int yq_sr_matrix(yq_sr sr, int* dim, double* out);
  * configurations, FP64 sums.  stats = {E, Var}; oloc, grad: P complex
  * (interleaved re, im); S: P x P complex row-major, or NULL to skip it. */
 int yq_exact(yq_rbm q, yq_ham H, int basis_kind, int nup, double* stats, double* oloc, double* grad, double* S);
+/* One epoch of RunRBMExact::run (Runners/RunRBMExact.hpp:46-80): constructExact over
+ * the basis (as yq_exact), v = LLT(corrMat() + shift I).solve(energyGrad()) on the
+ * device, params -= lr v (the SGD step of Optimizers/SGD.hpp:48-54 with the caller's
+ * rate).  out = {E, Var, |v|} (E and Var before the update).  A non-positive
+ * pivot returns YQ_E_NOT_PD (the reference ignores it). */
+int yq_exact_iteration(yq_rbm q, yq_ham H, int basis_kind, int nup, double shift, double lr, double* out);
 
 /* ---- FeedForward machine (Machines/FeedForward.hpp) ------------------------ */
 /* FeedForward with addLayer<Conv1D>(1, channels, kernel, stride 1, no bias),
@@ -313,13 +340,27 @@ typedef struct {
 
 typedef struct {
     double energy, energy_var;
-    double update_norm;    /* ||v|| (RunRBM.hpp:205 nv)                             */
-    double cg_err;
+    double update_norm;    /* ||v|| before the clip (RunRBM.hpp:205 nv)             */
+    double cg_err;         /* CG branch: ||apply(v) - grad|| (RunRBM.hpp:190); 0 for LLT */
     double accept_rate;
     int status;            /* 0 or the YQ_E_* code recorded by the device checks    */
 } yq_iter_result;
 
-/* sampler.randomize + sample + constructFromSamples + solve + update params by -lr v. */
+/* RunRBM::setMomentum(beta1, beta2) -- Runners/RunRBM.hpp:73-77 with ObsAvg
+ * (:13-37): yq_vmc_iteration averages energyGrad() with weight beta1 and, in the
+ * LLT branch, corrMat() with weight beta2 (bias-corrected by 1 - beta^t), in the
+ * order of RunRBM.hpp:180-201 (gradAvg is updated twice per LLT epoch, as there).
+ * beta2 != 0 needs the S-form (YQ_SR_AUTO then picks it; YQ_SR_T fails with
+ * YQ_E_UNSUPPORTED); beta1 != 0 in the T-form solves (S + lambda) v = grad by the
+ * Woodbury identity through T and needs lambda > 0.  Resets both averages.
+ * Batches (yq_batch_*) reject objects with momentum. */
+int yq_sr_set_momentum(yq_sr sr, double beta1, double beta2);
+/* RunRBM::setGradClip(clip) -- RunRBM.hpp:79-82, 205-209: v *= clip / ||v|| when
+ * ||v|| > clip (0 disables); applied on the device by yq_vmc_iteration and batches. */
+int yq_sr_set_grad_clip(yq_sr sr, double clip);
+
+/* sampler.randomize + sample + constructFromSamples + solve + update params by -lr v
+ * (Runners/RunRBM.hpp:166-214 for one epoch ll = p->epoch). */
 int yq_vmc_iteration(yq_sr sr, const yq_iter_params* p, yq_iter_result* r);
 
 /* ---- batches of independent problems --------------------------------------- */

@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <functional>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -242,6 +243,26 @@ yq_ham sweeper_ham(const S&, long) {
 }
 }  // namespace detail
 
+// Utilities/Utility.hpp:61-88: random configurations on the host, for the
+// randomizer functors a RunRBM driver passes to run() (entries +-1; nup values of -1).
+template <class RandomEngine>
+std::vector<int> randomSigma(int n, RandomEngine& re) {
+    std::vector<int> sigma(static_cast<size_t>(n));
+    std::uniform_int_distribution<> uid(0, 1);
+    for (int i = 0; i < n; ++i) sigma[size_t(i)] = -2 * uid(re) + 1;
+    return sigma;
+}
+template <class RandomEngine>
+std::vector<int> randomSigma(int n, int nup, RandomEngine& re) {
+    std::vector<int> sigma(size_t(n), -1);
+    for (int i = nup; i < n; ++i) sigma[size_t(i)] = 1;
+    std::shuffle(sigma.begin(), sigma.end(), re);
+    return sigma;
+}
+// A randomizer that draws the chains on the device (the sampler's own Philox
+// randomSigma, with its nup) instead of calling a host functor per chain.
+struct DeviceRandomSigma {};
+
 // Samples of the last sample() call; they stay on the device.
 struct SampleSet {
     yq_sampler sampler;
@@ -257,9 +278,13 @@ class SamplerMT {
     uint64_t seed_ = 0;
     uint32_t epoch_ = 0;
     bool reinit_ = true;
+    uint32_t nChains_ = 0, n_ = 0;
+    std::default_random_engine re_;
 
 public:
-    SamplerMT(const Machine& qs, uint32_t nTmps, uint32_t nChainsPer, const Sweeper& sw, int nup = -1) {
+    using RandomEngine = std::default_random_engine;
+    SamplerMT(const Machine& qs, uint32_t nTmps, uint32_t nChainsPer, const Sweeper& sw, int nup = -1)
+        : nChains_(nTmps * nChainsPer), n_(qs.getN()) {
         if (nTmps == 0 || (nTmps != 1 && nTmps % 2 != 0))
             throw std::invalid_argument("SamplerMT: nTmps must be 1 or even");  // SamplerMT.hpp:50
         if (sw.n != qs.getN()) throw std::invalid_argument("SamplerMT: sweeper size differs from the machine");
@@ -272,10 +297,35 @@ public:
     SamplerMT& operator=(const SamplerMT&) = delete;
     yq_sampler handle() const { return h_; }
 
-    // SamplerMT.hpp:72-79 (seeded instead of std::random_device)
-    void initializeRandomEngine(uint64_t seed = 0) { seed_ = seed; }
+    // SamplerMT.hpp:72-79, seeded instead of from std::random_device: the device's
+    // Philox streams and the host engine handed to randomizers both derive from seed
+    void initializeRandomEngine(uint64_t seed = 0) {
+        seed_ = seed;
+        re_.seed(static_cast<std::default_random_engine::result_type>(seed ^ (seed >> 32)));
+    }
     // SamplerMT.hpp:103-110: fresh random chains at the next sample() call
     void randomize() { reinit_ = true; }
+    void randomize(DeviceRandomSigma) { reinit_ = true; }
+    // SamplerMT.hpp:103-110 with a randomizer functor: chain c starts from
+    // randomizer(re) (any container of +-1 with size() and operator[], e.g.
+    // std::vector<int> or Eigen::VectorXi), drawn on the host and uploaded.
+    template <class Randomizer,
+              class = decltype(std::declval<Randomizer&>()(std::declval<std::default_random_engine&>()))>
+    void randomize(Randomizer&& randomizer) {
+        std::vector<int8_t> chains(size_t(nChains_) * n_);
+        for (uint32_t c = 0; c < nChains_; ++c) {
+            const auto sigma = randomizer(re_);
+            if (size_t(sigma.size()) != size_t(n_))
+                throw std::invalid_argument("randomize: the randomizer returned a configuration of the wrong size");
+            for (uint32_t i = 0; i < n_; ++i) {
+                const int v = int(sigma[i]);
+                if (v != 1 && v != -1) throw std::invalid_argument("randomize: configurations must hold +-1");
+                chains[size_t(c) * n_ + i] = int8_t(v);
+            }
+        }
+        check(yq_sampler_set_chains(h_, chains.data()));
+        reinit_ = false;
+    }
     // keep the chains across calls (persistent Markov chains)
     void keepChains() { reinit_ = false; }
     // SamplerMT.hpp:180-204
@@ -374,16 +424,23 @@ class RunRBM {
     bool useCG_ = false;
     double cgTol_ = 1e-4;
     double gradClip_ = 0.0;
+    double beta1_ = 0.0, beta2_ = 0.0;
+    uint64_t seed_ = 0;
     SGD opt_;
     bool initialized_ = false;
 
 public:
     RunRBM(Context& ctx, unsigned N, unsigned alpha, bool useBias) : ctx_(ctx), qs_(ctx, N, alpha * N, useBias) {}
+    // seed of the parameter initialisation and of the sampler's streams used by the
+    // reference-shaped run() (the reference seeds from std::random_device)
+    void setSeed(uint64_t seed) { seed_ = seed; }
     RBM<T>& getQs() { return qs_; }
     void initializeRandom(uint64_t seed, double wIni = 1e-3) {
         qs_.initializeRandom(seed, wIni);
         initialized_ = true;
     }
+    // AbstractRunner.hpp:96-101: N(0, wIni^2) parameters from the runner's seed (setSeed)
+    void initializeRandom(double wIni) { initializeRandom(seed_, wIni); }
     void setLambda(double ini, double decay = 1.0, double mn = 0.0) {
         lambdaIni_ = ini;
         lambdaDecay_ = decay;
@@ -407,14 +464,60 @@ public:
         cgTol_ = cgTol;
     }
     void setGradClip(double clip) { gradClip_ = clip; }
+    // RunRBM.hpp:73-77: ObsAvg weights of the gradient and of the Fisher matrix
+    // (beta2 != 0 needs the S-form, i.e. nSweeps x chains >= getDim() on the FP64 path)
+    void setMomentum(double beta1 = 0.0, double beta2 = 0.0) {
+        beta1_ = beta1;
+        beta2_ = beta2;
+    }
 
-    // callback(ll, currE, nv, cgErr, smp_ms, slv_ms) as RunRBM.hpp:219
+    // Runners/RunRBM.hpp:123-222 with the reference's signature: every epoch ll
+    // (0 .. maxIter) saves w%04d.dat when due, calls sampler.randomize(randomizer)
+    // (a host functor randomizer(re) -> configuration, or DeviceRandomSigma{}),
+    // samples nSweeps (default getDim()) after nSweepsDiscard (default 0.1 nSweeps)
+    // sweeps, and runs constructFromSamples, the momentum-averaged LLT or CG solve,
+    // the clip and the SGD step on the device in one yq_vmc_iteration;
+    // callback(ll, currE, nv, cgErr, smp_ms, slv_ms).
+    template <class Sampler, class Callback, class SweeperRandomizer, class Ham,
+              class = typename std::enable_if<std::is_base_of<Hamiltonian, typename std::decay<Ham>::type>::value>::type>
+    void run(Sampler& sampler, Callback&& callback, SweeperRandomizer&& randomizer, Ham&& ham, int nSweeps = -1,
+             int nSweepsDiscard = -1) {
+        if (!initialized_) initializeRandom(seed_, 1e-3);
+        SRMat<RBM<T>, typename std::decay<Ham>::type> srm(qs_, ham, sampler);
+        check(yq_sr_set_momentum(srm.handle(), beta1_, beta2_));
+        check(yq_sr_set_grad_clip(srm.handle(), gradClip_));
+        sampler.initializeRandomEngine(seed_);
+        const int dim = int(qs_.getDim());
+        if (nSweeps == -1) nSweeps = dim;
+        if (nSweepsDiscard == -1) nSweepsDiscard = int(0.1 * nSweeps);
+        for (int ll = 0; ll <= maxIter_; ++ll) {
+            if (saveWfPer_ != 0 && ll % saveWfPer_ == 0) {
+                char fileName[30];
+                std::snprintf(fileName, sizeof(fileName), "w%04d.dat", ll);
+                qs_.save(fileName);
+            }
+            sampler.randomize(randomizer);
+            const double lambda = std::max(lambdaIni_ * std::pow(lambdaDecay_, ll), lambdaMin_);
+            yq_iter_params p{nSweeps, nSweepsDiscard, sampler.reinit() ? 1 : 0, sampler.seed(), uint32_t(ll), lambda,
+                             opt_.eta(), useCG_ ? YQ_SOLVE_CG : YQ_SOLVE_LLT, cgTol_,
+                             std::is_same<T, std::complex<float>>::value ? 2 : 0};
+            yq_iter_result r;
+            check(yq_vmc_iteration(srm.handle(), &p, &r));
+            callback(ll, r.energy, r.update_norm, r.cg_err, ctx_.stageMs(0), ctx_.stageMs(4));
+        }
+    }
+
+    // The same loop with the chains' randomisation left to the sampler (randomize()
+    // for fresh device chains every epoch, keepChains() for persistent chains) and
+    // an explicit seed; callback(ll, currE, nv, cgErr, smp_ms, slv_ms) as RunRBM.hpp:219
     template <class Sampler, class Ham, class Callback>
     void run(Sampler& sampler, Callback&& callback, Ham& ham, int nSweeps, int nSweepsDiscard = -1,
              uint64_t seed = 0) {
         if (!initialized_) initializeRandom(seed, 1e-3);
         if (nSweepsDiscard < 0) nSweepsDiscard = int(0.1 * nSweeps);
         SRMat<RBM<T>, Ham> srm(qs_, ham, sampler);
+        check(yq_sr_set_momentum(srm.handle(), beta1_, beta2_));
+        check(yq_sr_set_grad_clip(srm.handle(), gradClip_));
         sampler.initializeRandomEngine(seed);
         for (int ll = 0; ll <= maxIter_; ++ll) {
             if (saveWfPer_ != 0 && ll % saveWfPer_ == 0) {
@@ -423,27 +526,12 @@ public:
                 qs_.save(fileName);
             }
             const double lambda = std::max(lambdaIni_ * std::pow(lambdaDecay_, ll), lambdaMin_);
-            const double eta = opt_.eta();
-            if (gradClip_ == 0.0) {
-                yq_iter_params p{nSweeps, nSweepsDiscard, sampler.reinit() ? 1 : 0, seed, uint32_t(ll), lambda, eta,
-                                 useCG_ ? YQ_SOLVE_CG : YQ_SOLVE_LLT, cgTol_,
-                                 std::is_same<T, std::complex<float>>::value ? 2 : 0};
-                yq_iter_result r;
-                check(yq_vmc_iteration(srm.handle(), &p, &r));
-                callback(ll, r.energy, r.update_norm, r.cg_err, ctx_.stageMs(0), ctx_.stageMs(4));
-            } else {
-                sampler.setEpoch(uint32_t(ll));
-                SampleSet sr = sampler.sample(uint32_t(nSweeps), uint32_t(nSweepsDiscard));
-                srm.constructFromSamples(sr);
-                std::vector<cd> v = useCG_ ? srm.solveCG(lambda, cgTol_) : srm.solveExact(lambda);
-                double nv = 0.0;
-                for (auto& x : v) nv += std::norm(x);
-                nv = std::sqrt(nv);
-                const double scale = nv > gradClip_ ? gradClip_ / nv : 1.0;  // RunRBM.hpp:205-209
-                for (auto& x : v) x *= -eta * scale;
-                qs_.updateParams(v);
-                callback(ll, srm.eloc(), nv, 0.0, ctx_.stageMs(0), ctx_.stageMs(4));
-            }
+            yq_iter_params p{nSweeps, nSweepsDiscard, sampler.reinit() ? 1 : 0, seed, uint32_t(ll), lambda,
+                             opt_.eta(), useCG_ ? YQ_SOLVE_CG : YQ_SOLVE_LLT, cgTol_,
+                             std::is_same<T, std::complex<float>>::value ? 2 : 0};
+            yq_iter_result r;
+            check(yq_vmc_iteration(srm.handle(), &p, &r));
+            callback(ll, r.energy, r.update_norm, r.cg_err, ctx_.stageMs(0), ctx_.stageMs(4));
         }
     }
 };

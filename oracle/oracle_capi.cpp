@@ -115,6 +115,17 @@ void orc_logderiv(int n, int m, int use_bias, const double* params, const int8_t
     make_rbm(n, m, use_bias, params).logDeriv(s, reinterpret_cast<const cd*>(theta), reinterpret_cast<cd*>(out));
 }
 
+// constructDelta (GroundState/utils.hpp:12-51): one logDeriv row per sample, OpenMP over samples.
+void orc_logderiv_batch(int n, int m, int use_bias, const double* params, int ns, const int8_t* s,
+                        const double* theta, double* out, int nthreads) {
+    RBM q = make_rbm(n, m, use_bias, params);
+    const cd* th = reinterpret_cast<const cd*>(theta);
+    cd* o = reinterpret_cast<cd*>(out);
+    const size_t P = q.dim();
+#pragma omp parallel for schedule(static) num_threads(nthreads > 0 ? nthreads : 1)
+    for (int k = 0; k < ns; ++k) q.logDeriv(s + size_t(k) * n, th + size_t(k) * m, o + size_t(k) * P);
+}
+
 // Hamiltonian: kind 0 TFI ring, 1 XXZ ring, 2 TFI 2D torus, 3 XXX, 4 J1J2, 5 XYZNNN,
 // 6 KitaevHex (oracle.hpp HamKind).
 double orc_ham_enumerate(int kind, int n, int lx, int ly, const double* hp, const int8_t* s,

@@ -60,6 +60,7 @@ def _declare(L):
         "orc_logratio": (None, [i, i, i, vp, vp, vp, i, vp, vp]),
         "orc_flip": (None, [i, i, i, vp, vp, vp, i, vp]),
         "orc_logderiv": (None, [i, i, i, vp, vp, vp, vp]),
+        "orc_logderiv_batch": (None, [i, i, i, vp, i, vp, vp, vp, i]),
         "orc_ham_enumerate": (d, [i, i, i, i, vp, vp, vp, vp, i, vp]),
         "orc_ham_column": (i, [i, i, i, i, vp, u64, vp, vp, i]),
         "orc_eloc": (None, [i, i, i, i, vp, i, i, vp, i, vp, vp, vp, i]),
@@ -207,6 +208,16 @@ def logderiv(n, m, params, sigma, th, use_bias=True):
     return o
 
 
+def logderiv_rows(n, m, params, sigma, th, use_bias=True, nthreads=0):
+    """constructDelta (GroundState/utils.hpp:12-51): logDeriv rows of a batch, Ns x P."""
+    sigma = _s8(sigma)
+    ns = sigma.shape[0]
+    th = np.ascontiguousarray(th, dtype=np.complex128)
+    o = np.zeros((ns, rbm_dim(n, m, use_bias)), dtype=np.complex128)
+    lib().orc_logderiv_batch(n, m, int(use_bias), _p(params), ns, _p(sigma), _p(th), _p(o), nthreads or os.cpu_count())
+    return o
+
+
 def ham_enumerate(ham, sigma, cap=4096):
     masks = np.zeros(cap, dtype=np.uint64)
     coeffs = np.zeros(cap)
@@ -286,6 +297,72 @@ def sr_step(ham, m, params, sigma, th, shift, mode=SR_S, solver=SOLVE_LLT, cgtol
                                cgtol, _p(v), _p(g), _p(ol), _p(el), _p(st), nthreads or os.cpu_count())
     return dict(status=status, v=v, grad=g, oloc=ol, elocs=el, energy=st[0], energy_var=st[1],
                 cg_iters=int(st[2]), cg_relres=st[3])
+
+
+class ObsAvg:
+    """Runners/RunRBM.hpp:13-37: obs = beta obs + (1 - beta) x per update; getAvg
+    divides by 1 - beta^t (t = number of updates)."""
+
+    def __init__(self, beta, ini):
+        self.beta, self.t, self.obs = beta, 0, np.array(ini, dtype=np.complex128)
+
+    def update(self, x):
+        self.obs = self.beta * self.obs + (1.0 - self.beta) * x
+        self.t += 1
+
+    def get_avg(self):
+        return self.obs / (1.0 - self.beta ** self.t)
+
+
+def run_rbm(ham, m, params, n_chains, epochs, n_sweeps, n_discard, seed, shift, lr, beta1=0.0, beta2=0.0,
+            grad_clip=0.0, use_cg=False, use_bias=True, move=MOVE_LOCAL, nup=-1, nthreads=0):
+    """Runners/RunRBM.hpp:151-221 restated for epochs ll = 0 .. epochs-1 with a fixed
+    lambda (`shift`) and SGD rate (`lr`): randomize + sample (Philox epoch ll),
+    constructFromSamples (E_loc, centred logDeriv rows, energyGrad), then
+
+      gradAvg.update(grad); g = gradAvg.getAvg()                    (:180-181)
+      CG branch (use_cg and beta2 == 0):  v = (S + lambda)^{-1} g,
+          cgErr = |apply(v) - g|                                    (:183-191)
+      LLT branch: gradAvg.update(grad) again; fisherAvg.update(S);
+          v = LLT(fisherAvg.getAvg() + lambda I).solve(g)           (:192-202)
+      nv = |v|; v *= clip / nv if clip != 0 and nv > clip          (:204-209)
+      params -= lr v                                                (SGD, :211-216)
+
+    The CG branch is solved exactly here (numpy), the limit of Eigen's CG as its
+    tolerance goes to 0.  Returns (per-epoch dicts energy / nv / cg_err / v, params)."""
+    n = ham.n
+    P = rbm_dim(n, m, use_bias)
+    p = np.array(params, dtype=np.complex128)
+    g_avg = ObsAvg(beta1, np.zeros(P))
+    f_avg = ObsAvg(beta2, np.zeros((P, P)))
+    out = []
+    for ll in range(epochs):
+        s, th, _, _ = sample(n, m, p, n_chains, move=move, nup=nup, seed=seed, epoch=ll, reinit=True,
+                             n_sweeps=n_sweeps, n_discard=n_discard, use_bias=use_bias, nthreads=nthreads)
+        O = logderiv_rows(n, m, p, s, th, use_bias, nthreads)
+        el = eloc(ham, m, p, s, th, use_bias, nthreads)
+        ns = len(s)
+        Oc = O - O.mean(axis=0)
+        grad = Oc.conj().T @ el / ns
+        S = Oc.conj().T @ Oc / ns
+        g_avg.update(grad)
+        g = g_avg.get_avg()
+        A = S + shift * np.eye(P)
+        if use_cg and beta2 == 0.0:
+            v = np.linalg.solve(A, g)
+            cg_err = float(np.linalg.norm(A @ v - g))
+        else:
+            g_avg.update(grad)
+            f_avg.update(S)
+            st, v = cholesky_solve(f_avg.get_avg() + shift * np.eye(P), g)  # Eigen::LLT restated
+            assert st == 0, "LLT met a non-positive pivot"
+            cg_err = 0.0
+        nv = float(np.linalg.norm(v))
+        if grad_clip != 0.0 and nv > grad_clip:
+            v = v * (grad_clip / nv)
+        p = p - lr * v
+        out.append(dict(energy=float(el.real.mean()), nv=nv, cg_err=cg_err, v=v))
+    return out, p
 
 
 def cholesky_solve(A, b):

@@ -24,7 +24,7 @@ def _build(tmp_path, name="rbm_tfi_driver"):
     return exe
 
 
-@pytest.mark.parametrize("name", ["rbm_tfi_driver", "j1j2_driver", "amplitude_phase_driver"])
+@pytest.mark.parametrize("name", ["rbm_tfi_driver", "j1j2_driver", "amplitude_phase_driver", "run_rbm_reference_shape"])
 def test_adapters_compile(tmp_path, name):
     _build(tmp_path, name)
 
@@ -77,3 +77,21 @@ def test_amplitude_phase_driver_runs(tmp_path, orc):
     e0 = orc.ed_ground(orc.Ham.j1j2(12, 1.0, 0.2, True), 1, 6) / 12
     assert e_last < e_first
     assert e_last >= e0 - 1e-9
+
+
+@pytest.mark.gpu
+def test_reference_shaped_run_with_randomizer(tmp_path, orc):
+    """RunRBM::run(sampler, callback, randomizer, std::move(ham), nSweeps, nDiscard)
+    as Examples/RBMTFI.cpp calls it: the host randomizer is called once per chain
+    per epoch (nTmp x K chains, epochs 0..maxIter), and the energy goes down
+    towards the ground state."""
+    exe = _build(tmp_path, "run_rbm_reference_shape")
+    out = subprocess.run([exe, "30"], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    calls = int([l for l in out.stdout.splitlines() if l.startswith("RANDOMIZER")][0].split()[1])
+    assert calls == 31 * 2 * 16
+    last = [l for l in out.stdout.splitlines() if l.startswith("OK")][0].split()
+    e_first, e_last = float(last[1]), float(last[2])
+    e0 = orc.ed_ground(orc.Ham.tfi(10, -1.0, -1.0)) / 10
+    assert e_last < e_first
+    assert e_last >= e0 - 1e-3

@@ -2,7 +2,9 @@
 and the captured-graph replays give, problem by problem, the same energies and
 parameters as running each problem alone through yq_vmc_iteration with the
 batch's seed + position and consecutive epochs (the same kernels on the same
-inputs; stated tolerance 1e-12 relative)."""
+inputs; stated tolerance 1e-12 relative), and, for the FP64 batch, the same as
+the oracle's restated loop per problem (SamplerMT with persistent chains,
+SRMat T-form, SGD: energies 1e-11, parameters 1e-9 relative)."""
 import numpy as np
 import pytest
 
@@ -59,6 +61,20 @@ def test_batch_matches_single_problems(orc, prec):
         assert all(got[it][k].status == 0 for it in range(ITERS))
         p = built[k][1].get_params()
         assert np.max(np.abs(p - single[k][1])) <= 1e-12 * np.max(np.abs(single[k][1]))
+    if prec == "fp64":
+        for k, (n, alpha, h, chains) in enumerate(specs):
+            m = alpha * n
+            ham = orc.Ham.tfi(n, -1.0, -h)
+            pp = orc.init_params(n, m, 100 + k, 0.05)
+            cs = None
+            for it in range(ITERS):
+                s, th, cs, _ = orc.sample(n, m, pp, chains, seed=SEED + k, epoch=it, reinit=(it == 0),
+                                          n_sweeps=SWEEPS, n_discard=DISCARD, chain_sigma=cs)
+                ref = orc.sr_step(ham, m, pp, s, th, SHIFT, orc.SR_T, orc.SOLVE_LLT)
+                assert got[it][k].energy == pytest.approx(ref["energy"], rel=1e-11), (k, it)
+                pp = pp - LR * ref["v"]
+            p = built[k][1].get_params()
+            assert np.max(np.abs(p - pp)) <= 1e-9 * np.max(np.abs(pp)), k
     # changed parameters: eager call and a new capture
     r = B.iteration(SWEEPS, DISCARD, SEED, ITERS, SHIFT, 0.5 * LR, reinit=False, ir_steps=ir)
     r2 = B.iteration(SWEEPS, DISCARD, SEED, ITERS + 1, SHIFT, 0.5 * LR, reinit=False, ir_steps=ir)

@@ -77,6 +77,47 @@ def test_log_psi_and_ratios(ctx, orc, dtype):
         assert np.max(np.abs(np.exp(got - ref) - 1)) < tol
 
 
+@pytest.mark.parametrize("dtype", [1, 0])
+def test_k_flip_and_state_ratios(ctx, orc, dtype):
+    """logRatio(vector<int>) and logRatio(other state) (States/RBMState.hpp:107-149)
+    as Tests/TestRBMStates.cpp:93-237 checks them -- N = M = 10, weights N(0, 1) --
+    against the oracle's k-flip ratio and the difference of exact log psi, modulo
+    2 pi i, for 1 to 10 flips; the flipped state's theta cache after 100 flips
+    equals a fresh calcTheta (:214-236), so the state ratio can use either."""
+    from yannq_b200 import api
+
+    n = m = 10
+    q, p = _rbm(api, ctx, orc, n, m, 11, 1.0, dtype)
+    rng = np.random.default_rng(3)
+    s = _rand_sigma(rng, 48, n)
+    th = np.array([orc.theta(n, m, p, x) for x in s])
+    # weights are evaluated in the machine's type, so the complex64 machine agrees at its tolerance
+    tol = TOL64 if dtype == api.C128 else 2e-4
+    for k in range(1, n + 1):
+        flips = np.array([rng.choice(n, k, replace=False) for _ in range(len(s))], np.int32)
+        got = q.log_ratio_k(s, th, flips)
+        ref = np.array([orc.logratio(n, m, p, x, t, f) for x, t, f in zip(s, th, flips)])
+        assert np.max(np.abs(np.exp(got - ref) - 1)) < tol, k
+        s2 = s.copy()
+        for r, f in enumerate(flips):
+            s2[r, f] *= -1
+        exact = np.array([orc.logpsi(n, m, p, b) - orc.logpsi(n, m, p, a) for a, b in zip(s, s2)])
+        assert np.max(np.abs(np.exp(got - exact) - 1)) < tol, k
+    # state vs state: random pairs, theta of the second state from 100 incremental flips
+    s_b = _rand_sigma(rng, len(s), n)
+    th_b = np.array([orc.theta(n, m, p, x) for x in s_b])
+    for r in range(len(s)):
+        sig, t = s_b[r].copy(), th_b[r].copy()
+        for f in rng.integers(0, n, 100):
+            orc.flip(n, m, p, sig, t, [int(f)])
+        assert np.max(np.abs(t - orc.theta(n, m, p, sig))) < 1e-6  # TestRBMStates.cpp:214-236
+        s_b[r], th_b[r] = sig, t
+    got = q.log_ratio_states(s, th, s_b, th_b)
+    exact = np.array([orc.logpsi(n, m, p, b) - orc.logpsi(n, m, p, a) for a, b in zip(s, s_b)])
+    assert np.max(np.abs(np.exp(got - exact) - 1)) < max(tol, 1e-9)
+    q.close()
+
+
 def test_log_deriv(ctx, orc):
     from yannq_b200 import api
 

@@ -229,3 +229,55 @@ def test_hamiltonian_sweeper_list_sizes_vary(orc):
 
     assert len(sizes(orc.Ham.j1j2(n, 1.0, 0.5, True))) > 1
     assert sizes(orc.Ham.xyznnn(n, 0.3, 0.7)) == {2 * n}
+
+
+def test_runner_restatement_without_momentum_is_the_sr_step_loop(orc):
+    """pyoracle.run_rbm (Runners/RunRBM.hpp:151-221) with beta1 = beta2 = 0 and no
+    clip is the loop of C++ oracle SR steps (S-form LLT) on the same samples."""
+    n, m = 8, 16
+    ham = orc.Ham.tfi(n, -1.0, -1.0)
+    p = orc.init_params(n, m, 20261203, 0.01)
+    out, pf = orc.run_rbm(ham, m, p, 16, 3, 16, 16, 7, 1e-3, 0.01)
+    pp = p.copy()
+    for it in range(3):
+        s, th, _, _ = orc.sample(n, m, pp, 16, seed=7, epoch=it, n_sweeps=16, n_discard=16)
+        ref = orc.sr_step(ham, m, pp, s, th, 1e-3, orc.SR_S, orc.SOLVE_LLT)
+        assert out[it]["energy"] == pytest.approx(ref["energy"], rel=1e-12)
+        assert np.linalg.norm(out[it]["v"] - ref["v"]) <= 1e-10 * np.linalg.norm(ref["v"])
+        pp = pp - 0.01 * ref["v"]
+    assert np.max(np.abs(pf - pp)) <= 1e-12
+
+
+def test_obs_avg_semantics(orc):
+    """ObsAvg (RunRBM.hpp:13-37): starting from zero, getAvg after t updates is the
+    bias-corrected exponential average; a constant input averages to itself and
+    beta = 0 returns the last input."""
+    a = orc.ObsAvg(0.9, np.zeros(3))
+    xs = [np.array([1.0, 2.0, 3.0]) * (k + 1) for k in range(4)]
+    for x in xs:
+        a.update(x)
+    w = np.array([0.9 ** (3 - k) * 0.1 for k in range(4)])
+    assert np.allclose(a.get_avg(), sum(wk * x for wk, x in zip(w, xs)) / (1 - 0.9 ** 4), rtol=1e-14)
+    c = orc.ObsAvg(0.95, np.zeros(2))
+    for _ in range(5):
+        c.update(np.array([2.0, -1.0]))
+    assert np.allclose(c.get_avg(), [2.0, -1.0], rtol=1e-14)
+    z = orc.ObsAvg(0.0, np.zeros(1))
+    z.update(np.array([5.0]))
+    z.update(np.array([7.0]))
+    assert z.get_avg()[0] == 7.0
+
+
+@pytest.mark.parametrize("beta1,beta2,clip", [(0.9, 0.0, 0.0), (0.0, 0.9, 0.0), (0.0, 0.0, 0.05)])
+def test_runner_options_change_the_trajectory(orc, beta1, beta2, clip):
+    """Each RunRBM option (gradient momentum, Fisher averaging, update clip) moves
+    the parameters away from the plain loop, and the clip bounds the step."""
+    n, m = 6, 12
+    ham = orc.Ham.tfi(n, -1.0, -1.0)
+    p = orc.init_params(n, m, 3, 0.05)
+    plain, p0 = orc.run_rbm(ham, m, p, 16, 3, 16, 16, 11, 1e-3, 0.05)
+    opt, p1 = orc.run_rbm(ham, m, p, 16, 3, 16, 16, 11, 1e-3, 0.05, beta1=beta1, beta2=beta2, grad_clip=clip)
+    assert plain[0]["energy"] == opt[0]["energy"]  # same parameters, same samples at epoch 0
+    assert np.max(np.abs(p1 - p0)) > 1e-8
+    if clip:
+        assert all(np.linalg.norm(o["v"]) <= clip * (1 + 1e-12) for o in opt)

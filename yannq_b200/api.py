@@ -55,6 +55,7 @@ SIGNATURES = {
     "yq_last_error": [C.c_char_p, _sz],
     "yq_version": [],
     "yq_launch_count": [_vp],
+    "yq_alloc_count": [_vp],
     "yq_host_alloc": [_sz, _vp],
     "yq_host_free": [_vp],
     "yq_ctx_create": [_i, _vp],
@@ -95,6 +96,8 @@ SIGNATURES = {
     "yq_rbm_log_psi": [_vp, _i, _vp, _vp],
     "yq_rbm_log_ratio": [_vp, _i, _vp, _vp, _i, _vp, _vp],
     "yq_rbm_log_deriv": [_vp, _i, _vp, _vp, _vp],
+    "yq_rbm_log_ratio_k": [_vp, _i, _vp, _vp, _i, _vp, _vp],
+    "yq_rbm_log_ratio_states": [_vp, _i, _vp, _vp, _vp, _vp, _vp],
     "yq_rbm_oloc_noalloc": [_vp, _i, _vp, _vp, _vp],
     "yq_ham_create": [_vp, _i, _i, _i, _i, _d, _d, _i, _vp],
     "yq_ham_create_kitaev_hex": [_vp, _i, _i, _d, _d, _d, _d, _vp],
@@ -118,9 +121,11 @@ SIGNATURES = {
     "yq_sampler_set_tempering": [_vp, _i],
     "yq_sampler_get_slots": [_vp, _vp],
     "yq_exact": [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp],
+    "yq_exact_iteration": [_vp, _vp, _i, _i, _d, _d, _vp],
     "yq_batch_create": [_vp, _i, _vp, _vp],
     "yq_batch_iteration": [_vp, _vp, _vp],
     "yq_batch_destroy": [_vp],
+    "yq_debug_wait_timeout": [_vp, _i, C.c_uint, _vp],
     "yq_sr_create": [_vp, _vp, _vp, _i, _i, _vp],
     "yq_sr_destroy": [_vp],
     "yq_sr_construct": [_vp],
@@ -128,6 +133,8 @@ SIGNATURES = {
     "yq_sr_get": [_vp, _i, _vp],
     "yq_sr_solve": [_vp, _d, _i, _d, _vp, _vp, _vp],
     "yq_sr_matrix": [_vp, _vp, _vp],
+    "yq_sr_set_momentum": [_vp, _d, _d],
+    "yq_sr_set_grad_clip": [_vp, _d],
     "yq_vmc_iteration": [_vp, _vp, _vp],
     "yq_ff_create": [_vp, _i, _i, _i, _i, _vp],
     "yq_ff_destroy": [_vp],
@@ -182,6 +189,20 @@ def exact(rbm, ham, basis_kind=0, nup=0, with_S=True):
     S = np.zeros((P, P), np.complex128) if with_S else None
     check(lib().yq_exact(rbm.h, ham.h, basis_kind, nup, _p(st), _p(ol), _p(g), _p(S) if with_S else None))
     return dict(energy=st[0], energy_var=st[1], oloc=ol, grad=g, S=S)
+
+
+def exact_iteration(rbm, ham, shift, lr, basis_kind=0, nup=0):
+    """One RunRBMExact epoch (Runners/RunRBMExact.hpp:46-80) on the device: returns
+    (E, Var, |v|), the energy before the update."""
+    out = np.zeros(3)
+    check(lib().yq_exact_iteration(rbm.h, ham.h, basis_kind, nup, shift, lr, _p(out)))
+    return float(out[0]), float(out[1]), float(out[2])
+
+
+def alloc_count():
+    v = C.c_uint64()
+    check(lib().yq_alloc_count(C.byref(v)))
+    return v.value
 
 
 def launch_count():
@@ -320,6 +341,25 @@ class RBM:
         f = np.ascontiguousarray(flips, dtype=np.int32).reshape(s.shape[0], -1)
         out = np.zeros(s.shape[0], np.complex128)
         check(lib().yq_rbm_log_ratio(self.h, s.shape[0], _p(s), _p(th), f.shape[1], _p(f), _p(out)))
+        return out
+
+    def log_ratio_k(self, sigma, theta, flips):
+        """logRatio(vector<int>) (States/RBMState.hpp:107-125): flips is ns x k."""
+        s = _s8(sigma).reshape(-1, self.n)
+        th = _c128(theta).reshape(s.shape[0], self.m)
+        f = np.ascontiguousarray(flips, dtype=np.int32).reshape(s.shape[0], -1)
+        out = np.zeros(s.shape[0], np.complex128)
+        check(lib().yq_rbm_log_ratio_k(self.h, s.shape[0], _p(s), _p(th), f.shape[1], _p(f), _p(out)))
+        return out
+
+    def log_ratio_states(self, sigma, theta, sigma_other, theta_other):
+        """logRatio(other state) (States/RBMState.hpp:136-149)."""
+        s = _s8(sigma).reshape(-1, self.n)
+        th = _c128(theta).reshape(s.shape[0], self.m)
+        so = _s8(sigma_other).reshape(s.shape[0], self.n)
+        tho = _c128(theta_other).reshape(s.shape[0], self.m)
+        out = np.zeros(s.shape[0], np.complex128)
+        check(lib().yq_rbm_log_ratio_states(self.h, s.shape[0], _p(s), _p(th), _p(so), _p(tho), _p(out)))
         return out
 
     def log_deriv(self, sigma, theta):
@@ -530,6 +570,14 @@ class SR:
         out = np.zeros((d.value, d.value), np.complex128)
         check(lib().yq_sr_matrix(self.h, C.byref(d), _p(out)))
         return out
+
+    def set_momentum(self, beta1, beta2=0.0):
+        """RunRBM::setMomentum (Runners/RunRBM.hpp:73-77), applied by iteration()."""
+        check(lib().yq_sr_set_momentum(self.h, beta1, beta2))
+
+    def set_grad_clip(self, clip):
+        """RunRBM::setGradClip (Runners/RunRBM.hpp:79-82), applied by iteration()."""
+        check(lib().yq_sr_set_grad_clip(self.h, clip))
 
     def iteration(self, n_sweeps, n_discard, seed, epoch, shift, lr, reinit=True, solver=SOLVE_LLT, cg_tol=1e-4,
                   ir_steps=0):

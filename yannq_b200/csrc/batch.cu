@@ -99,6 +99,9 @@ void batch_iteration(yq_batch_s* B, const yq_iter_params& p, yq_iter_result* res
     YQ_CHECK_ARG(p.solver == YQ_SOLVE_LLT, "batch: the captured iteration needs the LLT solver");
     YQ_CHECK_ARG(p.lr >= 0.0, "batch: lr must be >= 0");
     const int np = int(B->srs.size());
+    for (auto* sr : B->srs)
+        if (sr->beta1 != 0.0 || sr->beta2 != 0.0)
+            throw Error(YQ_E_UNSUPPORTED, "batch: momentum (yq_sr_set_momentum) is not captured in batch graphs");
     cudaStream_t master = B->ctx->stream;
     if (B->have_graph && same_params(B->captured, p)) {
         YQ_CUDA(cudaGraphLaunch(B->exec, master));

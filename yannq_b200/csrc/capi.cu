@@ -5,10 +5,12 @@
 #include <string>
 #include <vector>
 
+#include "chol.hpp"
 #include "internal.hpp"
 
 namespace yq {
 std::atomic<unsigned long long> g_launches{0};
+std::atomic<unsigned long long> g_device_allocs{0};
 void record_error(const std::string& msg);
 }
 
@@ -144,6 +146,13 @@ int yq_launch_count(uint64_t* out) {
     return guard([&] {
         need(out, "out");
         *out = g_launches.load(std::memory_order_relaxed);
+    });
+}
+
+int yq_alloc_count(uint64_t* out) {
+    return guard([&] {
+        need(out, "out");
+        *out = g_device_allocs.load(std::memory_order_relaxed);
     });
 }
 
@@ -448,6 +457,59 @@ int yq_rbm_log_ratio(yq_rbm q, int ns, const int8_t* sigma, const double* theta,
         int* df = sf.up(flips, size_t(ns) * nflip, st);
         c128* d = so.alloc<c128>(ns);
         rbm_log_ratio(q, ns, ds, dth, nflip, df, d);
+        down(reinterpret_cast<c128*>(out), d, ns, st);
+    });
+}
+
+int yq_rbm_log_ratio_k(yq_rbm q, int ns, const int8_t* sigma, const double* theta, int k, const int* flips,
+                       double* out) {
+    return guard([&] {
+        need(q, "rbm");
+        need(sigma, "sigma");
+        need(theta, "theta");
+        need(flips, "flips");
+        need(out, "out");
+        if (ns < 0) throw Error(YQ_E_ARG, "ns < 0");
+        if (k < 1 || k > q->n) throw Error(YQ_E_ARG, "log_ratio_k: k must lie in [1, n]");
+        check_sigma(sigma, size_t(ns) * q->n);
+        for (int s = 0; s < ns; ++s)
+            for (int e = 0; e < k; ++e) {
+                const int f = flips[size_t(s) * k + e];
+                if (f < 0 || f >= q->n) throw Error(YQ_E_ARG, "log_ratio_k: flip site out of range");
+                for (int d = 0; d < e; ++d)
+                    if (flips[size_t(s) * k + d] == f) throw Error(YQ_E_ARG, "log_ratio_k: repeated flip site");
+            }
+        Staging ss, st64, sf, so;
+        cudaStream_t st = q->ctx->stream;
+        int8_t* ds = ss.up(sigma, size_t(ns) * q->n, st);
+        c128* dth = st64.up(reinterpret_cast<const c128*>(theta), size_t(ns) * q->m, st);
+        int* df = sf.up(flips, size_t(ns) * k, st);
+        c128* d = so.alloc<c128>(ns);
+        rbm_log_ratio_k(q, ns, ds, dth, k, df, d);
+        down(reinterpret_cast<c128*>(out), d, ns, st);
+    });
+}
+
+int yq_rbm_log_ratio_states(yq_rbm q, int ns, const int8_t* sigma, const double* theta, const int8_t* sigma_other,
+                            const double* theta_other, double* out) {
+    return guard([&] {
+        need(q, "rbm");
+        need(sigma, "sigma");
+        need(theta, "theta");
+        need(sigma_other, "sigma_other");
+        need(theta_other, "theta_other");
+        need(out, "out");
+        if (ns < 0) throw Error(YQ_E_ARG, "ns < 0");
+        check_sigma(sigma, size_t(ns) * q->n);
+        check_sigma(sigma_other, size_t(ns) * q->n);
+        Staging sa, ta, sb, tb, so;
+        cudaStream_t st = q->ctx->stream;
+        int8_t* dsa = sa.up(sigma, size_t(ns) * q->n, st);
+        c128* dta = ta.up(reinterpret_cast<const c128*>(theta), size_t(ns) * q->m, st);
+        int8_t* dsb = sb.up(sigma_other, size_t(ns) * q->n, st);
+        c128* dtb = tb.up(reinterpret_cast<const c128*>(theta_other), size_t(ns) * q->m, st);
+        c128* d = so.alloc<c128>(ns);
+        rbm_log_ratio_states(q, ns, dsa, dta, dsb, dtb, d);
         down(reinterpret_cast<c128*>(out), d, ns, st);
     });
 }
@@ -781,6 +843,16 @@ int yq_sampler_put_samples(yq_sampler S, int ns, const int8_t* sigma, const doub
     });
 }
 
+int yq_debug_wait_timeout(yq_ctx ctx, int which, unsigned cap, int* published) {
+    return guard([&] {
+        need(ctx, "ctx");
+        need(published, "published");
+        if (which != 0 && which != 1) throw Error(YQ_E_ARG, "debug_wait_timeout: which must be 0 or 1");
+        *published = chol_debug_unpublished_flag(which, cap, ctx->status.as<int>(), ctx->sm_count, ctx->stream);
+        raise_device_status(ctx);
+    });
+}
+
 // ---- SR ---------------------------------------------------------------------------
 int yq_sr_create(yq_rbm q, yq_ham H, yq_sampler S, int mode, int precision, yq_sr* out) {
     return guard([&] {
@@ -890,6 +962,18 @@ int yq_exact(yq_rbm q, yq_ham H, int basis_kind, int nup, double* stats, double*
     });
 }
 
+int yq_exact_iteration(yq_rbm q, yq_ham H, int basis_kind, int nup, double shift, double lr, double* out) {
+    return guard([&] {
+        need(q, "rbm");
+        need(H, "hamiltonian");
+        need(out, "out");
+        if (q->ctx != H->ctx) throw Error(YQ_E_ARG, "exact: RBM and Hamiltonian belong to different contexts");
+        if (!(shift >= 0.0) || !(lr >= 0.0)) throw Error(YQ_E_ARG, "exact_iteration: shift and lr must be >= 0");
+        exact_iteration(q, H, basis_kind, nup, shift, lr, out);
+        raise_device_status(q->ctx);
+    });
+}
+
 int yq_sr_matrix(yq_sr sr, int* dim, double* out) {
     return guard([&] {
         need(sr, "sr");
@@ -904,6 +988,26 @@ int yq_sr_matrix(yq_sr sr, int* dim, double* out) {
                                   size_t(sr->dim) * sizeof(c128), size_t(sr->dim), cudaMemcpyDeviceToHost, st));
         YQ_CUDA(cudaStreamSynchronize(st));
         raise_device_status(sr->q->ctx);
+    });
+}
+
+int yq_sr_set_momentum(yq_sr sr, double beta1, double beta2) {
+    return guard([&] {
+        need(sr, "sr");
+        if (!(beta1 >= 0.0 && beta1 < 1.0) || !(beta2 >= 0.0 && beta2 < 1.0))
+            throw Error(YQ_E_ARG, "set_momentum: beta1 and beta2 must lie in [0, 1)");
+        sr->beta1 = beta1;
+        sr->beta2 = beta2;
+        sr->t_grad = 0;
+        sr->t_fisher = 0;
+    });
+}
+
+int yq_sr_set_grad_clip(yq_sr sr, double clip) {
+    return guard([&] {
+        need(sr, "sr");
+        if (!(clip >= 0.0)) throw Error(YQ_E_ARG, "set_grad_clip: clip must be >= 0");
+        sr->grad_clip = clip;
     });
 }
 
@@ -922,8 +1026,8 @@ int yq_vmc_iteration(yq_sr sr, const yq_iter_params* p, yq_iter_result* r) {
         ctx->stage_end(ST_SAMPLE);
         sr_construct(sr);
         int iters = 0;
-        double relres = 0.;
-        sr_solve(sr, p->shift, p->solver, p->cg_tol, p->ir_steps, &iters, &relres);
+        double relres = 0., cg_err = 0.;
+        sr_solve_runner(sr, p->shift, p->solver, p->cg_tol, p->ir_steps, &iters, &relres, &cg_err);
         sr_update_params(sr, p->lr);
         ctx->stage_end(ST_TOTAL);
         double h[8];
@@ -937,7 +1041,7 @@ int yq_vmc_iteration(yq_sr sr, const yq_iter_params* p, yq_iter_result* r) {
         r->energy = h[0];
         r->energy_var = h[1];
         r->update_norm = h[4];
-        r->cg_err = relres;
+        r->cg_err = cg_err;
         r->accept_rate = tot / (double(sr->S->n_chains) * double(sr->S->proposals));
         int code = status_to_code(ctx->read_status_and_clear());
         r->status = code;

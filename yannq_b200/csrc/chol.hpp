@@ -37,4 +37,9 @@ void chol_factor_panels(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int*
 void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c128* LinvH, c128* b, c128* out,
                       int* status, void* scratch, int sm_count, cudaStream_t st);
 
+// Failure injection for the bounded flag waits (tests only): which = 0 the tile
+// factorisation, 1 the forward solve, each with the flag of its first work item
+// never published and a wait limit of `cap` polls.  Returns the flags published.
+int chol_debug_unpublished_flag(int which, unsigned cap, int* status, int sm_count, cudaStream_t st);
+
 }  // namespace yq

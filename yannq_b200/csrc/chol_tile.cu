@@ -705,4 +705,62 @@ void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c
     if (out != b) YQ_CUDA(cudaMemcpyAsync(out, b, size_t(n) * sizeof(c128), cudaMemcpyDeviceToDevice, st));
 }
 
+// Failure injection for the bounded waits (tests only): a 4 x 4-tile problem whose
+// first work item -- the tile (0, 0) of the factorisation (which = 0) or the block
+// row 0 of the forward solve (which = 1) -- is never claimed, because its counter
+// starts at 1, so the flag that item would publish is never set.  Every other item
+// depends on it; the first wait to pass `cap` polls sets DS_TIMEOUT and the abort
+// word, and every CTA returns through its normal exit (pending copies drained).
+// Returns the number of flags published (0 when every CTA stopped).
+int chol_debug_unpublished_flag(int which, unsigned cap, int* status, int sm_count, cudaStream_t st) {
+    constexpr int nt = 4, n = nt * TB;
+    DevBuf G, Li, LiH, b, scratch;
+    G.ensure(size_t(n) * n * sizeof(c128));
+    Li.ensure(size_t(n) * TB * sizeof(c128));
+    LiH.ensure(size_t(n) * TB * sizeof(c128));
+    b.ensure(size_t(n) * sizeof(c128));
+    scratch.ensure(chol_tile_scratch_bytes(n));
+    YQ_CUDA(cudaMemsetAsync(G.p, 0, G.bytes, st));
+    YQ_CUDA(cudaMemsetAsync(Li.p, 0, Li.bytes, st));
+    YQ_CUDA(cudaMemsetAsync(LiH.p, 0, LiH.bytes, st));
+    YQ_CUDA(cudaMemsetAsync(b.p, 0, b.bytes, st));
+    Scratch sc(scratch.p, nt);
+    write_items(sc, nt, st);
+    YQ_CUDA(cudaMemsetAsync(sc.words, 0, reinterpret_cast<char*>(sc.items) - reinterpret_cast<char*>(sc.words), st));
+    const int one = 1;
+    int* published_base = nullptr;
+    int nflags = 0;
+    if (which == 0) {
+        YQ_CUDA(cudaMemcpyAsync(sc.words + 0, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+        const int nitems = nt * (nt + 1) / 2;
+        TileArgs a{G.as<c128>(), size_t(n), nt, 0, Li.as<c128>(), LiH.as<c128>(), sc.items, nitems, sc.words + 0,
+                   sc.flags, Sync{status, sc.words + 1, cap}};
+        launch_tiles(a, nitems, sm_count, st);
+        published_base = sc.flags;
+        nflags = nt * nt;
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            YQ_CUDA(cudaFuncSetAttribute(chol_fwd_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(SM_SOLVE)));
+            attr = true;
+        }
+        YQ_CUDA(cudaMemcpyAsync(sc.words + 3, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+        const int grid = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_fwd_tile_kernel), 128,
+                                                        SM_SOLVE, sm_count));
+        SolveArgs fa{G.as<c128>(), size_t(n), nt, Li.as<c128>(), LiH.as<c128>(), b.as<c128>(), sc.sflags,
+                     sc.words + 3, Sync{status, sc.words + 2, cap}};
+        chol_fwd_tile_kernel<<<grid, 128, SM_SOLVE, st>>>(fa);
+        YQ_LAUNCH_CHECK();
+        published_base = sc.sflags;
+        nflags = nt;
+    }
+    std::vector<int> flags(static_cast<size_t>(nflags));
+    YQ_CUDA(cudaMemcpyAsync(flags.data(), published_base, size_t(nflags) * sizeof(int), cudaMemcpyDeviceToHost, st));
+    YQ_CUDA(cudaStreamSynchronize(st));
+    int published = 0;
+    for (int f : flags) published += f != 0;
+    return published;
+}
+
 }  // namespace yq

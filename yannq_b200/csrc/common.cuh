@@ -35,8 +35,10 @@ struct Error : std::runtime_error {
         if (!(cond)) throw ::yq::Error(YQ_E_ARG, std::string(msg)); \
     } while (0)
 
-// Counts the library's own kernel launches (reported by yq_launch_count).
+// Counts the library's own kernel launches (reported by yq_launch_count) and its
+// device allocations (every one goes through DevBuf::ensure; yq_alloc_count).
 extern std::atomic<unsigned long long> g_launches;
+extern std::atomic<unsigned long long> g_device_allocs;
 #define YQ_LAUNCH_CHECK()                                               \
     do {                                                                \
         ::yq::g_launches.fetch_add(1, std::memory_order_relaxed);       \
@@ -261,6 +263,7 @@ struct DevBuf {
         if (b <= bytes && p) return;
         release();
         if (b == 0) return;
+        g_device_allocs.fetch_add(1, std::memory_order_relaxed);
         cudaError_t e = cudaMalloc(&p, b);
         if (e != cudaSuccess) {
             p = nullptr;

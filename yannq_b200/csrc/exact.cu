@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "basis.cuh"
+#include "chol.hpp"
 #include "gemm64.cuh"
 #include "internal.hpp"
 
@@ -321,7 +322,7 @@ void basis_state(yq_rbm_s* q, int kind, int nup, BasisState& bs) {
 }  // namespace
 
 void exact_summation(yq_rbm_s* q, yq_ham_s* H, int kind, int nup, double* stats, c128* d_oloc, c128* d_grad,
-                     c128* d_S) {
+                     c128* d_S, size_t ldS, double shift) {
     YQ_CHECK_ARG(H->n == q->n, "exact: Hamiltonian and RBM sizes differ");
     YQ_CHECK_ARG(kind != YQ_BASIS_JZ || H->conserves_sz,
                  "exact: the Jz basis needs a Hamiltonian that conserves Sz (XXZ, XXX, J1J2)");
@@ -378,12 +379,86 @@ void exact_summation(yq_rbm_s* q, yq_ham_s* H, int kind, int nup, double* stats,
                                                                                         eloc.as<c128>(), y.as<c128>());
     YQ_LAUNCH_CHECK();
     colsum<true>(O.as<c128>(), dim, P, y.as<c128>(), cpart.as<c128>(), nsplit, d_grad, st);
-    if (d_S) gram_fp64<double>(O.as<c128>(), P, 1, int(P), int(dim), d_S, P, 1.0, 0, 0.0, st);
+    if (d_S) gram_fp64<double>(O.as<c128>(), P, 1, int(P), int(dim), d_S, ldS ? ldS : P, 1.0, 0, shift, st);
     double h[4];
     YQ_CUDA(cudaMemcpyAsync(h, out.p, sizeof(h), cudaMemcpyDeviceToHost, st));
     YQ_CUDA(cudaStreamSynchronize(st));
     stats[0] = h[0];
     stats[1] = h[1];
+}
+
+namespace {
+// unit diagonal and zeros outside the leading dim x dim block of the padded matrix
+__global__ void exact_pad_kernel(c128* G, int dim, int dim_pad) {
+    const size_t total = size_t(dim_pad) * dim_pad;
+    for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < total; q += size_t(gridDim.x) * blockDim.x) {
+        const int r = int(q / dim_pad), c = int(q % dim_pad);
+        if (r >= dim || c >= dim) G[q] = mk(r == c ? 1.0 : 0.0, 0.0);
+    }
+}
+
+// params -= lr v; |v|^2 accumulated by one block (P is at most a few tens of thousands)
+__global__ void exact_update_kernel(size_t P, double lr, const c128* __restrict__ v, c128* __restrict__ p64,
+                                    double* __restrict__ out) {
+    __shared__ double red[32];
+    double acc = 0.;
+    for (size_t p = threadIdx.x; p < P; p += blockDim.x) {
+        const c128 x = v[p];
+        acc += x.re * x.re + x.im * x.im;
+        p64[p] = p64[p] - lr * x;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) r += red[w];
+        out[0] = sqrt(r);
+    }
+}
+}  // namespace
+
+// One epoch of RunRBMExact::run (Runners/RunRBMExact.hpp:46-80): constructExact,
+// corrMat + lambda I by LLT (tile Cholesky on the device), v = LLT.solve(energyGrad),
+// params -= lr v.  out = {E, Var, |v|}.
+void exact_iteration(yq_rbm_s* q, yq_ham_s* H, int kind, int nup, double shift, double lr, double* out) {
+    yq_ctx_s* ctx = q->ctx;
+    cudaStream_t st = ctx->stream;
+    const size_t P = q->P;
+    const int dim_pad = int((P + CHOL_NB - 1) / CHOL_NB) * CHOL_NB;
+    const size_t dp = size_t(dim_pad);
+    DevBuf G, Li, LiH, oloc, grad, b, x, work, nv;
+    G.ensure(dp * dp * sizeof(c128));
+    Li.ensure(dp * CHOL_NB * sizeof(c128));
+    LiH.ensure(dp * CHOL_NB * sizeof(c128));
+    oloc.ensure(P * sizeof(c128));
+    grad.ensure(P * sizeof(c128));
+    b.ensure(dp * sizeof(c128));
+    x.ensure(dp * sizeof(c128));
+    work.ensure(chol_tile_scratch_bytes(dim_pad));
+    nv.ensure(sizeof(double));
+    if (dim_pad != int(P)) {
+        exact_pad_kernel<<<std::min(148u * 8, cdiv_u(dp * dp, 256)), 256, 0, st>>>(G.as<c128>(), int(P), dim_pad);
+        YQ_LAUNCH_CHECK();
+    }
+    double stats[2];
+    exact_summation(q, H, kind, nup, stats, oloc.as<c128>(), grad.as<c128>(), G.as<c128>(), dp, shift);
+    chol_factor_tiled(G.as<c128>(), dim_pad, dp, Li.as<c128>(), LiH.as<c128>(), ctx->status.as<int>(), work.p,
+                      ctx->sm_count, st);
+    YQ_CUDA(cudaMemsetAsync(b.p, 0, dp * sizeof(c128), st));
+    YQ_CUDA(cudaMemcpyAsync(b.p, grad.p, P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+    chol_solve_tiled(G.as<c128>(), dim_pad, dp, Li.as<c128>(), LiH.as<c128>(), b.as<c128>(), x.as<c128>(),
+                     ctx->status.as<int>(), work.p, ctx->sm_count, st);
+    exact_update_kernel<<<1, 1024, 0, st>>>(P, lr, x.as<c128>(), q->p64.as<c128>(), nv.as<double>());
+    YQ_LAUNCH_CHECK();
+    q->version++;
+    double h = 0.;
+    YQ_CUDA(cudaMemcpyAsync(&h, nv.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    YQ_CUDA(cudaStreamSynchronize(st));
+    out[0] = stats[0];
+    out[1] = stats[1];
+    out[2] = h;
 }
 
 void sampler_sample_exact(yq_sampler_s* S, int ns, uint64_t seed, uint32_t epoch, uint64_t* d_pos) {

@@ -27,6 +27,7 @@ struct yq_ctx_s {
     yq::DevBuf status;  // int device status word
     yq::DevBuf scratch; // small reduction scratch (doubles)
     bool timing = true; // stage events recorded (off while a batch graph is captured)
+    void* noalloc_scratch = nullptr;  // device address of the no-allocation entry point's array
 
     void stage_begin(int s);
     void stage_end(int s);
@@ -139,6 +140,14 @@ struct yq_sr_s {
     yq::DevBuf xh, xl, yh, yl;
     yq::DevBuf gram_ws;  // FP32 partials of the Gram's K-split tiles
     double host_stats[8] = {};
+    // RunRBM's exponential averages of the gradient (beta1) and of the Fisher
+    // matrix (beta2) and its update clip (Runners/RunRBM.hpp:13-37, 73-82, 181-209),
+    // applied by yq_vmc_iteration only; t_* count the ObsAvg updates
+    double beta1 = 0., beta2 = 0., grad_clip = 0.;
+    long t_grad = 0, t_fisher = 0;
+    yq::DevBuf gavg, gused;  // P c128: running average and the bias-corrected gradient
+    yq::DevBuf favg;         // dim_pad x dim_pad c128 running Fisher average (S-form)
+    yq::DevBuf trhs;         // ns c128: right-hand side of a T-form solve with a given gradient
 };
 
 // A batch of SR problems advanced together (batch.cu).
@@ -173,6 +182,10 @@ void rbm_log_psi(yq_rbm_s* q, int ns, const int8_t* d_sigma, c128* d_out);
 void rbm_log_ratio(yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_theta, int nflip, const int* d_flips,
                    c128* d_out);
 void rbm_log_deriv(yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_theta, c128* d_out);
+void rbm_log_ratio_k(yq_rbm_s* q, int ns, const int8_t* d_sigma, const c128* d_theta, int k, const int* d_flips,
+                     c128* d_out);
+void rbm_log_ratio_states(yq_rbm_s* q, int ns, const int8_t* d_sa, const c128* d_tha, const int8_t* d_sb,
+                          const c128* d_thb, c128* d_out);
 void rbm_init_params_host(int n, int m, bool bias, uint64_t seed, double sd, c128* p);
 
 void sampler_run(yq_sampler_s* S, int n_sweeps, int n_discard, uint64_t seed, uint32_t epoch, int reinit);
@@ -191,13 +204,19 @@ void ham_enumerate(yq_ham_s* H, int ns, const int8_t* d_sigma, int* d_a, int* d_
 void ham_eloc(yq_ham_s* H, yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_theta, c128* d_out);
 
 void sr_construct(yq_sr_s* sr);
+// d_S (optional) receives the lower triangle of S + shift I with leading dimension ldS (0: P)
 void exact_summation(yq_rbm_s* q, yq_ham_s* H, int kind, int nup, double* stats, c128* d_oloc, c128* d_grad,
-                     c128* d_S);
+                     c128* d_S, size_t ldS = 0, double shift = 0.0);
+void exact_iteration(yq_rbm_s* q, yq_ham_s* H, int kind, int nup, double shift, double lr, double* out);
 void sampler_sample_exact(yq_sampler_s* S, int ns, uint64_t seed, uint32_t epoch, uint64_t* d_pos);
 void batch_create(yq_ctx_s* ctx, int np, yq_sr_s* const* srs, yq_batch_s** out);
 void batch_destroy(yq_batch_s* B);
 void batch_iteration(yq_batch_s* B, const yq_iter_params& p, yq_iter_result* res);
 void sr_solve(yq_sr_s* sr, double shift, int solver, double cg_tol, int ir_steps, int* iters, double* relres);
+// RunRBM.hpp:181-203: the solve of one runner epoch with the ObsAvg momentum of
+// the gradient and the Fisher matrix; cg_err = |apply(v) - grad| for the CG branch
+void sr_solve_runner(yq_sr_s* sr, double shift, int solver, double cg_tol, int ir_steps, int* iters, double* relres,
+                     double* cg_err);
 void sr_update_params(yq_sr_s* sr, double lr);
 void sr_form_matrix_public(yq_sr_s* sr, double shift);
 }  // namespace yq

@@ -14,7 +14,6 @@
 // serialised by the caller.  Every partial slot a call reads was written earlier
 // by the same call, so nothing has to be cleared between calls.
 #include <algorithm>
-#include <mutex>
 
 #include "internal.hpp"
 
@@ -26,29 +25,71 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 void record_error(const std::string& msg);  // capi.cu
 
 namespace {
-// Partial sums over a chunk of samples of s_i tanh(theta_j) for i in [0, n]
-// (i = n stands for s := 1, the b block) and j in [0, m] (j = m: t := 1, the a block),
-// with tanh(theta) evaluated in place (the SR object keeps a tanh buffer instead).
+constexpr int TS = 8;  // samples staged per step
+
+// Partial sums over a chunk of samples of s_i t_j, t_j = tanh(theta_j), for rows
+// i in [0, n] and columns j in [0, m]: row i = n (s := 1) sums t_j, the gradient of
+// the hidden bias b_j; column j = m (t := 1) sums s_i, the gradient of the visible
+// bias a_i; the others are the W_ji entries.  A block covers 32 columns x 32 rows
+// (a thread keeps four rows of one column) and stages, for TS samples at a time,
+// tanh(theta) of its 32 columns and sigma of its 32 rows in shared memory, so each
+// tanh is evaluated once per block rather than once per row.
 template <typename R>
-__global__ void oloc_partial_noalloc_kernel(int n, int m, int ns, int chunk, const int8_t* __restrict__ sigma,
-                                            const cplx<R>* __restrict__ theta, c128* __restrict__ part) {
-    const int j = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int i = blockIdx.y * 8 + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(256) oloc_partial_noalloc_kernel(int n, int m, int ns, int chunk,
+                                                                   const int8_t* __restrict__ sigma,
+                                                                   const cplx<R>* __restrict__ theta,
+                                                                   c128* __restrict__ part) {
+    __shared__ double t_re[TS][32], t_im[TS][32];
+    __shared__ double s_v[TS][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int jb = blockIdx.x * 32, ib = blockIdx.y * 32;
+    const int j = jb + lane;
     const int split = blockIdx.z;
-    if (i > n || j > m) return;
     const int s0 = split * chunk, s1 = min(ns, s0 + chunk);
-    double ar = 0., ai = 0.;
-    for (int s = s0; s < s1; ++s) {
-        const double sv = (i < n) ? double(sigma[size_t(s) * n + i]) : 1.0;
-        if (j < m) {
-            const cplx<R> tv = ctanh(theta[size_t(s) * m + j]);
-            ar += sv * double(tv.re);
-            ai += sv * double(tv.im);
-        } else {
-            ar += sv;
+    double ar[4] = {0., 0., 0., 0.}, ai[4] = {0., 0., 0., 0.};
+    for (int sb = s0; sb < s1; sb += TS) {
+        // one (sample, column) tanh and one (sample, row) spin per thread
+        {
+            const int ss = threadIdx.x >> 5, c = threadIdx.x & 31;
+            const int s = sb + ss;
+            double tr = 0., ti = 0., sv = 0.;
+            if (s < s1) {
+                const int jj = jb + c, ii = ib + c;
+                if (jj < m) {
+                    const cplx<R> tv = ctanh(theta[size_t(s) * m + jj]);
+                    tr = double(tv.re);
+                    ti = double(tv.im);
+                } else if (jj == m) {
+                    tr = 1.0;
+                }
+                if (ii < n)
+                    sv = double(sigma[size_t(s) * n + ii]);
+                else if (ii == n)
+                    sv = 1.0;
+            }
+            t_re[ss][c] = tr;
+            t_im[ss][c] = ti;
+            s_v[ss][c] = sv;
         }
+        __syncthreads();
+#pragma unroll
+        for (int ss = 0; ss < TS; ++ss) {
+            const double tr = t_re[ss][lane], ti = t_im[ss][lane];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double sv = s_v[ss][warp * 4 + k];
+                ar[k] += sv * tr;
+                ai[k] += sv * ti;
+            }
+        }
+        __syncthreads();
     }
-    part[size_t(split) * (n + 1) * (m + 1) + size_t(i) * (m + 1) + j] = mk(ar, ai);
+    if (j > m) return;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int i = ib + warp * 4 + k;
+        if (i <= n) part[size_t(split) * (n + 1) * (m + 1) + size_t(i) * (m + 1) + j] = mk(ar[k], ai[k]);
+    }
 }
 
 __global__ void oloc_finish_noalloc_kernel(int n, int m, bool bias, int nsplit, double inv_ns,
@@ -69,20 +110,19 @@ __global__ void oloc_finish_noalloc_kernel(int n, int m, bool bias, int nsplit, 
     }
 }
 
-// Device address of the scratch array, looked up once per device (with that device current).
-void* scratch_address(int device) {
-    static std::mutex mu;
-    static void* addr[64] = {};
-    YQ_CHECK_ARG(device >= 0 && device < 64, "oloc_noalloc: device index out of range");
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[device]) {
+// Device address of the scratch array for this context's device, looked up at the
+// context's first call of the entry point with that device current.  It is kept
+// with the context: a device reset, which ends every context's stream and buffers,
+// cannot leave a stale address behind for a new context.
+void* scratch_address(yq_ctx_s* ctx) {
+    if (!ctx->noalloc_scratch) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             throw Error(YQ_E_CUDA, std::string("oloc_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-        addr[device] = p;
+        ctx->noalloc_scratch = p;
     }
-    return addr[device];
+    return ctx->noalloc_scratch;
 }
 
 template <typename R>
@@ -90,9 +130,9 @@ void oloc_noalloc_t(yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_th
     const int n = q->n, m = q->m;
     const size_t cnt = size_t(n + 1) * (m + 1);
     const size_t cap = NOALLOC_SCRATCH_BYTES / sizeof(c128);
-    dim3 g(cdiv_u(m + 1, 32), cdiv_u(n + 1, 8), 1);
+    dim3 g(cdiv_u(m + 1, 32), cdiv_u(n + 1, 32), 1);
     int nsplit = int(std::min<size_t>(64, cap / cnt));
-    nsplit = std::max(1, std::min(nsplit, ns));
+    nsplit = std::max(1, std::min({nsplit, ns, std::max(1, int((8 * 148) / std::max(1u, g.x * g.y)))}));
     const int chunk = (ns + nsplit - 1) / nsplit;
     g.z = nsplit;
     cudaStream_t st = q->ctx->stream;
@@ -116,8 +156,8 @@ extern "C" int yq_rbm_oloc_noalloc(yq_rbm q, int ns, const int8_t* d_sigma, cons
             throw Error(YQ_E_ARG, "oloc_noalloc: (n + 1) (m + 1) = " + std::to_string(cnt) +
                                       " exceeds the static scratch of 4 MiB (at most 262144 complex partial sums)");
         YQ_CUDA(cudaSetDevice(q->ctx->device));
-        c128* part = static_cast<c128*>(scratch_address(q->ctx->device));
-        rbm_prepare(q);  // refreshes derived arrays allocated when the RBM was created
+        c128* part = static_cast<c128*>(scratch_address(q->ctx));
+        // only sigma and theta are read: the machine's parameters play no part
         if (q->dtype == YQ_C64)
             oloc_noalloc_t<float>(q, ns, d_sigma, d_theta, reinterpret_cast<c128*>(d_oloc), part);
         else

@@ -188,6 +188,68 @@ void rbm_log_ratio(yq_rbm_s* q, int ns, const int8_t* d_sigma, const void* d_the
     YQ_CUDA(cudaStreamSynchronize(q->ctx->stream));
 }
 
+// logRatio(vector) -- States/RBMState.hpp:107-125, k distinct flips per sample, in
+// the reference's form: -2 sum_e a_e s_e + sum_j [logCosh(theta_j - 2 sum_e s_e W_je)
+// - logCosh(theta_j)], evaluated in FP64 from the machine's weights (W in the
+// compute type, m x n column-major; a the FP64 master values).
+template <typename R>
+__global__ void log_ratio_k_kernel(int n, int m, int ns, int k, const int8_t* __restrict__ sigma,
+                                   const c128* __restrict__ theta, const int* __restrict__ flips,
+                                   const cplx<R>* __restrict__ W, const c128* __restrict__ a, c128* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ns) return;
+    const int8_t* sg = sigma + size_t(s) * n;
+    const int* f = flips + size_t(s) * k;
+    c128 res = mk(0., 0.);
+    if (a)
+        for (int e = 0; e < k; ++e) res = res - (2.0 * double(sg[f[e]])) * a[f[e]];
+    for (int j = 0; j < m; ++j) {
+        const c128 th = theta[size_t(s) * m + j];
+        c128 t = th;
+        for (int e = 0; e < k; ++e) t = t - (2.0 * double(sg[f[e]])) * cast<double>(W[size_t(f[e]) * m + j]);
+        res = res + (clogcosh(t) - clogcosh(th));
+    }
+    out[s] = res;
+}
+
+// logRatio(other) -- States/RBMState.hpp:136-149: a^T (s' - s) + sum_j [logCosh(theta'_j)
+// - logCosh(theta_j)] between two states of the same machine.
+__global__ void log_ratio_states_kernel(int n, int m, int ns, const int8_t* __restrict__ sa,
+                                        const c128* __restrict__ tha, const int8_t* __restrict__ sb,
+                                        const c128* __restrict__ thb, const c128* __restrict__ a,
+                                        c128* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ns) return;
+    c128 res = mk(0., 0.);
+    if (a)
+        for (int i = 0; i < n; ++i) res = res + double(sb[size_t(s) * n + i] - sa[size_t(s) * n + i]) * a[i];
+    for (int j = 0; j < m; ++j) res = res + (clogcosh(thb[size_t(s) * m + j]) - clogcosh(tha[size_t(s) * m + j]));
+    out[s] = res;
+}
+
+void rbm_log_ratio_k(yq_rbm_s* q, int ns, const int8_t* d_sigma, const c128* d_theta, int k, const int* d_flips,
+                     c128* d_out) {
+    if (ns <= 0) return;
+    rbm_prepare(q);
+    const c128* a = q->use_bias ? q->p64.as<c128>() + size_t(q->n) * q->m : nullptr;
+    if (q->dtype == YQ_C64)
+        log_ratio_k_kernel<float><<<cdiv_u(ns, 64), 64, 0, q->ctx->stream>>>(q->n, q->m, ns, k, d_sigma, d_theta,
+                                                                            d_flips, q->W.as<c64>(), a, d_out);
+    else
+        log_ratio_k_kernel<double><<<cdiv_u(ns, 64), 64, 0, q->ctx->stream>>>(q->n, q->m, ns, k, d_sigma, d_theta,
+                                                                             d_flips, q->W.as<c128>(), a, d_out);
+    YQ_LAUNCH_CHECK();
+}
+
+void rbm_log_ratio_states(yq_rbm_s* q, int ns, const int8_t* d_sa, const c128* d_tha, const int8_t* d_sb,
+                          const c128* d_thb, c128* d_out) {
+    if (ns <= 0) return;
+    const c128* a = q->use_bias ? q->p64.as<c128>() + size_t(q->n) * q->m : nullptr;
+    log_ratio_states_kernel<<<cdiv_u(ns, 64), 64, 0, q->ctx->stream>>>(q->n, q->m, ns, d_sa, d_tha, d_sb, d_thb, a,
+                                                                      d_out);
+    YQ_LAUNCH_CHECK();
+}
+
 // O row = [s_i tanh(theta_j) | s | tanh(theta)] (RBM.hpp:390-406), c128 output.
 __global__ void log_deriv_kernel(int n, int m, bool bias, int ns, const int8_t* __restrict__ sigma,
                                  const c128* __restrict__ theta, c128* __restrict__ out) {

@@ -505,7 +505,10 @@ void sr_construct(yq_sr_s* sr) {
     const int ns = S->ns;
     const size_t P = q->P;
     sr->ns = ns;
-    sr->mode = sr->mode_req == YQ_SR_AUTO ? (size_t(ns) < P ? YQ_SR_T : YQ_SR_S) : sr->mode_req;
+    // AUTO takes the sample-space form when Ns < P, unless the runner averages the
+    // Fisher matrix over iterations (beta2 != 0), which only the S-form can hold
+    sr->mode = sr->mode_req == YQ_SR_AUTO ? ((size_t(ns) < P && sr->beta2 == 0.0) ? YQ_SR_T : YQ_SR_S)
+                                          : sr->mode_req;
     // mixed precision: T-form on the tensor cores; S-form (Ns >= P) with FP32 O~ and FP64 sums
     sr->dim = sr->mode == YQ_SR_T ? ns : int(P);
     sr->dim_pad = ((sr->dim + NB - 1) / NB) * NB;
@@ -650,9 +653,10 @@ static c128 dotc(yq_sr_s* sr, size_t n, const c128* a, const c128* b) {
     return r;
 }
 
-// Eigen::ConjugateGradient<..., Lower|Upper, IdentityPreconditioner> semantics.
+// Eigen::ConjugateGradient<..., Lower|Upper, IdentityPreconditioner> semantics,
+// solving (S + shift) x = b into sr->v.
 template <typename R>
-static void solve_cg_t(yq_sr_s* sr, double shift, double tol, int* iters, double* relres) {
+static void solve_cg_t(yq_sr_s* sr, const c128* b, double shift, double tol, int* iters, double* relres) {
     cudaStream_t st = sr->q->ctx->stream;
     const size_t P = sr->q->P;
     DevBuf rb, pb, tb;
@@ -661,7 +665,7 @@ static void solve_cg_t(yq_sr_s* sr, double shift, double tol, int* iters, double
     tb.ensure(P * sizeof(c128));
     c128 *x = sr->v.as<c128>(), *r = rb.as<c128>(), *p = pb.as<c128>(), *tmp = tb.as<c128>();
     YQ_CUDA(cudaMemsetAsync(x, 0, P * sizeof(c128), st));
-    YQ_CUDA(cudaMemcpyAsync(r, sr->grad.as<c128>(), P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+    YQ_CUDA(cudaMemcpyAsync(r, b, P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
     const unsigned g = std::min(148u * 8, cdiv_u(P, 256));
     double rhsNorm2 = dotc(sr, P, r, r).re;
     int it = 0;
@@ -696,20 +700,51 @@ __global__ void residual_kernel(size_t n, const c128* __restrict__ b, const c128
         r[i] = b[i] - ax[i];
 }
 
-template <typename R>
-static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps) {
-    yq_ctx_s* ctx = sr->q->ctx;
-    cudaStream_t st = ctx->stream;
-    const size_t P = sr->q->P;
-    const int ns = sr->ns;
-    ctx->stage_begin(ST_GRAM);
-    form_matrix_t<R>(sr, shift);
-    ctx->stage_end(ST_GRAM);
-    ctx->stage_begin(ST_SOLVE);
-    // Factorisation: the mixed-precision T-form (whose matrix comes from BF16x3
-    // products) uses the panel form with tensor-core trailing updates; everything
-    // else the persistent FP64 tile kernel.  YQ_CHOLESKY=tiled|recursive overrides
-    // (the recursive launch-per-step variant is kept for comparison).
+// v = (g - w) / shift: the Woodbury form of (S + shift)^{-1} g in T-mode, with
+// w = O~^H (T + shift)^{-1} O~ g / Ns (S = O~^H O~ / Ns, T = O~ O~^H / Ns).
+__global__ void woodbury_kernel(size_t P, double inv_shift, const c128* __restrict__ g, const c128* __restrict__ w,
+                                c128* __restrict__ v) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < P; i += size_t(gridDim.x) * blockDim.x)
+        v[i] = inv_shift * (g[i] - w[i]);
+}
+
+// ObsAvg::update (Runners/RunRBM.hpp:26-30): avg = beta avg + (1 - beta) x.
+__global__ void ema_kernel(size_t n, double beta, const c128* __restrict__ x, c128* __restrict__ avg) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        avg[i] = beta * avg[i] + (1.0 - beta) * x[i];
+}
+
+// ObsAvg::getAvg (RunRBM.hpp:32-35): out = avg / denom, denom = 1 - beta^t.
+__global__ void avg_div_kernel(size_t n, double denom, const c128* __restrict__ avg, c128* __restrict__ out) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        out[i] = mk(avg[i].re / denom, avg[i].im / denom);
+}
+
+// fisherAvg.update(corrMat()) and fisher = getAvg() + lambda I (RunRBM.hpp:187-190)
+// on the lower triangle of the padded S-form matrix G (formed without shift; the
+// padding's unit diagonal averages to itself).
+__global__ void fisher_avg_kernel(int dim, int dim_pad, double beta, double denom, double shift, c128* __restrict__ G,
+                                  c128* __restrict__ favg) {
+    const size_t total = size_t(dim_pad) * dim_pad;
+    for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < total; q += size_t(gridDim.x) * blockDim.x) {
+        const int r = int(q / dim_pad), c = int(q % dim_pad);
+        if (c > r) continue;
+        const c128 f = beta * favg[q] + (1.0 - beta) * G[q];
+        favg[q] = f;
+        G[q] = mk(f.re / denom + ((r == c && r < dim) ? shift : 0.0), f.im / denom);
+    }
+}
+
+// The factorisation used for the LLT solves of one SR object.  The mixed-precision
+// T-form (whose matrix comes from BF16x3 products) uses the panel form with
+// tensor-core trailing updates; everything else the persistent FP64 tile kernel.
+// YQ_CHOLESKY=tiled|recursive overrides (the recursive launch-per-step variant is
+// kept for comparison).
+struct LltPlan {
+    bool recursive = false, panels = false;
+};
+
+static LltPlan llt_plan(const yq_sr_s* sr) {
     static const int forced = [] {
         const char* e = std::getenv("YQ_CHOLESKY");
         if (!e) return 0;
@@ -717,13 +752,20 @@ static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps) {
         if (std::string(e) == "tiled") return 2;
         return 0;
     }();
-    const bool recursive = forced == 1;
-    const bool panels = forced == 0 && sr->precision == YQ_PREC_MIXED && sr->mode == YQ_SR_T;
+    LltPlan pl;
+    pl.recursive = forced == 1;
+    pl.panels = forced == 0 && sr->precision == YQ_PREC_MIXED && sr->mode == YQ_SR_T;
+    return pl;
+}
+
+static void llt_factor(yq_sr_s* sr, const LltPlan& pl) {
+    yq_ctx_s* ctx = sr->q->ctx;
+    cudaStream_t st = ctx->stream;
     sr->chol_work.ensure(chol_tile_scratch_bytes(sr->dim_pad));
-    if (recursive) {
+    if (pl.recursive) {
         chol_factor(sr->G.as<c128>(), sr->dim_pad, size_t(sr->dim_pad), sr->Linv.as<c128>(), sr->LinvH.as<c128>(),
                     ctx->status.as<int>(), st);
-    } else if (panels) {
+    } else if (pl.panels) {
         sr->chol_planes.ensure(chol_panel_planes_bytes(sr->dim_pad));
         chol_factor_panels(sr->G.as<c128>(), sr->dim_pad, size_t(sr->dim_pad), sr->Linv.as<c128>(),
                            sr->LinvH.as<c128>(), ctx->status.as<int>(), sr->chol_work.p, sr->chol_planes.p,
@@ -732,46 +774,102 @@ static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps) {
         chol_factor_tiled(sr->G.as<c128>(), sr->dim_pad, size_t(sr->dim_pad), sr->Linv.as<c128>(),
                           sr->LinvH.as<c128>(), ctx->status.as<int>(), sr->chol_work.p, ctx->sm_count, st);
     }
+}
+
+// out = (L L^H)^{-1} b (b is overwritten; tmp is scratch for the recursive form).
+static void llt_apply(yq_sr_s* sr, const LltPlan& pl, c128* b, c128* tmp, c128* out) {
+    yq_ctx_s* ctx = sr->q->ctx;
     const size_t dp = size_t(sr->dim_pad);
-    const c128* G = sr->G.as<c128>();
-    const c128* Li = sr->Linv.as<c128>();
-    const c128* LiH = sr->LinvH.as<c128>();
-    auto chol_solve = [&](const c128* G_, int n_, size_t ld_, const c128* Li_, const c128* LiH_, c128* b_, c128* tmp_,
-                          c128* out_, cudaStream_t st_) {
-        if (recursive)
-            yq::chol_solve(G_, n_, ld_, Li_, LiH_, b_, tmp_, out_, st_);
-        else
-            chol_solve_tiled(G_, n_, ld_, Li_, LiH_, b_, out_, ctx->status.as<int>(), sr->chol_work.p, ctx->sm_count,
-                             st_);
-    };
+    if (pl.recursive)
+        yq::chol_solve(sr->G.as<c128>(), sr->dim_pad, dp, sr->Linv.as<c128>(), sr->LinvH.as<c128>(), b, tmp, out,
+                       ctx->stream);
+    else
+        chol_solve_tiled(sr->G.as<c128>(), sr->dim_pad, dp, sr->Linv.as<c128>(), sr->LinvH.as<c128>(), b, out,
+                         ctx->status.as<int>(), sr->chol_work.p, ctx->sm_count, ctx->stream);
+}
+
+// T-form: sol = (T + shift)^{-1} rhs (dim_pad entries, zero beyond ns), then
+// ir_steps iterative-refinement steps against the exact operator
+// T y = O~ (O~^H y) / Ns + shift y with FP64 sums.
+template <typename R>
+static void t_solve(yq_sr_s* sr, const LltPlan& pl, double shift, const c128* rhs, c128* sol, int ir_steps) {
+    cudaStream_t st = sr->q->ctx->stream;
+    const size_t dp = size_t(sr->dim_pad);
+    const int ns = sr->ns;
+    c128* b = sr->rhs.as<c128>();
+    c128* tmp = sr->s2.as<c128>();
+    YQ_CUDA(cudaMemcpyAsync(b, rhs, dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+    llt_apply(sr, pl, b, tmp, sol);
+    for (int k = 0; k < ir_steps; ++k) {
+        c128* ty = sr->s3.as<c128>();
+        c128* r = sr->rhs.as<c128>();
+        c128* dy = sr->s4.as<c128>();
+        YQ_CUDA(cudaMemsetAsync(ty, 0, dp * sizeof(c128), st));
+        op_ohy<R>(sr, sol, 1.0, sr->work_p.as<c128>(), nullptr, 0.0);
+        op_ox<R>(sr, sr->work_p.as<c128>(), 1.0 / ns, ty);
+        axpy_kernel<<<cdiv_u(ns, 256), 256, 0, st>>>(size_t(ns), mk(shift, 0.0), sol, ty);
+        residual_kernel<<<cdiv_u(dp, 256), 256, 0, st>>>(dp, rhs, ty, r);
+        YQ_LAUNCH_CHECK();
+        llt_apply(sr, pl, r, tmp, dy);
+        axpy_kernel<<<cdiv_u(dp, 256), 256, 0, st>>>(dp, mk(1.0, 0.0), dy, sol);
+        YQ_LAUNCH_CHECK();
+    }
+}
+
+// solveExact (SRMat.hpp:231-237) or its T-form dual into sr->v.  rhs (P entries)
+// replaces energyGrad() when given; in T-mode it is solved through the Woodbury
+// form (needs shift > 0).  fisher_beta >= 0 averages the S-form matrix into
+// sr->favg before the shift is added (RunRBM.hpp:187-190).
+template <typename R>
+static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps, const c128* rhs = nullptr,
+                        double fisher_beta = -1.0) {
+    yq_ctx_s* ctx = sr->q->ctx;
+    cudaStream_t st = ctx->stream;
+    const size_t P = sr->q->P;
+    const int ns = sr->ns;
+    const bool avg = fisher_beta >= 0.0;
+    ctx->stage_begin(ST_GRAM);
+    form_matrix_t<R>(sr, avg ? 0.0 : shift);
+    if (avg) {
+        const size_t cnt = size_t(sr->dim_pad) * sr->dim_pad;
+        if (sr->t_fisher == 0) {
+            sr->favg.ensure(cnt * sizeof(c128));
+            YQ_CUDA(cudaMemsetAsync(sr->favg.p, 0, cnt * sizeof(c128), st));
+        }
+        ++sr->t_fisher;
+        const double denom = 1.0 - std::pow(fisher_beta, double(sr->t_fisher));
+        fisher_avg_kernel<<<std::min(148u * 16, cdiv_u(cnt, 256)), 256, 0, st>>>(
+            sr->dim, sr->dim_pad, fisher_beta, denom, shift, sr->G.as<c128>(), sr->favg.as<c128>());
+        YQ_LAUNCH_CHECK();
+    }
+    ctx->stage_end(ST_GRAM);
+    ctx->stage_begin(ST_SOLVE);
+    const LltPlan pl = llt_plan(sr);
+    llt_factor(sr, pl);
+    const size_t dp = size_t(sr->dim_pad);
     if (sr->mode == YQ_SR_T) {
-        // y = (T + shift)^{-1} (E - <E>) / Ns ; v = O~^H y   (push-through identity)
-        c128* b = sr->rhs.as<c128>();
-        YQ_CUDA(cudaMemcpyAsync(b, sr->y.as<c128>(), dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
         c128* sol = sr->s1.as<c128>();
-        c128* tmp = sr->s2.as<c128>();
-        chol_solve(G, sr->dim_pad, dp, Li, LiH, b, tmp, sol, st);
-        // iterative refinement against the exact operator (T y = O~ (O~^H y) / Ns + shift y, FP64 sums)
-        for (int k = 0; k < ir_steps; ++k) {
-            c128* ty = sr->s3.as<c128>();
-            c128* r = sr->rhs.as<c128>();
-            c128* dy = sr->s4.as<c128>();
-            YQ_CUDA(cudaMemsetAsync(ty, 0, dp * sizeof(c128), st));
+        if (!rhs) {
+            // y = (T + shift)^{-1} (E - <E>) / Ns ; v = O~^H y   (push-through identity)
+            t_solve<R>(sr, pl, shift, sr->y.as<c128>(), sol, ir_steps);
+            op_ohy<R>(sr, sol, 1.0, sr->v.as<c128>(), nullptr, 0.0);
+        } else {
+            // v = (g - O~^H (T + shift)^{-1} O~ g / Ns) / shift
+            sr->trhs.ensure(dp * sizeof(c128));
+            c128* b = sr->trhs.as<c128>();
+            YQ_CUDA(cudaMemsetAsync(b, 0, dp * sizeof(c128), st));
+            op_ox<R>(sr, rhs, 1.0 / ns, b);
+            t_solve<R>(sr, pl, shift, b, sol, ir_steps);
             op_ohy<R>(sr, sol, 1.0, sr->work_p.as<c128>(), nullptr, 0.0);
-            op_ox<R>(sr, sr->work_p.as<c128>(), 1.0 / ns, ty);
-            axpy_kernel<<<cdiv_u(ns, 256), 256, 0, st>>>(size_t(ns), mk(shift, 0.0), sol, ty);
-            residual_kernel<<<cdiv_u(dp, 256), 256, 0, st>>>(dp, sr->y.as<c128>(), ty, r);
-            YQ_LAUNCH_CHECK();
-            chol_solve(G, sr->dim_pad, dp, Li, LiH, r, tmp, dy, st);
-            axpy_kernel<<<cdiv_u(dp, 256), 256, 0, st>>>(dp, mk(1.0, 0.0), dy, sol);
+            woodbury_kernel<<<cdiv_u(P, 256), 256, 0, st>>>(P, 1.0 / shift, rhs, sr->work_p.as<c128>(),
+                                                           sr->v.as<c128>());
             YQ_LAUNCH_CHECK();
         }
-        op_ohy<R>(sr, sol, 1.0, sr->v.as<c128>(), nullptr, 0.0);
     } else {
         c128* b = sr->rhs.as<c128>();
         YQ_CUDA(cudaMemsetAsync(b, 0, dp * sizeof(c128), st));
-        YQ_CUDA(cudaMemcpyAsync(b, sr->grad.as<c128>(), P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
-        chol_solve(G, sr->dim_pad, dp, Li, LiH, b, sr->s2.as<c128>(), sr->s1.as<c128>(), st);
+        YQ_CUDA(cudaMemcpyAsync(b, rhs ? rhs : sr->grad.as<c128>(), P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+        llt_apply(sr, pl, b, sr->s2.as<c128>(), sr->s1.as<c128>());
         YQ_CUDA(cudaMemcpyAsync(sr->v.as<c128>(), sr->s1.p, P * sizeof(c128), cudaMemcpyDeviceToDevice, st));
     }
     ctx->stage_end(ST_SOLVE);
@@ -783,9 +881,9 @@ void sr_solve(yq_sr_s* sr, double shift, int solver, double cg_tol, int ir_steps
     if (solver == YQ_SOLVE_CG) {
         sr->q->ctx->stage_begin(ST_SOLVE);
         if (sr->q->dtype == YQ_C64)
-            solve_cg_t<float>(sr, shift, cg_tol, iters, relres);
+            solve_cg_t<float>(sr, sr->grad.as<c128>(), shift, cg_tol, iters, relres);
         else
-            solve_cg_t<double>(sr, shift, cg_tol, iters, relres);
+            solve_cg_t<double>(sr, sr->grad.as<c128>(), shift, cg_tol, iters, relres);
         sr->q->ctx->stage_end(ST_SOLVE);
     } else {
         if (sr->q->dtype == YQ_C64)
@@ -798,7 +896,112 @@ void sr_solve(yq_sr_s* sr, double shift, int solver, double cg_tol, int ir_steps
     sr->solved = true;
 }
 
+// |apply(v) - b| (RunRBM.hpp:190: cgErr = (srm.apply(v) - grad).norm()).
+template <typename R>
+static double cg_residual_norm(yq_sr_s* sr, const c128* b, double shift) {
+    cudaStream_t st = sr->q->ctx->stream;
+    const size_t P = sr->q->P;
+    DevBuf rb;
+    rb.ensure(P * sizeof(c128));
+    c128* ax = sr->work_p.as<c128>();
+    c128* r = rb.as<c128>();
+    sr_apply<R>(sr, sr->v.as<c128>(), shift, ax);
+    residual_kernel<<<std::min(148u * 8, cdiv_u(P, 256)), 256, 0, st>>>(P, b, ax, r);
+    YQ_LAUNCH_CHECK();
+    return std::sqrt(dotc(sr, P, r, r).re);
+}
+
+void sr_solve_runner(yq_sr_s* sr, double shift, int solver, double cg_tol, int ir_steps, int* iters, double* relres,
+                     double* cg_err) {
+    if (!sr->constructed) throw Error(YQ_E_STATE, "solve: call construct first");
+    YQ_CHECK_ARG(shift >= 0.0, "solve: shift must be >= 0");
+    *cg_err = 0.;
+    const bool c64 = sr->q->dtype == YQ_C64;
+    const bool use_cg = solver == YQ_SOLVE_CG && sr->beta2 == 0.0;  // RunRBM.hpp:184
+    if (sr->beta2 != 0.0 && sr->mode != YQ_SR_S)
+        throw Error(YQ_E_UNSUPPORTED, "iteration: averaging the Fisher matrix (beta2 != 0) needs the S-form");
+    if (sr->beta1 != 0.0 && sr->mode == YQ_SR_T && !use_cg && !(shift > 0.0))
+        throw Error(YQ_E_ARG, "iteration: gradient momentum in the T-form needs shift > 0");
+    cudaStream_t st = sr->q->ctx->stream;
+    const size_t P = sr->q->P;
+    const unsigned g = std::min(148u * 8, cdiv_u(P, 256));
+    // gradAvg.update(energyGrad()); grad = gradAvg.getAvg()  (RunRBM.hpp:180-181)
+    const c128* rhs = nullptr;
+    auto grad_update = [&] {
+        if (sr->t_grad == 0) {
+            sr->gavg.ensure(P * sizeof(c128));
+            YQ_CUDA(cudaMemsetAsync(sr->gavg.p, 0, P * sizeof(c128), st));
+        }
+        ema_kernel<<<g, 256, 0, st>>>(P, sr->beta1, sr->grad.as<c128>(), sr->gavg.as<c128>());
+        YQ_LAUNCH_CHECK();
+        ++sr->t_grad;
+    };
+    if (sr->beta1 != 0.0) {
+        grad_update();
+        sr->gused.ensure(P * sizeof(c128));
+        avg_div_kernel<<<g, 256, 0, st>>>(P, 1.0 - std::pow(sr->beta1, double(sr->t_grad)), sr->gavg.as<c128>(),
+                                          sr->gused.as<c128>());
+        YQ_LAUNCH_CHECK();
+        rhs = sr->gused.as<c128>();
+    }
+    if (use_cg) {
+        const c128* b = rhs ? rhs : sr->grad.as<c128>();
+        sr->q->ctx->stage_begin(ST_SOLVE);
+        if (c64)
+            solve_cg_t<float>(sr, b, shift, cg_tol, iters, relres);
+        else
+            solve_cg_t<double>(sr, b, shift, cg_tol, iters, relres);
+        *cg_err = c64 ? cg_residual_norm<float>(sr, b, shift) : cg_residual_norm<double>(sr, b, shift);
+        sr->q->ctx->stage_end(ST_SOLVE);
+    } else {
+        if (sr->beta1 != 0.0) grad_update();  // the second gradAvg.update of RunRBM.hpp:186
+        const double fb = sr->beta2 != 0.0 ? sr->beta2 : -1.0;
+        if (c64)
+            solve_llt_t<float>(sr, shift, ir_steps, rhs, fb);
+        else
+            solve_llt_t<double>(sr, shift, ir_steps, rhs, fb);
+        if (iters) *iters = 0;
+        if (relres) *relres = 0.;
+    }
+    sr->solved = true;
+}
+
 void sr_form_matrix_public(yq_sr_s* sr, double shift) { form_matrix(sr, shift); }
+
+// |v| into stats[4] and the clip factor min(1, clip / |v|) into stats[5]
+// (RunRBM.hpp:205-209; clip 0 disables it).
+__global__ void norm_clip_kernel(int nb, double clip, const double* __restrict__ part, double* __restrict__ stats,
+                                 int* __restrict__ status) {
+    double r = 0.;
+    for (int i = 0; i < nb; ++i) r += part[i];
+    const double nv = sqrt(r);
+    stats[4] = nv;
+    stats[5] = (clip != 0.0 && nv > clip) ? clip / nv : 1.0;
+    if (!isfinite(r)) atomicOr(status, DS_NONFINITE);
+}
+
+__global__ void norm_parts_kernel(size_t P, const c128* __restrict__ v, double* __restrict__ part) {
+    __shared__ double red[8];
+    double acc = 0.;
+    for (size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += size_t(gridDim.x) * blockDim.x)
+        acc += v[p].re * v[p].re + v[p].im * v[p].im;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) s += red[w];
+        part[blockIdx.x] = s;
+    }
+}
+
+__global__ void clipped_update_kernel(size_t P, double lr, const double* __restrict__ stats,
+                                      const c128* __restrict__ v, c128* __restrict__ p64) {
+    const double s = lr * stats[5];
+    for (size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += size_t(gridDim.x) * blockDim.x)
+        p64[p] = p64[p] - s * v[p];
+}
 
 void sr_update_params(yq_sr_s* sr, double lr) {
     if (!sr->solved) throw Error(YQ_E_STATE, "update: call solve first");
@@ -806,11 +1009,21 @@ void sr_update_params(yq_sr_s* sr, double lr) {
     cudaStream_t st = ctx->stream;
     ctx->stage_begin(ST_UPDATE);
     const int blocks = 148;
-    update_kernel<<<blocks, 256, 0, st>>>(sr->q->P, lr, sr->v.as<c128>(), sr->q->p64.as<c128>(),
-                                          ctx->scratch.as<double>());
-    finish_norm_kernel<<<1, 1, 0, st>>>(blocks, ctx->scratch.as<double>(), sr->stats.as<double>(),
-                                        ctx->status.as<int>());
-    YQ_LAUNCH_CHECK();
+    if (sr->grad_clip == 0.0) {
+        update_kernel<<<blocks, 256, 0, st>>>(sr->q->P, lr, sr->v.as<c128>(), sr->q->p64.as<c128>(),
+                                              ctx->scratch.as<double>());
+        finish_norm_kernel<<<1, 1, 0, st>>>(blocks, ctx->scratch.as<double>(), sr->stats.as<double>(),
+                                            ctx->status.as<int>());
+        YQ_LAUNCH_CHECK();
+    } else {
+        // |v| first, then the update scaled by the clip factor (device-side, no host round trip)
+        norm_parts_kernel<<<blocks, 256, 0, st>>>(sr->q->P, sr->v.as<c128>(), ctx->scratch.as<double>());
+        norm_clip_kernel<<<1, 1, 0, st>>>(blocks, sr->grad_clip, ctx->scratch.as<double>(), sr->stats.as<double>(),
+                                          ctx->status.as<int>());
+        clipped_update_kernel<<<blocks, 256, 0, st>>>(sr->q->P, lr, sr->stats.as<double>(), sr->v.as<c128>(),
+                                                      sr->q->p64.as<c128>());
+        YQ_LAUNCH_CHECK();
+    }
     sr->q->version++;
     ctx->stage_end(ST_UPDATE);
 }
