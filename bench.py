@@ -15,7 +15,9 @@ the sample-space form T = O~ O~^H / Ns + 1e-3 I (Ns < P), Cholesky, SGD lr 0.01.
 
 --impl reference times the CPU restatement of the reference path (OpenMP
 oracle + numpy BLAS/LAPACK for the dense algebra) on a bounded sample of the
-same workload and extrapolates to one iteration.
+same workload per step and extrapolates each piece to one iteration (the line
+says so field by field); --impl reference --cpu-full-iteration times one whole
+iteration beside that estimate.
 """
 from __future__ import annotations
 
@@ -187,56 +189,111 @@ def _run_precision(api, ctx, precision, steps, warmup, pg, device, with_e2e):
     return out
 
 
-def cpu_sample(steps=1, warmup=0):
-    """Reference CPU path (oracle restatement + numpy BLAS/LAPACK) on a bounded
-    sample of the workload, extrapolated to one full iteration.  Returns
-    (iterations/s, cores, description)."""
+def _cpu_iteration_pieces(orc, rep, cores, full):
+    """One iteration of the reference path on the host cores -- the oracle's
+    restated SamplerMT / Energy / constructDelta (C++, OpenMP over chains and
+    samples) and numpy BLAS/LAPACK for T = O~ O~^H / Ns, its Cholesky and the two
+    triangular solves, v = O~^H y -- either whole (full=True) or as a bounded
+    sample whose pieces are scaled to the whole iteration.  Returns {piece:
+    {"timed": what ran, "s": measured seconds, "scale": factor to one iteration}}."""
     import numpy as np
+    import scipy.linalg as sla
 
+    n = W["lx"] * W["ly"]
+    m = W["alpha"] * n
+    Ns = W["chains"] * W["n_sweeps"]
+    ham = orc.Ham.tfi2d(W["lx"], W["ly"], W["J"], W["h"])
+    p = orc.init_params(n, m, W["seed"], W["init_sd"])
+    # the sample keeps every host thread busy for about eight chains each, and the
+    # zgemm block large enough to run near the full product's efficiency
+    ch = W["chains"] if full else min(W["chains"], max(64, 8 * cores))
+    no = Ns if full else 1024
+    nb = Ns if full else 1024
+    nc = Ns if full else 2048
+    out = {}
+    t = time.perf_counter()
+    s, th, _, _ = orc.sample(n, m, p, ch, seed=W["seed"], epoch=rep, n_sweeps=W["n_sweeps"],
+                             n_discard=W["n_discard"], nthreads=cores)
+    out["sample"] = {"timed": f"{ch} chains x {W['n_discard'] + W['n_sweeps']} sweeps",
+                     "s": time.perf_counter() - t, "scale": W["chains"] / ch}
+    t = time.perf_counter()
+    e = orc.eloc(ham, m, p, s, th, nthreads=cores)
+    out["eloc"] = {"timed": f"{len(s)} samples", "s": time.perf_counter() - t, "scale": Ns / len(s)}
+    rows = np.resize(np.arange(len(s)), no)  # sample rows reused when the sample has fewer than `no`
+    t = time.perf_counter()
+    O = orc.logderiv_rows(n, m, p, s[rows], th[rows], nthreads=cores)
+    Oc = O - O.mean(axis=0)
+    out["O"] = {"timed": f"{no} logDeriv rows + centring", "s": time.perf_counter() - t, "scale": Ns / no}
+    del O
+    A = Oc[:nb] if nb <= no else np.resize(Oc, (nb, Oc.shape[1]))
+    t = time.perf_counter()
+    T = A @ A.conj().T / Ns
+    out["T"] = {"timed": f"{nb} x {nb} block of T (zgemm, K = {A.shape[1]})", "s": time.perf_counter() - t,
+                "scale": (Ns / nb) ** 2}
+    if full:
+        G = T
+        G[np.diag_indices(Ns)] += W["shift"]
+        y0 = (e - e.mean()) / Ns
+    else:
+        X = np.random.default_rng(0).normal(size=(nc, nc)) + 1j * np.random.default_rng(1).normal(size=(nc, nc))
+        G = X @ X.conj().T / nc + np.eye(nc)
+        y0 = np.ones(nc, np.complex128)
+    t = time.perf_counter()
+    L = np.linalg.cholesky(G)
+    out["cholesky"] = {"timed": f"{nc} x {nc} Cholesky", "s": time.perf_counter() - t, "scale": (Ns / nc) ** 3}
+    t = time.perf_counter()
+    y = sla.solve_triangular(L, y0, lower=True)
+    y = sla.solve_triangular(L, y, lower=True, trans="C")
+    out["solve"] = {"timed": f"two {nc} x {nc} triangular solves", "s": time.perf_counter() - t,
+                    "scale": (Ns / nc) ** 2}
+    t = time.perf_counter()
+    v = A.conj().T @ (y[:nb] if nb <= len(y) else np.resize(y, nb))
+    out["update"] = {"timed": f"O~^H y over {nb} rows", "s": time.perf_counter() - t, "scale": Ns / nb}
+    del T, G, L, Oc, A, v
+    return out
+
+
+def _cpu_estimate(pieces):
+    return sum(x["s"] * x["scale"] for x in pieces.values())
+
+
+def cpu_sample(steps=1, warmup=0):
+    """Reference CPU path on the host cores: every step times the bounded sample of
+    one iteration (_cpu_iteration_pieces) and scales each piece to the whole
+    iteration.  Returns (estimated iterations/s, cores, description, measured
+    seconds per step, the last step's pieces)."""
     from oracle import pyoracle as orc
 
     orc.build()
-    n = W["lx"] * W["ly"]
-    m = W["alpha"] * n
-    P = n * m + n + m
-    Ns = W["chains"] * W["n_sweeps"]
     cores = os.cpu_count() or 1
-    ham = orc.Ham.tfi2d(W["lx"], W["ly"], W["J"], W["h"])
-    p = orc.init_params(n, m, W["seed"], W["init_sd"])
-    ch = max(cores, 16)
-    nb, nc = 512, 2048
-    times = []
+    est, wall = [], []
+    pieces = None
     for rep in range(warmup + steps):
         t = time.perf_counter()
-        s, th, _, _ = orc.sample(n, m, p, ch, seed=W["seed"], epoch=rep, n_sweeps=W["n_sweeps"],
-                                 n_discard=W["n_discard"], nthreads=cores)
-        t_samp = (time.perf_counter() - t) * (W["chains"] / ch)
-        t = time.perf_counter()
-        e = orc.eloc(ham, m, p, s, th, nthreads=cores)
-        t_eloc = (time.perf_counter() - t) * (Ns / len(s))
-        t = time.perf_counter()
-        O = np.array([orc.logderiv(n, m, p, a, b) for a, b in zip(s[:64], th[:64])])
-        t_o = (time.perf_counter() - t) * (Ns / 64)
-        A = np.tile(O, (nb // 64, 1)) - O.mean(0)
-        t = time.perf_counter()
-        Tb = A @ A.conj().T / Ns
-        t_t = (time.perf_counter() - t) * ((Ns * Ns / 2) / (nb * nb))
-        X = np.random.default_rng(0).normal(size=(nc, nc)) + 1j * np.random.default_rng(1).normal(size=(nc, nc))
-        G = X @ X.conj().T / nc + np.eye(nc)
-        t = time.perf_counter()
-        np.linalg.cholesky(G)
-        t_c = (time.perf_counter() - t) * (Ns / nc) ** 3
-        t = time.perf_counter()
-        A.conj().T @ np.ones(nb)
-        t_v = (time.perf_counter() - t) * (Ns / nb) * 2
-        tot = t_samp + t_eloc + t_o + t_t + t_c + t_v
+        pieces = _cpu_iteration_pieces(orc, rep, cores, full=False)
         if rep >= warmup:
-            times.append(tot)
-        del Tb
-    sample = (f"{ch} chains x {W['n_discard'] + W['n_sweeps']} sweeps, E_loc on {ch * W['n_sweeps']} samples, "
-              f"O on 64 rows, a {nb}x{nb} block of T and a {nc}x{nc} Cholesky timed, each scaled to the "
-              f"Ns={Ns}, P={P} iteration; OpenMP oracle + numpy BLAS")
-    return 1.0 / statistics.mean(times), cores, sample
+            wall.append(time.perf_counter() - t)
+            est.append(_cpu_estimate(pieces))
+    sample = ("each step times a bounded sample of one Ns = 8192 iteration and scales every piece to it: " +
+              "; ".join(f"{k}: {v['timed']} x {v['scale']:.4g}" for k, v in pieces.items()) +
+              " (OpenMP oracle restatement + numpy BLAS/LAPACK; the whole-iteration estimate is checked against one "
+              "fully measured iteration in profiles/cpu_iteration_tfi2d12x12.md)")
+    return 1.0 / statistics.mean(est), cores, sample, statistics.mean(wall), pieces
+
+
+def cpu_full_iteration():
+    """One whole reference iteration on the host cores (no scaling) beside the
+    bounded-sample estimate of the same host: the check of the extrapolation."""
+    from oracle import pyoracle as orc
+
+    orc.build()
+    cores = os.cpu_count() or 1
+    est = _cpu_estimate(_cpu_iteration_pieces(orc, 0, cores, full=False))
+    t = time.perf_counter()
+    full = _cpu_iteration_pieces(orc, 0, cores, full=True)
+    total = time.perf_counter() - t
+    return {"cores": cores, "full_iteration_s": total, "full_pieces_s": {k: v["s"] for k, v in full.items()},
+            "estimate_s": est, "estimate_over_measured": est / total}
 
 
 def suite(api, ctx, hbm_gbs):
@@ -447,6 +504,8 @@ def main():
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-suite", action="store_true", help="skip the secondary workloads")
+    ap.add_argument("--cpu-full-iteration", action="store_true",
+                    help="with --impl reference: time one whole CPU iteration beside the bounded-sample estimate")
     args = ap.parse_args()
     ws, rank, lrank, pg = _dist()
     warmup = max(3, args.warmup)
@@ -454,12 +513,22 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        v, cores, sample = cpu_sample(steps=args.steps, warmup=warmup)
+        if args.cpu_full_iteration:
+            print(json.dumps({"impl": "reference", "workload": W["workload"], **cpu_full_iteration()}))
+            return
+        v, cores, sample, step_s, pieces = cpu_sample(steps=args.steps, warmup=warmup)
         print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": 0,
-                          "steps": args.steps, "warmup": warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
-                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "steps": args.steps, "warmup": warmup, "ms_per_step": 1e3 * step_s,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic",
                           "config": {"workload": W["workload"], "Ns": W["chains"] * W["n_sweeps"],
                                      "chains": W["chains"], "inputs": "larger than L2"},
+                          "extrapolated": {"value_is": "whole-iteration rate estimated from each step's bounded "
+                                                       "sample; ms_per_step is the measured time of one step",
+                                           "estimate_ms_per_iteration": 1e3 / v,
+                                           "pieces": {k: {"timed": x["timed"], "ms": 1e3 * x["s"],
+                                                          "scale": x["scale"]} for k, x in pieces.items()},
+                                           "check": "profiles/cpu_iteration_tfi2d12x12.md"},
                           "cpu_baseline": {"value": v, "unit": "iters/s", "cores": cores, "kind": "port",
                                            "sample": sample},
                           "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
@@ -522,7 +591,7 @@ def main():
     if not args.no_suite:
         line["suite"] = suite(api, ctx, peaks.get("hbm_gbs", 6553.9))
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_sample(steps=1, warmup=0)
+        v, cores, sample, _, _ = cpu_sample(steps=1, warmup=0)
         line["cpu_baseline"] = {"value": v, "unit": "iters/s", "cores": cores, "kind": "port", "sample": sample}
     ctx.close()
     if rank == 0:

@@ -124,3 +124,33 @@ def test_mixed_panel_cholesky_matches_fp64(ctx, orc, chains, sweeps):
     assert err < TOL_V, err
     for x in (sr, S, H, q):
         x.close()
+
+
+# S-form of the complex64 machine (Ns >= P): the centred O~ rows of the complex64
+# writer (32 bytes per thread; P = 152 even, 175 odd) feed the FP64-accumulating
+# Gram; S and F against numpy products of the oracle's FP64 rows.
+@pytest.mark.parametrize("n,m,chains", [(8, 16, 48), (10, 15, 40)])
+def test_complex64_s_form_matches_oracle(ctx, orc, n, m, chains):
+    from yannq_b200 import api
+
+    p = orc.init_params(n, m, 8, 0.1)
+    s, th, _, _ = orc.sample(n, m, p, chains, seed=5, n_sweeps=8, n_discard=20)
+    q = api.RBM(ctx, n, m, True, api.C64)
+    q.set_params(p)
+    H = api.Hamiltonian.tfi(ctx, n, -1.0, -1.0)
+    S = api.Sampler(q, chains)
+    S.put_samples(s, th)
+    sr = api.SR(q, H, S, api.SR_S, api.PREC_MIXED)
+    sr.construct()
+    O = orc.logderiv_rows(n, m, p, s, th)
+    Oc = O - O.mean(0)
+    e = orc.eloc(orc.Ham.tfi(n, -1.0, -1.0), m, p, s, th)
+    F = Oc.conj().T @ (e - e.mean()) / len(s)
+    Sm = Oc.conj().T @ Oc / len(s)
+    got_F = sr.get(2, q.dim)
+    assert np.max(np.abs(got_F - F)) / np.max(np.abs(F)) < 5e-5
+    got_S = sr.matrix()
+    low = np.tril_indices(q.dim)
+    assert np.max(np.abs(got_S[low] - Sm[low])) / np.max(np.abs(Sm)) < 5e-6
+    for x in (sr, S, H, q):
+        x.close()

@@ -115,12 +115,28 @@ __global__ void ff_adjoint_kernel(FFDims d, int batch, const float* __restrict__
     for (int e = tid; e < nsb * d.F; e += nt) s_z2[e] = tanhf(s_z2[e]);  // d2 = 1 * tanh(z2)
     for (int e = tid; e < nsb * d.LC; e += nt) s_a1[e] = logcoshf_ref(s_z1[e]);
     __syncthreads();
-    // FullyConnected.hpp:170-172: der_w = a1 d2^T, column-major (LC x F) after the conv block
-    for (int s = 0; s < nsb; ++s) {
-        float* row = O + size_t(b0 + s) * d.P + d.KC;
-        for (int e = tid; e < d.LC * d.F; e += nt) {
-            const int o = e / d.LC, i = e % d.LC;
-            row[e] = s_a1[s * d.LC + i] * s_z2[s * d.F + o];
+    // FullyConnected.hpp:170-172: der_w = a1 d2^T, column-major (LC x F) after the conv block.
+    // With KC, LC and P multiples of 4 the block is written as aligned float4 runs
+    // of a1 (one 16-byte store per thread and step); otherwise one float at a time.
+    if ((d.KC & 3) == 0 && (d.LC & 3) == 0 && (d.P & 3) == 0) {
+        const int lc4 = d.LC >> 2, tot4 = lc4 * d.F;
+        const float4* a14 = reinterpret_cast<const float4*>(s_a1);
+        for (int e = tid; e < tot4; e += nt) {
+            const int o = e / lc4, i4 = e - o * lc4;
+            for (int s = 0; s < nsb; ++s) {
+                const float4 a = a14[s * lc4 + i4];
+                const float g = s_z2[s * d.F + o];
+                *reinterpret_cast<float4*>(O + size_t(b0 + s) * d.P + d.KC + size_t(4) * e) =
+                    make_float4(a.x * g, a.y * g, a.z * g, a.w * g);
+            }
+        }
+    } else {
+        for (int s = 0; s < nsb; ++s) {
+            float* row = O + size_t(b0 + s) * d.P + d.KC;
+            for (int e = tid; e < d.LC * d.F; e += nt) {
+                const int o = e / d.LC, i = e % d.LC;
+                row[e] = s_a1[s * d.LC + i] * s_z2[s * d.F + o];
+            }
         }
     }
     // d1 = W d2, then the LnCosh Jacobian: dz1 = d1 * tanh(z1) (in place of z1)

@@ -103,6 +103,62 @@ __device__ __forceinline__ R warp_allsum(R v) {
     return v;
 }
 
+// The proposal draws of one chain, 32 at a time: lane l evaluates the Philox
+// block of proposal 32 b + l once, and proposal g reads its four words from lane
+// g mod 32 -- the same values as one draw(seed, g, ...) per proposal, at 1/32 of
+// the Philox rounds.  The block index only changes with g, so it is warp-uniform.
+struct DrawCache {
+    uint32_t blk = 0xffffffffu;
+    U4 mine;
+    __device__ __forceinline__ U4 get(uint64_t seed, uint32_t g, uint32_t epoch, uint32_t chain, int lane) {
+        const uint32_t b = g >> 5;
+        if (b != blk) {
+            blk = b;
+            mine = draw(seed, (b << 5) + uint32_t(lane), epoch, chain, TAG_SWEEP);
+        }
+        const int src = int(g & 31u);
+        U4 r;
+        r.x = __shfl_sync(0xffffffffu, mine.x, src);
+        r.y = __shfl_sync(0xffffffffu, mine.y, src);
+        r.z = __shfl_sync(0xffffffffu, mine.z, src);
+        r.w = __shfl_sync(0xffffffffu, mine.w, src);
+        return r;
+    }
+};
+
+// Per-unit arithmetic of the complex64 sampler.  Its products, logs and the
+// acceptance exponential feed only the Metropolis comparison u < p and the
+// incremental tanh update, so the single-precision hardware approximations
+// (MUFU log2 / exp2, correctly rounded reciprocal) replace the accurate library
+// forms; the complex128 path keeps the accurate ones (draw-for-draw parity with the
+// FP64 reference restatement).
+template <typename R>
+__device__ __forceinline__ R sampler_log(R x) {
+    return log(x);
+}
+template <>
+__device__ __forceinline__ float sampler_log<float>(float x) {
+    return __logf(x);
+}
+template <typename R>
+__device__ __forceinline__ R sampler_exp(R x) {
+    return exp(x);
+}
+template <>
+__device__ __forceinline__ float sampler_exp<float>(float x) {
+    return __expf(x);
+}
+// a / b for the tanh update (b = the unit's factor, away from 0 by the cancellation guard)
+template <typename R>
+__device__ __forceinline__ cplx<R> sampler_div(cplx<R> a, cplx<R> b) {
+    return cdiv(a, b);
+}
+template <>
+__device__ __forceinline__ cplx<float> sampler_div<float>(cplx<float> a, cplx<float> b) {
+    const float r = __frcp_rn(b.re * b.re + b.im * b.im);
+    return mk((a.re * b.re + a.im * b.im) * r, (a.im * b.re - a.re * b.im) * r);
+}
+
 template <typename R>
 struct LogGroup {
     static constexpr int G = 8;
@@ -199,7 +255,8 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     // (register pipelining for complex64 only: complex128 would spill)
     constexpr bool REGPIPE = MOVE == YQ_MOVE_LOCAL && sizeof(R) == 4;
     constexpr bool HAMMOVE = MOVE == YQ_MOVE_HAMILTONIAN;  // proposals depend on the state: nothing ahead
-    U4 xcur = draw(A.seed, uint32_t(A.sw0) * L, epoch, uint32_t(c), TAG_SWEEP);
+    DrawCache dc;
+    U4 xcur = dc.get(A.seed, uint32_t(A.sw0) * L, epoch, uint32_t(c), lane);
     cplx<R> tvn[JPL], wvn[JPL];
     double lkn = 0., abn = 0.;
     auto load_cols = [&](int kq) {
@@ -230,7 +287,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
         for (uint32_t p = 0; p < L; ++p) {
             const uint32_t g = uint32_t(A.sw0 + sw) * L + p;
             const U4 x = xcur;
-            const U4 xn = draw(A.seed, g + 1u, epoch, uint32_t(c), TAG_SWEEP);
+            const U4 xn = dc.get(A.seed, g + 1u, epoch, uint32_t(c), lane);
             xcur = xn;
             if (!REGPIPE && !HAMMOVE) {
                 // prefetch the next proposal's columns into L1
@@ -308,7 +365,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 for (int r = 0; r < JPL; ++r) {
                     pr = pr * d[r];
                     if ((r % G) == G - 1 || r == JPL - 1) {
-                        ls += log(norm2(pr));
+                        ls += sampler_log<R>(norm2(pr));
                         pr = mk(R(1), R(0));
                     }
                 }
@@ -316,14 +373,14 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 const double base = lk - 2.0 * double(sk) * ab;
                 const R logr = R(0.5) * ls + R(base);
                 // LocalSweeper.hpp:45-47: p = min(1, exp(beta * 2 * Re logRatio)); accept if u < p
-                if (u < exp(two * bexp * logr) * wfac) {
+                if (u < sampler_exp<R>(two * bexp * logr) * wfac) {
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
                         int j = lane + 32 * r;
                         if (j < m) {
                             const cplx<R> w = REGPIPE ? wv[r] : wk[j];
                             th[r] = th[r] - (two * sk) * w;
-                            t[r] = ((exact >> r) & 1u) ? ctanh(th[r]) : cdiv(t[r] - sk * tv[r], d[r]);
+                            t[r] = ((exact >> r) & 1u) ? ctanh(th[r]) : sampler_div<R>(t[r] - sk * tv[r], d[r]);
                         }
                     }
                     __syncwarp();
@@ -362,7 +419,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 for (int r = 0; r < JPL; ++r) {
                     pr = pr * d[r];
                     if ((r % G) == G - 1 || r == JPL - 1) {
-                        ls += log(norm2(pr));
+                        ls += sampler_log<R>(norm2(pr));
                         pr = mk(R(1), R(0));
                     }
                 }
@@ -372,7 +429,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                     base -= 2.0 * double(sk) * A.p64[size_t(n) * m + k].re +
                             2.0 * double(sl) * A.p64[size_t(n) * m + l].re;
                 const R logr = R(0.5) * ls + R(base);
-                if (u < exp(two * bexp * logr) * wfac) {
+                if (u < sampler_exp<R>(two * bexp * logr) * wfac) {
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
                         int j = lane + 32 * r;
@@ -383,7 +440,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                             th[r] = th[r] + dd;
                             cplx<R> sxy = tx[r] + ty[r];
                             t[r] = ((exact >> r) & 1u) ? ctanh(th[r])
-                                                       : cdiv(t[r] * (one<R>() + tx[r] * ty[r]) - sxy, d[r]);
+                                                       : sampler_div<R>(t[r] * (one<R>() + tx[r] * ty[r]) - sxy, d[r]);
                         }
                     }
                     __syncwarp();

@@ -115,35 +115,72 @@ __global__ void oloc_reduce_kernel(int n, int m, bool bias, int nsplit, double i
 }
 
 // Centred log-derivative rows O~[s, p] = O[s, p] - oloc[p] (GroundState/utils.hpp:12-51 and
-// SRMat.hpp:99-100).  Row-major, P contiguous; two complex values per thread.
+// SRMat.hpp:99-100).  Row-major, P contiguous.  A thread owns two adjacent columns:
+// their place in [s_i t_j | s | t] and their means are resolved once, then the
+// thread walks O_ROWS rows, reading sigma and t from L1/L2 and storing both values
+// at once (one 16-byte store for complex64 rows of even P, two for complex128).
+constexpr int O_ROWS = 16;
 template <typename R>
 __global__ void __launch_bounds__(256) o_writer_kernel(int n, int m, bool bias, size_t P, int ns,
                                                        const int8_t* __restrict__ sigma,
                                                        const cplx<R>* __restrict__ t, const c128* __restrict__ oloc,
                                                        cplx<R>* __restrict__ O) {
+    const size_t p0 = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 2;
+    if (p0 >= P) return;
     const size_t nm = size_t(n) * m;
-    for (int s = blockIdx.y; s < ns; s += gridDim.y)
-    for (size_t p0 = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 2; p0 < P;
-         p0 += size_t(gridDim.x) * blockDim.x * 2) {
+    int kind[2], ci[2], cj[2];  // kind 0: s_i t_j, 1: s_i, 2: t_j, 3: past the row
+    R olr[2], oli[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const size_t p = p0 + e;
+        kind[e] = 3;
+        ci[e] = cj[e] = 0;
+        olr[e] = oli[e] = R(0);
+        if (p < P) {
+            if (p < nm) {
+                kind[e] = 0;
+                ci[e] = int(p / m);
+                cj[e] = int(p - size_t(ci[e]) * m);
+            } else if (p < nm + n) {
+                kind[e] = 1;
+                ci[e] = int(p - nm);
+            } else {
+                kind[e] = 2;
+                cj[e] = int(p - nm - n);
+            }
+            const c128 o = oloc[p];
+            olr[e] = R(o.re);
+            oli[e] = R(o.im);
+        }
+    }
+    const bool pair16 = sizeof(R) == 4 && (P % 2) == 0 && kind[1] != 3;
+    const int groups = (ns + O_ROWS - 1) / O_ROWS;
+    for (int gi = blockIdx.y; gi < groups; gi += gridDim.y)
+    for (int s = gi * O_ROWS, s1 = min(ns, s + O_ROWS); s < s1; ++s) {
         const int8_t* sg = sigma + size_t(s) * n;
         const cplx<R>* ts = t + size_t(s) * m;
-        cplx<R>* row = O + size_t(s) * P;
+        cplx<R> v[2];
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-            size_t p = p0 + e;
-            if (p >= P) break;
-            cplx<R> v;
-            if (p < nm) {
-                int i = int(p / m), j = int(p - size_t(i) * m);
-                R sv = R(sg[i]);
-                v = mk(sv * ts[j].re, sv * ts[j].im);
-            } else if (p < nm + n) {
-                v = mk(R(sg[p - nm]), R(0));
-            } else {
-                v = ts[p - nm - n];
+            cplx<R> x = mk(R(0), R(0));
+            if (kind[e] == 0) {
+                const R sv = R(sg[ci[e]]);
+                const cplx<R> tv = ts[cj[e]];
+                x = mk(sv * tv.re, sv * tv.im);
+            } else if (kind[e] == 1) {
+                x = mk(R(sg[ci[e]]), R(0));
+            } else if (kind[e] == 2) {
+                x = ts[cj[e]];
             }
-            c128 o = oloc[p];
-            row[p] = mk(v.re - R(o.re), v.im - R(o.im));
+            v[e] = mk(x.re - olr[e], x.im - oli[e]);
+        }
+        cplx<R>* row = O + size_t(s) * P;
+        if (pair16) {
+            *reinterpret_cast<float4*>(row + p0) =
+                make_float4(float(v[0].re), float(v[0].im), float(v[1].re), float(v[1].im));
+        } else {
+            row[p0] = v[0];
+            if (kind[1] != 3) row[p0 + 1] = v[1];
         }
     }
 }
@@ -472,7 +509,7 @@ static void construct_t(yq_sr_s* sr) {
         }
     }
     if (!fused) {
-        dim3 g(std::max(1u, std::min(64u, cdiv_u(P, 512))), unsigned(std::min(ns, 65535)));
+        const dim3 g(cdiv_u(P, 512), std::min(65535u, cdiv_u(size_t(ns), O_ROWS)));
         o_writer_kernel<R><<<g, 256, 0, st>>>(n, m, q->use_bias, P, ns, sigma, sr->tanhs.as<cplx<R>>(),
                                               sr->oloc.as<c128>(), sr->O.as<cplx<R>>());
         YQ_LAUNCH_CHECK();

@@ -67,6 +67,61 @@ def _same_samples(api, ctx, qm, Sm, srm):
     return out
 
 
+def steady(api, a):
+    """Steady-state comparison at a converged parameter set.
+
+    An FP64 run of `--pre` iterations from the initial parameters gives p*; then for
+    each of `--pairs` seeds a mixed run and an FP64 run start from p* with the same
+    Philox seed (64 thermalisation sweeps, then the bench's 8 + 8 sweeps per
+    iteration) for `--iters` iterations, and the mean energy per site over the last
+    `--iters - --burn` iterations is taken per run.  The pair differences (mixed -
+    FP64) are independent across seeds, so their mean and standard error resolve a
+    systematic difference below the Monte Carlo noise of a single pair."""
+    ctx = api.Context(0)
+    n = LX * LY
+    q, H_, S, sr = _problem(api, ctx, "fp64", SEED)
+    pre = []
+    for it in range(a.pre):
+        r = sr.iteration(SWEEPS, THERM + DISCARD if it == 0 else DISCARD, SEED, it, SHIFT, LR, reinit=it == 0)
+        pre.append(r.energy / n)
+    pstar = q.get_params()
+    for x in (sr, S, H_, q):
+        x.close()
+    if a.save_params:
+        np.save(a.save_params, pstar.astype(np.complex64))
+    pairs = []
+    for k in range(a.pairs):
+        seed = a.seed + 1000 * k
+        tails = {}
+        for prec in ("mixed", "fp64"):
+            q, H_, S, sr = _problem(api, ctx, prec, SEED)
+            q.set_params(pstar)
+            ir = 2 if prec == "mixed" else 0
+            e = []
+            for it in range(a.iters):
+                r = sr.iteration(SWEEPS, THERM + DISCARD if it == 0 else DISCARD, seed, it, SHIFT, LR,
+                                 reinit=it == 0, ir_steps=ir)
+                e.append(r.energy / n)
+            tail = np.array(e[a.burn:])
+            tails[prec] = float(tail.mean())
+            for x in (sr, S, H_, q):
+                x.close()
+        pairs.append({"seed": seed, "mixed": tails["mixed"], "fp64": tails["fp64"],
+                      "diff": tails["mixed"] - tails["fp64"]})
+    ctx.close()
+    d = np.array([p["diff"] for p in pairs])
+    mx = np.array([p["mixed"] for p in pairs])
+    fp = np.array([p["fp64"] for p in pairs])
+    out = {"workload": "tfi2d_12x12_rbm_alpha2", "mode": "steady", "pre_iterations": a.pre,
+           "pre_energy_per_site_last10": float(np.mean(pre[-10:])), "iterations_per_run": a.iters,
+           "burn_in": a.burn, "pairs": pairs,
+           "mean_diff_per_site": float(d.mean()),
+           "sem_diff_per_site": float(d.std(ddof=1) / np.sqrt(len(d))) if len(d) > 1 else None,
+           "mixed_mean": float(mx.mean()), "mixed_sem": float(mx.std(ddof=1) / np.sqrt(len(mx))) if len(mx) > 1 else None,
+           "fp64_mean": float(fp.mean()), "fp64_sem": float(fp.std(ddof=1) / np.sqrt(len(fp))) if len(fp) > 1 else None}
+    print(json.dumps(out))
+
+
 def main():
     from yannq_b200 import api
 
@@ -74,7 +129,15 @@ def main():
     ap.add_argument("--iters", type=int, default=300)
     ap.add_argument("--every", type=int, default=50)
     ap.add_argument("--seed", type=int, default=SEED, help="parameter and Philox seed of both runs")
+    ap.add_argument("--steady", action="store_true", help="seed pairs at a converged parameter set (see steady())")
+    ap.add_argument("--pre", type=int, default=300, help="--steady: FP64 iterations that reach p*")
+    ap.add_argument("--pairs", type=int, default=36, help="--steady: seed pairs")
+    ap.add_argument("--burn", type=int, default=25, help="--steady: iterations left out of each run's mean")
+    ap.add_argument("--save-params", default="", help="--steady: write p* (complex64 .npy) here")
     a = ap.parse_args()
+    if a.steady:
+        steady(api, a)
+        return
     ctx = api.Context(0)
     n = LX * LY
     runs = {}

@@ -13,6 +13,13 @@ BF16 operand planes 1.4 GB).
 times the complex64 sampler of the same lattice (1024 chains, 8 + 8 local sweeps
 per call, chains kept) at M = 288, 192, 144, 96, 64, 32 hidden units, i.e. 9 down
 to 1 hidden units per lane: device ms of the sample stage, best of three calls.
+
+    python -m yannq_b200.profile_cases --case xxz_o --chains 4096 --sweeps 4 --precision mixed
+
+builds the S-form SR of the kernel-throughput machine (XXZ chain N = 64, Delta = 1,
+Sz = 0, RBM alpha = 4, P = 16,704; neighbour exchanges) on chains x sweeps samples,
+so that the centred O writer (o_writer_kernel) writes a few GB: 16,384 x 16,704
+complex64 = 2.2 GB.
 """
 import argparse
 import os
@@ -25,7 +32,7 @@ def main():
     from yannq_b200 import api
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default="iteration", choices=["iteration", "sampler_scaling"])
+    ap.add_argument("--case", default="iteration", choices=["iteration", "sampler_scaling", "xxz_o"])
     ap.add_argument("--chains", type=int, default=1024)
     ap.add_argument("--sweeps", type=int, default=2)
     ap.add_argument("--discard", type=int, default=8)
@@ -49,6 +56,19 @@ def main():
             S.close()
             q.close()
         ctx.close()
+        return
+    if a.case == "xxz_o":
+        q = api.RBM(ctx, 64, 256, True, api.C64 if a.precision == "mixed" else api.C128)
+        q.init_random(20261203, 0.01)
+        H = api.Hamiltonian.xxz(ctx, 64, 1.0, 1.0, False)
+        S = api.Sampler(q, a.chains, api.MOVE_EXCHANGE_NN, 32)
+        S.sample(a.sweeps, 32, 20261203, 0, True)
+        sr = api.SR(q, H, S, api.SR_S, api.PREC_MIXED if a.precision == "mixed" else api.PREC_FP64)
+        for _ in range(a.iters):
+            sr.construct()
+            print(f"O stage {ctx.stage_ms('O'):.3f} ms for {a.chains * a.sweeps} x {q.dim} samples x parameters")
+        for x in (sr, S, H, q, ctx):
+            x.close()
         return
     q = api.RBM(ctx, n, m, True, api.C64 if a.precision == "mixed" else api.C128)
     q.init_random(20261203, 0.01)
