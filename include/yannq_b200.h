@@ -231,11 +231,16 @@ int yq_sampler_get_samples(yq_sampler S, int8_t* sigma, double* theta);
 int yq_sampler_set_tempering(yq_sampler S, int ntemps);
 /* Ladder slot of every chain (0 = beta 1), n_chains entries. */
 int yq_sampler_get_slots(yq_sampler S, int* slots);
-/* No reference counterpart: chains per CTA (warps per block) that the sampler's
- * autotuner chose for the configuration of the last yq_sample (0 before any).  The
- * choice is timed once per configuration per process (1, 2 or 4); YQ_AUTOTUNE=0
- * in the environment fixes it at 4, YQ_CHAINS_PER_CTA=1, 2 or 4 at that value. */
+/* No reference counterpart: the launch shape that the sampler's autotuner chose
+ * for the configuration of the last yq_sample (0 before any): chains per CTA and
+ * warps per chain.  The choice is timed once per configuration per process among
+ * 1, 2 and 4 chains per CTA with one warp per chain and, for complex64 plain
+ * chains of local or exchange moves, 1 and 2 chains per CTA with two warps per
+ * chain (each warp holding half of the hidden units); YQ_AUTOTUNE=0 in the
+ * environment fixes 4 chains per CTA and one warp per chain, YQ_CHAINS_PER_CTA=1, 2
+ * or 4 and YQ_WARPS_PER_CHAIN=1 or 2 restrict the choice. */
 int yq_sampler_chains_per_cta(yq_sampler S, int* out);
+int yq_sampler_warps_per_chain(yq_sampler S, int* out);
 /* Accepted proposals per chain in the last yq_sample (LocalSweeper::sweep's return). */
 int yq_sampler_get_accepts(yq_sampler S, uint64_t* acc);
 /* Replace the device samples by host ones (for SR on externally supplied samples). */

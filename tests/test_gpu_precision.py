@@ -1,0 +1,99 @@
+"""Precision of the mixed path against the FP64 path and the oracle.
+
+* Reduced lattice (2D TFI 4 x 4, h = 3, the precision workload's model and
+  optimisation at a size the CPU restatement runs; tests/golden/
+  tfi2d4x4_trajectory.json from make_tfi2d4x4_trajectory.py): 300 epochs of the
+  restated RunRBM loop (chains re-randomised every epoch).  The FP64 device run
+  reproduces the oracle's energies epoch by epoch (1e-9 relative) while both runs
+  draw the same samples -- checked over the first 50 epochs -- and the mixed run's
+  mean energy over the last 100 epochs agrees with the oracle's within 4 combined
+  standard errors; both lie above the exact ground energy.
+* Late-run 12 x 12 parameters (tests/golden/tfi2d12x12_late_params.npy: the FP64
+  path's parameters after 300 iterations of the bench workload, complex64): on one
+  and the same 8192-sample set the mixed SR step (complex64 O, BF16x3 tcgen05 T,
+  panel Cholesky, two FP64 refinement steps) against the FP64 SR step: energy per
+  site within 2e-8, force within 1e-4 relative, update within 6e-2 relative (T is
+  ill-conditioned here; the refinement converges to the complex64-O solution).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from yannq_b200 import api
+
+    c = api.Context(0)
+    yield c
+    c.close()
+
+
+def _run(api, ctx, d, prec):
+    n, m = d["n"], d["m"]
+    q = api.RBM(ctx, n, m, True, api.C64 if prec == "mixed" else api.C128)
+    q.init_random(d["seed"], 0.01)
+    H = api.Hamiltonian.tfi2d(ctx, d["lx"], d["ly"], -1.0, -3.0)
+    S = api.Sampler(q, d["chains"])
+    sr = api.SR(q, H, S, api.SR_AUTO, api.PREC_MIXED if prec == "mixed" else api.PREC_FP64)
+    es = [sr.iteration(d["n_sweeps"], d["n_discard"], d["seed"], ll, d["shift"], d["lr"], reinit=True,
+                       ir_steps=2 if prec == "mixed" else 0).energy / n for ll in range(d["epochs"])]
+    for x in (sr, S, H, q):
+        x.close()
+    return np.array(es)
+
+
+def test_reduced_lattice_runs_against_oracle(ctx, orc):
+    from yannq_b200 import api
+
+    with open(os.path.join(HERE, "golden", "tfi2d4x4_trajectory.json")) as f:
+        d = json.load(f)
+    ref = np.array(d["energies"]) / d["n"]
+    e0 = d["ed_energy"] / d["n"]
+    fp = _run(api, ctx, d, "fp64")
+    np.testing.assert_allclose(fp[:50], ref[:50], rtol=1e-9, atol=0)
+    mx = _run(api, ctx, d, "mixed")
+    for run in (fp, mx):
+        tail, rtail = run[-100:], ref[-100:]
+        sem = np.hypot(tail.std(ddof=1), rtail.std(ddof=1)) / np.sqrt(len(tail))
+        assert abs(tail.mean() - rtail.mean()) <= 4 * sem, (tail.mean(), rtail.mean(), sem)
+        assert tail.mean() > e0 - 4 * tail.std(ddof=1) / np.sqrt(len(tail))
+        assert abs(tail.mean() - e0) < 1e-2 * abs(e0)
+
+
+def test_late_run_same_sample_mixed_vs_fp64(ctx, orc):
+    from yannq_b200 import api
+
+    p = np.load(os.path.join(HERE, "golden", "tfi2d12x12_late_params.npy")).astype(np.complex128)
+    n, m, chains = 144, 288, 1024
+    qm = api.RBM(ctx, n, m, True, api.C64)
+    qm.set_params(p)
+    Hm = api.Hamiltonian.tfi2d(ctx, 12, 12, -1.0, -3.0)
+    Sm = api.Sampler(qm, chains)
+    Sm.sample(8, 64, 11, 0, True)
+    srm = api.SR(qm, Hm, Sm, api.SR_T, api.PREC_MIXED)
+    srm.construct()
+    vm, _, _ = srm.solve(1e-3, api.SOLVE_LLT)
+    em, _ = srm.energy()
+    Fm = srm.get(2, qm.dim)
+    sig, _ = Sm.get_samples()
+    qf = api.RBM(ctx, n, m, True, api.C128)
+    qf.set_params(p)
+    Sf = api.Sampler(qf, chains)
+    Sf.put_samples(sig, qf.theta(sig))
+    srf = api.SR(qf, Hm, Sf, api.SR_T, api.PREC_FP64)
+    srf.construct()
+    vf, _, _ = srf.solve(1e-3, api.SOLVE_LLT)
+    ef, _ = srf.energy()
+    Ff = srf.get(2, qf.dim)
+    assert abs(em - ef) / n < 2e-8
+    assert np.linalg.norm(Fm - Ff) / np.linalg.norm(Ff) < 1e-4
+    assert np.linalg.norm(vm - vf) / np.linalg.norm(vf) < 6e-2
+    for x in (srm, srf, Sm, Sf, Hm, qm, qf):
+        x.close()

@@ -118,6 +118,7 @@ SIGNATURES = {
     "yq_sampler_put_samples": [_vp, _i, _vp, _vp],
     "yq_sampler_sample_exact": [_vp, _i, _u64, _u32, _vp],
     "yq_sampler_chains_per_cta": [_vp, _vp],
+    "yq_sampler_warps_per_chain": [_vp, _vp],
     "yq_sampler_set_tempering": [_vp, _i],
     "yq_sampler_get_slots": [_vp, _vp],
     "yq_exact": [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp],
@@ -508,6 +509,11 @@ class Sampler:
         out = np.zeros(self.n_chains, np.int32)
         check(lib().yq_sampler_get_slots(self.h, _p(out)))
         return out
+
+    def warps_per_chain(self):
+        v = C.c_int()
+        check(lib().yq_sampler_warps_per_chain(self.h, C.byref(v)))
+        return v.value
 
     def chains_per_cta(self):
         v = C.c_int()

@@ -805,6 +805,14 @@ int yq_sampler_chains_per_cta(yq_sampler S, int* out) {
     });
 }
 
+int yq_sampler_warps_per_chain(yq_sampler S, int* out) {
+    return guard([&] {
+        need(S, "sampler");
+        need(out, "out");
+        *out = S->warps_per_chain;
+    });
+}
+
 int yq_sampler_sample_exact(yq_sampler S, int ns, uint64_t seed, uint32_t epoch, uint64_t* positions) {
     return guard([&] {
         need(S, "sampler");

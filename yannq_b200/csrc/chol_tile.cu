@@ -85,11 +85,15 @@ __device__ bool wait_flag(const int* flag, const Sync& S, int* s_ok) {
     return *s_ok != 0;
 }
 
-// Publishes a flag after every thread's global writes of the tile.
+// Publishes a flag after every thread's global writes of the tile: the CTA
+// barrier orders them before thread 0's gpu-scope fence, which is cumulative over
+// what the barrier made it observe, and the release store then publishes them.
 __device__ void publish(int* flag) {
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) st_release(flag, 1);
+    if (threadIdx.x == 0) {
+        __threadfence();
+        st_release(flag, 1);
+    }
 }
 
 // c (4 x 4 sub-tiles of the warp's 32 x 32 block) += A B^H over K = 4 * nk,

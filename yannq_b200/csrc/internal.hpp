@@ -89,7 +89,8 @@ struct yq_sampler_s {
     int ns = 0;
     uint64_t proposals = 0;  // per chain, last call
     const uint32_t* epoch_dev = nullptr;  // device epoch offset added to the call's epoch (batched graphs)
-    int chains_per_cta = 0;               // autotuned launch shape of the last sample call
+    int chains_per_cta = 0;               // autotuned launch shape of the last sample call:
+    int warps_per_chain = 0;              //   chains per CTA and warps per chain
     const yq_ham_s* ham = nullptr;        // proposals of YQ_MOVE_HAMILTONIAN
     // parallel tempering (SamplerMT nTmps > 1): chains c = ntemps group + k
     int ntemps = 1;

@@ -159,6 +159,27 @@ __device__ __forceinline__ cplx<float> sampler_div<float>(cplx<float> a, cplx<fl
     return mk((a.re * b.re + a.im * b.im) * r, (a.im * b.re - a.re * b.im) * r);
 }
 
+// Sum of the chain's WPC warp partials (each already a warp butterfly sum), in
+// warp order, through the chain's double-buffered slots at a named barrier of the
+// WPC warps (barrier 0 stays __syncthreads).  A slot pair is rewritten two
+// proposals later, after every warp of the chain has passed the barrier that
+// follows its reads.
+template <typename R, int WPC>
+__device__ __forceinline__ R chain_sum(R v, R* part, int& pbuf, int wchain, int sub, int lane) {
+    if constexpr (WPC == 1) {
+        return v;
+    } else {
+        R* b = part + pbuf * WPC;
+        if (lane == 0) b[sub] = v;
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + wchain), "r"(32 * WPC) : "memory");
+        R t = b[0];
+#pragma unroll
+        for (int w = 1; w < WPC; ++w) t += b[w];
+        pbuf ^= 1;
+        return t;
+    }
+}
+
 template <typename R>
 struct LogGroup {
     static constexpr int G = 8;
@@ -169,11 +190,12 @@ struct LogGroup<float> {
 };
 
 template <typename R, int JPL>
-__device__ __forceinline__ void theta_fp64(const SampArgs<R>& A, const int8_t* s, int lane, cplx<R> (&th)[JPL]) {
+__device__ __forceinline__ void theta_fp64(const SampArgs<R>& A, const int8_t* s, int lane, cplx<R> (&th)[JPL],
+                                           int sub = 0, int wpc = 1) {
     const size_t nm = size_t(A.n) * A.m;
 #pragma unroll
     for (int r = 0; r < JPL; ++r) {
-        const int j = lane + 32 * r;
+        const int j = lane + 32 * (sub + wpc * r);
         if (j < A.m) {
             double ar = 0., ai = 0.;
             for (int i = 0; i < A.n; ++i) {
@@ -194,16 +216,27 @@ __device__ __forceinline__ void theta_fp64(const SampArgs<R>& A, const int8_t* s
     }
 }
 
-template <typename R, int MOVE, int JPL>
-__global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
+// WPC warps per chain: hidden unit j = lane + 32 (sub + WPC r) of the chain's warp
+// `sub`.  With WPC = 2 the two warps draw the same proposals, keep their own copy
+// of sigma, and combine their partial log-sums through shared memory at a named
+// barrier of the pair (one per proposal, double-buffered), adding the two halves
+// in the same order so that both take the same decision.  Only plain chains
+// (no tempering) of local or exchange moves use it.
+template <typename R, int MOVE, int JPL, int WPC>
+__global__ void __launch_bounds__(128, WPC == 2 ? 4 : 1) metropolis_kernel(SampArgs<R> A) {
     extern __shared__ int8_t smem_sig[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (c >= A.n_chains) return;  // warp-uniform
+    const int wchain = warp / WPC, sub = warp - wchain * WPC;
+    const int c = blockIdx.x * ((blockDim.x >> 5) / WPC) + wchain;
+    if (c >= A.n_chains) return;  // uniform over the chain's warps
     const int n = A.n, m = A.m;
     const uint32_t epoch = A.epoch_dev ? A.epoch + *A.epoch_dev : A.epoch;
     int8_t* s = smem_sig + warp * A.nstride;
     int8_t* cs = A.chains + size_t(c) * n;
+    // partial log-sums of the chain's warps: [2 buffers][WPC], after every warp's sigma row
+    R* part = reinterpret_cast<R*>(smem_sig + ((size_t((blockDim.x >> 5)) * A.nstride + 15) & ~size_t(15))) +
+              size_t(wchain) * 2 * WPC;
+    int pbuf = 0;
 
     // ---- chain initialisation (SamplerMT::randomize, Utilities/Utility.hpp:63-88)
     if (A.reinit) {
@@ -234,11 +267,11 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     if (A.theta_in) {
 #pragma unroll
         for (int r = 0; r < JPL; ++r) {
-            const int j = lane + 32 * r;
+            const int j = lane + 32 * (sub + WPC * r);
             th[r] = j < m ? A.theta_in[size_t(c) * m + j] : mk(R(0), R(0));
         }
     } else {
-        theta_fp64<R, JPL>(A, s, lane, th);
+        theta_fp64<R, JPL>(A, s, lane, th, sub, WPC);
     }
 #pragma unroll
     for (int r = 0; r < JPL; ++r) t[r] = ctanh(th[r]);
@@ -262,7 +295,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
     auto load_cols = [&](int kq) {
 #pragma unroll
         for (int r = 0; r < JPL; ++r) {
-            const int j = lane + 32 * r;
+            const int j = lane + 32 * (sub + WPC * r);
             tvn[r] = j < m ? A.tau[size_t(kq) * m + j] : mk(R(0), R(0));
             wvn[r] = j < m ? A.W[size_t(kq) * m + j] : mk(R(0), R(0));
         }
@@ -275,7 +308,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
         const int k0 = int(draw_site(xcur.x, uint32_t(n)));
 #pragma unroll
         for (int r = 0; r < JPL; ++r) {
-            int j = lane + 32 * r;
+            int j = lane + 32 * (sub + WPC * r);
             if (j < m) {
                 prefetch_l1(A.tau + size_t(k0) * m + j);
                 prefetch_l1(A.W + size_t(k0) * m + j);
@@ -295,7 +328,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 int ln = (MOVE == YQ_MOVE_EXCHANGE_ANY) ? int(draw_site(xn.y, uint32_t(n))) : (kn + 1) % n;
 #pragma unroll
                 for (int r = 0; r < JPL; ++r) {
-                    int j = lane + 32 * r;
+                    int j = lane + 32 * (sub + WPC * r);
                     if (j < m) {
                         prefetch_l1(A.tau + size_t(kn) * m + j);
                         prefetch_l1(A.W + size_t(kn) * m + j);
@@ -341,7 +374,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 } else {
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
-                        const int j = lane + 32 * r;
+                        const int j = lane + 32 * (sub + WPC * r);
                         tv[r] = j < m ? A.tau[size_t(k) * m + j] : mk(R(0), R(0));
                     }
                     lk = A.Lk[k].re;
@@ -350,7 +383,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 unsigned exact = 0u;  // bit r: factor r re-evaluated in logcosh form (ratio.cuh)
 #pragma unroll
                 for (int r = 0; r < JPL; ++r) {
-                    int j = lane + 32 * r;
+                    int j = lane + 32 * (sub + WPC * r);
                     if (j < m) {
                         bool ex;
                         d[r] = factor1<R>(t[r], tv[r], sk, th[r], REGPIPE ? &wv[r] : wk + j, ex);
@@ -369,14 +402,14 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                         pr = mk(R(1), R(0));
                     }
                 }
-                ls = warp_allsum(ls);
+                ls = chain_sum<R, WPC>(warp_allsum(ls), part, pbuf, wchain, sub, lane);
                 const double base = lk - 2.0 * double(sk) * ab;
                 const R logr = R(0.5) * ls + R(base);
                 // LocalSweeper.hpp:45-47: p = min(1, exp(beta * 2 * Re logRatio)); accept if u < p
                 if (u < sampler_exp<R>(two * bexp * logr) * wfac) {
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
-                        int j = lane + 32 * r;
+                        int j = lane + 32 * (sub + WPC * r);
                         if (j < m) {
                             const cplx<R> w = REGPIPE ? wv[r] : wk[j];
                             th[r] = th[r] - (two * sk) * w;
@@ -400,7 +433,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 unsigned exact = 0u;
 #pragma unroll
                 for (int r = 0; r < JPL; ++r) {
-                    int j = lane + 32 * r;
+                    int j = lane + 32 * (sub + WPC * r);
                     if (j < m) {
                         tx[r] = sk * tk[j];
                         ty[r] = sl * tl[j];
@@ -423,7 +456,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                         pr = mk(R(1), R(0));
                     }
                 }
-                ls = warp_allsum(ls);
+                ls = chain_sum<R, WPC>(warp_allsum(ls), part, pbuf, wchain, sub, lane);
                 double base = A.Lk[k].re + A.Lk[l].re;
                 if (A.bias)
                     base -= 2.0 * double(sk) * A.p64[size_t(n) * m + k].re +
@@ -432,7 +465,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
                 if (u < sampler_exp<R>(two * bexp * logr) * wfac) {
 #pragma unroll
                     for (int r = 0; r < JPL; ++r) {
-                        int j = lane + 32 * r;
+                        int j = lane + 32 * (sub + WPC * r);
                         if (j < m) {
                             cplx<R> a = wk[j], b = wl[j];
                             // States/RBMState.hpp:261-262: theta += -2 s_k W_k - 2 s_l W_l
@@ -457,23 +490,25 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
         // tempered sampling records after mixChains, in pt_mix_kernel
         if (sw >= A.n_discard && !A.slot) {
             const size_t idx = size_t(sw - A.n_discard) * A.n_chains + c;
-            for (int i = lane; i < n; i += 32) A.out_sigma[idx * n + i] = s[i];
+            if (sub == 0)
+                for (int i = lane; i < n; i += 32) A.out_sigma[idx * n + i] = s[i];
 #pragma unroll
             for (int r = 0; r < JPL; ++r) {
-                int j = lane + 32 * r;
+                int j = lane + 32 * (sub + WPC * r);
                 if (j < m) A.out_theta[idx * m + j] = th[r];
             }
         }
-        if (A.resync > 0 && ((A.sw0 + sw + 1) % A.resync) == 0) theta_fp64<R, JPL>(A, s, lane, th);
+        if (A.resync > 0 && ((A.sw0 + sw + 1) % A.resync) == 0) theta_fp64<R, JPL>(A, s, lane, th, sub, WPC);
 #pragma unroll
         for (int r = 0; r < JPL; ++r) t[r] = ctanh(th[r]);
     }
     __syncwarp();
-    for (int i = lane; i < n; i += 32) cs[i] = s[i];
+    if (sub == 0)
+        for (int i = lane; i < n; i += 32) cs[i] = s[i];
     if (A.theta_out) {
 #pragma unroll
         for (int r = 0; r < JPL; ++r) {
-            const int j = lane + 32 * r;
+            const int j = lane + 32 * (sub + WPC * r);
             if (j < m) A.theta_out[size_t(c) * m + j] = th[r];
         }
     }
@@ -482,7 +517,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
         double lp = 0.;
 #pragma unroll
         for (int r = 0; r < JPL; ++r) {
-            const int j = lane + 32 * r;
+            const int j = lane + 32 * (sub + WPC * r);
             if (j < m) lp += clogcosh(cast<double>(th[r])).re;
         }
         if (A.bias)
@@ -490,7 +525,7 @@ __global__ void __launch_bounds__(128) metropolis_kernel(SampArgs<R> A) {
         lp = warp_allsum(lp);
         if (lane == 0) A.lp_out[c] = lp;
     }
-    if (lane == 0) A.acc[c] = (A.acc_add ? A.acc[c] : 0ull) + nacc;
+    if (lane == 0 && sub == 0) A.acc[c] = (A.acc_add ? A.acc[c] : 0ull) + nacc;
 }
 
 // mixChains (SamplerMT.hpp:120-153) for one group per thread: even slot pairs
@@ -541,53 +576,122 @@ __global__ void pt_reset_kernel(int n_chains, int ntemps, int* __restrict__ slot
     beta[c] = double(ntemps - c % ntemps) / double(ntemps);
 }
 
-template <typename R, int MOVE, int JPL>
+template <typename R, int MOVE, int JPL, int WPC>
 static void launch_w(const SampArgs<R>& A, int warps, cudaStream_t st) {
-    dim3 grid(cdiv_u(A.n_chains, warps));
-    size_t smem = size_t(warps) * A.nstride;
-    metropolis_kernel<R, MOVE, JPL><<<grid, warps * 32, smem, st>>>(A);
+    const int chains_per_cta = warps / WPC;
+    dim3 grid(cdiv_u(A.n_chains, chains_per_cta));
+    const size_t smem = ((size_t(warps) * A.nstride + 15) & ~size_t(15)) + size_t(chains_per_cta) * 2 * WPC * sizeof(R);
+    metropolis_kernel<R, MOVE, JPL, WPC><<<grid, warps * 32, smem, st>>>(A);
     YQ_LAUNCH_CHECK();
 }
 
-// Autotuned chains per CTA (warps per block).  On the first call of a
-// configuration (type, move, hidden units per lane, n, m, chains, sweep length) the
-// kernel runs two sweeps from a scratch copy of the chains into scratch outputs at
-// 1, 2 and 4 chains per CTA (the kernel's launch bound is 128 threads), timed with
-// CUDA events on the library stream after one untimed launch, the candidates taken
-// in turn over two rounds so that a clock still ramping up weighs on all of them
-// alike; the fastest (least of its two times) is kept for the process.  The
-// chains evolve identically whatever the choice (each warp owns one chain and its
-// own Philox counters).  Calls made while the stream is being captured, and
-// YQ_AUTOTUNE=0, use 4; YQ_CHAINS_PER_CTA=1, 2 or 4 fixes the choice.
-constexpr int N_TUNE = 3;
+// Units per lane for WPC warps per chain: the smallest instantiated count that covers m.
+template <typename R, int MOVE, int WPC>
+static void launch_jpl(const SampArgs<R>& A, int warps, cudaStream_t st) {
+    const int need = (A.m + 32 * WPC - 1) / (32 * WPC);
+#define YQ_JPL(J)                                   \
+    if (need <= J) {                                \
+        launch_w<R, MOVE, J, WPC>(A, warps, st);    \
+        return;                                     \
+    }
+    if constexpr (WPC == 1) {
+        YQ_JPL(1) YQ_JPL(2) YQ_JPL(4) YQ_JPL(8) YQ_JPL(9) YQ_JPL(12) YQ_JPL(16) YQ_JPL(32)
+    } else {
+        YQ_JPL(1) YQ_JPL(2) YQ_JPL(3) YQ_JPL(4) YQ_JPL(5) YQ_JPL(6) YQ_JPL(8) YQ_JPL(16)
+    }
+#undef YQ_JPL
+    throw Error(YQ_E_UNSUPPORTED, "sampler: m > 1024 hidden units is not built");
+}
+
+// Launch shape: warps per chain (1, or 2 for complex64 plain chains of local and
+// exchange moves) and warps per block (at most 4, the kernel's launch bound).
+struct Shape {
+    int wpc, warps;
+};
+
+template <typename R, int MOVE>
+static constexpr bool split_ok() {
+    return sizeof(R) == 4 && MOVE != YQ_MOVE_HAMILTONIAN;
+}
+
+template <typename R, int MOVE>
+static void launch_shape(const SampArgs<R>& A, Shape sh, cudaStream_t st) {
+    if constexpr (split_ok<R, MOVE>()) {
+        if (sh.wpc == 2) {
+            launch_jpl<R, MOVE, 2>(A, sh.warps, st);
+            return;
+        }
+    }
+    launch_jpl<R, MOVE, 1>(A, sh.warps, st);
+}
+
+// Autotuned launch shape.  On the first call of a configuration (type, move, n, m,
+// chains, sweep length, tempering) the kernel runs two sweeps from a scratch copy
+// of the chains into scratch outputs in every candidate shape -- 1, 2 and 4 chains
+// per CTA with one warp per chain, and for complex64 plain chains 1 and 2 chains
+// per CTA with two warps per chain -- timed with CUDA events on the library stream
+// after one untimed launch, the candidates taken in turn over two rounds so that a
+// clock still ramping up weighs on all of them alike; the fastest (least of its two
+// times) is kept for the process.  With one warp per chain the chains evolve
+// identically whatever the block shape (each warp owns one chain and its own
+// Philox counters); two warps per chain draw the same proposals and add the two
+// halves of each log-ratio sum, a different rounding of the same sum.  Calls made
+// while the stream is being captured, and YQ_AUTOTUNE=0, use 4 chains per CTA and
+// one warp per chain; YQ_CHAINS_PER_CTA=1, 2 or 4 fixes the chains per CTA (one
+// warp per chain unless YQ_WARPS_PER_CHAIN=2), YQ_WARPS_PER_CHAIN=1 or 2 restricts
+// the candidates to that split.
+constexpr int N_TUNE = 5;
 struct TuneEntry {
-    int warps;
+    Shape shape;
     float ms[N_TUNE];
 };
 static std::mutex g_tune_mu;
 static std::map<std::vector<long long>, TuneEntry> g_tune;
 
-template <typename R, int MOVE, int JPL>
-static int tuned_warps(const SampArgs<R>& A, cudaStream_t st) {
+static int env_int(const char* name) {
+    const char* e = std::getenv(name);
+    return e ? std::atoi(e) : 0;
+}
+
+template <typename R, int MOVE>
+static Shape tuned_shape(const SampArgs<R>& A, cudaStream_t st) {
     static const bool enabled = [] {
         const char* e = std::getenv("YQ_AUTOTUNE");
         return !(e && std::string(e) == "0");
     }();
-    static const int forced = [] {
-        const char* e = std::getenv("YQ_CHAINS_PER_CTA");
-        const int v = e ? std::atoi(e) : 0;
+    static const int forced_cpc = [] {
+        const int v = env_int("YQ_CHAINS_PER_CTA");
         return (v == 1 || v == 2 || v == 4) ? v : 0;
     }();
-    if (forced) return forced;
+    static const int forced_wpc = [] {
+        const int v = env_int("YQ_WARPS_PER_CHAIN");
+        return (v == 1 || v == 2) ? v : 0;
+    }();
+    const bool plain = A.slot == nullptr && A.theta_in == nullptr && A.theta_out == nullptr && A.lp_out == nullptr;
+    const bool can_split = split_ok<R, MOVE>() && plain;
+    Shape cand[N_TUNE];
+    int nc = 0;
+    for (int wpc = 1; wpc <= 2; ++wpc) {
+        if (wpc == 2 && !can_split) continue;
+        if (forced_wpc && wpc != forced_wpc) continue;
+        for (int cpc = 1; cpc <= 4; cpc *= 2) {
+            if (cpc * wpc > 4) continue;
+            if (forced_cpc && cpc != forced_cpc) continue;
+            cand[nc++] = Shape{wpc, cpc * wpc};
+        }
+    }
+    if (nc == 0) cand[nc++] = Shape{1, forced_cpc ? forced_cpc : 4};  // a split the configuration does not take
+    if (nc == 1) return cand[0];
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     YQ_CUDA(cudaStreamIsCapturing(st, &cap));
-    const std::vector<long long> key = {static_cast<long long>(sizeof(R)), MOVE, JPL, A.n, A.m, A.n_chains, A.L};
+    const std::vector<long long> key = {static_cast<long long>(sizeof(R)), MOVE, A.n, A.m, A.n_chains, A.L,
+                                        plain ? 1 : 0};
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune.find(key);
-        if (it != g_tune.end()) return it->second.warps;
+        if (it != g_tune.end()) return it->second.shape;
     }
-    if (!enabled || cap != cudaStreamCaptureStatusNone) return 4;
+    if (!enabled || cap != cudaStreamCaptureStatusNone) return Shape{1, 4};
     // Two sweeps, the last one recorded: the kernel writes recorded sweep sw to
     // rows (sw - n_discard) * n_chains + chain, so the scratch outputs hold
     // (n_total - n_discard) x n_chains rows.
@@ -616,13 +720,12 @@ static int tuned_warps(const SampArgs<R>& A, cudaStream_t st) {
     cudaEvent_t e0, e1;
     YQ_CUDA(cudaEventCreate(&e0));
     YQ_CUDA(cudaEventCreate(&e1));
-    const int cand[N_TUNE] = {1, 2, 4};
-    TuneEntry best{4, {1e30f, 1e30f, 1e30f}};
-    launch_w<R, MOVE, JPL>(T, cand[0], st);  // untimed: caches and clocks
+    TuneEntry best{cand[0], {1e30f, 1e30f, 1e30f, 1e30f, 1e30f}};
+    launch_shape<R, MOVE>(T, cand[0], st);  // untimed: caches and clocks
     for (int round = 0; round < rounds; ++round) {
-        for (int c = 0; c < N_TUNE; ++c) {
+        for (int c = 0; c < nc; ++c) {
             YQ_CUDA(cudaEventRecord(e0, st));
-            launch_w<R, MOVE, JPL>(T, cand[c], st);
+            launch_shape<R, MOVE>(T, cand[c], st);
             YQ_CUDA(cudaEventRecord(e1, st));
             YQ_CUDA(cudaEventSynchronize(e1));
             float t = 0.f;
@@ -631,46 +734,36 @@ static int tuned_warps(const SampArgs<R>& A, cudaStream_t st) {
         }
     }
     float best_ms = 1e30f;
-    for (int c = 0; c < N_TUNE; ++c) {
+    for (int c = 0; c < nc; ++c) {
         if (best.ms[c] < best_ms) {
             best_ms = best.ms[c];
-            best.warps = cand[c];
+            best.shape = cand[c];
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = best;
-    return best.warps;
-}
-
-template <typename R, int MOVE, int JPL>
-static void launch_t(const SampArgs<R>& A, cudaStream_t st, int* chosen) {
-    const int warps = tuned_warps<R, MOVE, JPL>(A, st);
-    if (chosen) *chosen = warps;
-    launch_w<R, MOVE, JPL>(A, warps, st);
+    return best.shape;
 }
 
 template <typename R, int MOVE>
-static void dispatch_jpl(const SampArgs<R>& A, cudaStream_t st, int* chosen) {
-    const int need = (A.m + 31) / 32;
-#define YQ_JPL(J)                                \
-    if (need <= J) {                             \
-        launch_t<R, MOVE, J>(A, st, chosen);     \
-        return;                                  \
-    }
-    YQ_JPL(1) YQ_JPL(2) YQ_JPL(4) YQ_JPL(8) YQ_JPL(9) YQ_JPL(12) YQ_JPL(16) YQ_JPL(32)
-#undef YQ_JPL
-            throw Error(YQ_E_UNSUPPORTED, "sampler: m > 1024 hidden units is not built");
+static void dispatch_shape(const SampArgs<R>& A, cudaStream_t st, int* chains_per_cta, int* warps_per_chain) {
+    const Shape sh = tuned_shape<R, MOVE>(A, st);
+    if (chains_per_cta) *chains_per_cta = sh.warps / sh.wpc;
+    if (warps_per_chain) *warps_per_chain = sh.wpc;
+    launch_shape<R, MOVE>(A, sh, st);
 }
 
 template <typename R>
 static void launch_sweeps(yq_sampler_s* S, const SampArgs<R>& A, cudaStream_t st) {
+    int* cpc = &S->chains_per_cta;
+    int* wpc = &S->warps_per_chain;
     switch (S->move) {
-        case YQ_MOVE_LOCAL: dispatch_jpl<R, YQ_MOVE_LOCAL>(A, st, &S->chains_per_cta); break;
-        case YQ_MOVE_EXCHANGE_ANY: dispatch_jpl<R, YQ_MOVE_EXCHANGE_ANY>(A, st, &S->chains_per_cta); break;
-        case YQ_MOVE_HAMILTONIAN: dispatch_jpl<R, YQ_MOVE_HAMILTONIAN>(A, st, &S->chains_per_cta); break;
-        default: dispatch_jpl<R, YQ_MOVE_EXCHANGE_NN>(A, st, &S->chains_per_cta); break;
+        case YQ_MOVE_LOCAL: dispatch_shape<R, YQ_MOVE_LOCAL>(A, st, cpc, wpc); break;
+        case YQ_MOVE_EXCHANGE_ANY: dispatch_shape<R, YQ_MOVE_EXCHANGE_ANY>(A, st, cpc, wpc); break;
+        case YQ_MOVE_HAMILTONIAN: dispatch_shape<R, YQ_MOVE_HAMILTONIAN>(A, st, cpc, wpc); break;
+        default: dispatch_shape<R, YQ_MOVE_EXCHANGE_NN>(A, st, cpc, wpc); break;
     }
 }
 

@@ -52,7 +52,7 @@ def main():
                 S.sample(8, 8, 1, e, False)
                 ts.append(ctx.stage_ms("sample"))
             print(f"M {mm:4d}  units per lane {(mm + 31) // 32:2d}  sample {min(ts):.3f} ms  "
-                  f"chains per CTA {S.chains_per_cta()}")
+                  f"chains per CTA {S.chains_per_cta()}  warps per chain {S.warps_per_chain()}")
             S.close()
             q.close()
         ctx.close()
