@@ -11,9 +11,11 @@
 * Late-run 12 x 12 parameters (tests/golden/tfi2d12x12_late_params.npy: the FP64
   path's parameters after 300 iterations of the bench workload, complex64): on one
   and the same 8192-sample set the mixed SR step (complex64 O, BF16x3 tcgen05 T,
-  panel Cholesky, two FP64 refinement steps) against the FP64 SR step: energy per
-  site within 2e-8, force within 1e-4 relative, update within 6e-2 relative (T is
-  ill-conditioned here; the refinement converges to the complex64-O solution).
+  panel Cholesky, two steps of CG preconditioned by that factor, FP64 residuals)
+  against the FP64 SR step: energy per site within 2e-8, force within 1e-4
+  relative, update within 2e-3 relative (T is ill-conditioned here: plain
+  iterative refinement with the same factor moved away from the solution from its
+  second step on, 0.9 % after two).
 """
 import json
 import os
@@ -94,6 +96,6 @@ def test_late_run_same_sample_mixed_vs_fp64(ctx, orc):
     Ff = srf.get(2, qf.dim)
     assert abs(em - ef) / n < 2e-8
     assert np.linalg.norm(Fm - Ff) / np.linalg.norm(Ff) < 1e-4
-    assert np.linalg.norm(vm - vf) / np.linalg.norm(vf) < 6e-2
+    assert np.linalg.norm(vm - vf) / np.linalg.norm(vf) < 2e-3
     for x in (srm, srf, Sm, Sf, Hm, qm, qf):
         x.close()

@@ -149,6 +149,7 @@ struct yq_sr_s {
     yq::DevBuf gavg, gused;  // P c128: running average and the bias-corrected gradient
     yq::DevBuf favg;         // dim_pad x dim_pad c128 running Fisher average (S-form)
     yq::DevBuf trhs;         // ns c128: right-hand side of a T-form solve with a given gradient
+    yq::DevBuf pcg;          // T-form PCG vectors r, z, p, q (dim_pad c128 each) and step scalars
 };
 
 // A batch of SR problems advanced together (batch.cu).

@@ -825,11 +825,56 @@ static void llt_apply(yq_sr_s* sr, const LltPlan& pl, c128* b, c128* tmp, c128* 
                          ctx->status.as<int>(), sr->chol_work.p, ctx->sm_count, ctx->stream);
 }
 
-// T-form: sol = (T + shift)^{-1} rhs (dim_pad entries, zero beyond ns), then
-// ir_steps iterative-refinement steps against the exact operator
-// T y = O~ (O~^H y) / Ns + shift y with FP64 sums.
+// Hermitian inner product Re <a, b> = Re sum conj(a_i) b_i of two device vectors
+// into *out, one block (the T-form vectors hold at most a few hundred thousand
+// entries), FP64 sums in a fixed order.
+__global__ void __launch_bounds__(1024) dot_re_kernel(size_t n, const c128* __restrict__ a,
+                                                      const c128* __restrict__ b, double* __restrict__ out) {
+    __shared__ double red[32];
+    double acc = 0.;
+    for (size_t i = threadIdx.x; i < n; i += blockDim.x) acc += a[i].re * b[i].re + a[i].im * b[i].im;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) t += red[w];
+        *out = t;
+    }
+}
+
+// PCG step scalars on the device (sc: [0] <r, z>, [1] <p, q>, [2] <r', z'>):
+// x += a p, r -= a q with a = <r, z> / <p, q>.
+__global__ void pcg_xr_kernel(size_t n, const double* __restrict__ sc, const c128* __restrict__ p,
+                              const c128* __restrict__ q, c128* __restrict__ x, c128* __restrict__ r) {
+    const double a = sc[1] != 0.0 ? sc[0] / sc[1] : 0.0;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        x[i] = x[i] + a * p[i];
+        r[i] = r[i] - a * q[i];
+    }
+}
+// p = z + b p with b = <r', z'> / <r, z>; afterwards <r', z'> becomes <r, z> (one
+// block does the swap after every block has read the old value: a separate launch).
+__global__ void pcg_p_kernel(size_t n, const double* __restrict__ sc, const c128* __restrict__ z,
+                             c128* __restrict__ p) {
+    const double b = sc[0] != 0.0 ? sc[2] / sc[0] : 0.0;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        p[i] = z[i] + b * p[i];
+}
+__global__ void pcg_swap_kernel(double* sc) { sc[0] = sc[2]; }
+
+// T-form: sol = (T + shift)^{-1} rhs (dim_pad entries, zero beyond ns) with the
+// Cholesky factor, then `steps` iterations of conjugate gradients preconditioned
+// by that factor, on the exact operator T y = O~ (O~^H y) / Ns + shift y with FP64
+// sums and residuals.  (Plain iterative refinement x += M^{-1} (b - T x) diverges
+// where the BF16x3 factor is a poor approximation of an ill-conditioned T -- at
+// converged parameters of the 12 x 12 workload its second step already moved the
+// solution away -- while CG preconditioned by the same Hermitian positive definite
+// factor converges for any such preconditioner.)  The step scalars stay on the
+// device, so the sequence has no host round trip and can be captured in a graph.
 template <typename R>
-static void t_solve(yq_sr_s* sr, const LltPlan& pl, double shift, const c128* rhs, c128* sol, int ir_steps) {
+static void t_solve(yq_sr_s* sr, const LltPlan& pl, double shift, const c128* rhs, c128* sol, int steps) {
     cudaStream_t st = sr->q->ctx->stream;
     const size_t dp = size_t(sr->dim_pad);
     const int ns = sr->ns;
@@ -837,19 +882,44 @@ static void t_solve(yq_sr_s* sr, const LltPlan& pl, double shift, const c128* rh
     c128* tmp = sr->s2.as<c128>();
     YQ_CUDA(cudaMemcpyAsync(b, rhs, dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
     llt_apply(sr, pl, b, tmp, sol);
-    for (int k = 0; k < ir_steps; ++k) {
-        c128* ty = sr->s3.as<c128>();
-        c128* r = sr->rhs.as<c128>();
-        c128* dy = sr->s4.as<c128>();
-        YQ_CUDA(cudaMemsetAsync(ty, 0, dp * sizeof(c128), st));
-        op_ohy<R>(sr, sol, 1.0, sr->work_p.as<c128>(), nullptr, 0.0);
-        op_ox<R>(sr, sr->work_p.as<c128>(), 1.0 / ns, ty);
-        axpy_kernel<<<cdiv_u(ns, 256), 256, 0, st>>>(size_t(ns), mk(shift, 0.0), sol, ty);
-        residual_kernel<<<cdiv_u(dp, 256), 256, 0, st>>>(dp, rhs, ty, r);
+    if (steps <= 0) return;
+    sr->pcg.ensure(4 * dp * sizeof(c128) + 8 * sizeof(double));
+    c128* r = sr->pcg.as<c128>();
+    c128* z = r + dp;
+    c128* p = z + dp;
+    c128* q = p + dp;
+    double* sc = reinterpret_cast<double*>(q + dp);
+    const unsigned g = std::min(148u * 8, cdiv_u(dp, 256));
+    auto apply_T = [&](const c128* x, c128* out) {  // out = T x (+ shift x), zero beyond ns
+        YQ_CUDA(cudaMemsetAsync(out, 0, dp * sizeof(c128), st));
+        op_ohy<R>(sr, x, 1.0, sr->work_p.as<c128>(), nullptr, 0.0);
+        op_ox<R>(sr, sr->work_p.as<c128>(), 1.0 / ns, out);
+        axpy_kernel<<<cdiv_u(ns, 256), 256, 0, st>>>(size_t(ns), mk(shift, 0.0), x, out);
         YQ_LAUNCH_CHECK();
-        llt_apply(sr, pl, r, tmp, dy);
-        axpy_kernel<<<cdiv_u(dp, 256), 256, 0, st>>>(dp, mk(1.0, 0.0), dy, sol);
+    };
+    auto precond = [&](const c128* in, c128* out) {  // out = M^{-1} in (in kept)
+        YQ_CUDA(cudaMemcpyAsync(out, in, dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+        llt_apply(sr, pl, out, tmp, out);
+    };
+    apply_T(sol, q);
+    residual_kernel<<<g, 256, 0, st>>>(dp, rhs, q, r);
+    YQ_LAUNCH_CHECK();
+    precond(r, z);
+    YQ_CUDA(cudaMemcpyAsync(p, z, dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+    dot_re_kernel<<<1, 1024, 0, st>>>(dp, r, z, sc + 0);
+    YQ_LAUNCH_CHECK();
+    for (int k = 0; k < steps; ++k) {
+        apply_T(p, q);
+        dot_re_kernel<<<1, 1024, 0, st>>>(dp, p, q, sc + 1);
+        pcg_xr_kernel<<<g, 256, 0, st>>>(dp, sc, p, q, sol, r);
         YQ_LAUNCH_CHECK();
+        if (k + 1 < steps) {
+            precond(r, z);
+            dot_re_kernel<<<1, 1024, 0, st>>>(dp, r, z, sc + 2);
+            pcg_p_kernel<<<g, 256, 0, st>>>(dp, sc, z, p);
+            pcg_swap_kernel<<<1, 1, 0, st>>>(sc);
+            YQ_LAUNCH_CHECK();
+        }
     }
 }
 
