@@ -266,8 +266,9 @@ int yq_debug_wait_timeout(yq_ctx ctx, int which, unsigned cap, int* published);
 /* SRMat<Machine, Hamiltonian>(qs, ham) -- SRMat.hpp:83-87, bound to a sampler.
  * mode: S = O~^H O~ / Ns (P x P), T = O~ O~^H / Ns (Ns x Ns, push-through dual),
  * AUTO picks T when Ns < P.  precision: FP64 everywhere, or MIXED (c64 sampling
- * and O, BF16x3 tensor-core S/T with FP32 accumulation, FP64 Cholesky + iterative
- * refinement, FP64 means). */
+ * and O, BF16x3 tensor-core S/T with FP32 accumulation, a Cholesky factor of the
+ * shifted T used as the preconditioner of CG steps with FP64 residuals on the
+ * exact operator, FP64 means). */
 int yq_sr_create(yq_rbm q, yq_ham H, yq_sampler S, int mode, int precision, yq_sr* out);
 int yq_sr_destroy(yq_sr sr);
 /* constructFromSamples -- SRMat.hpp:89-103 (E_loc, O, mean, centring, F). */
@@ -340,7 +341,7 @@ typedef struct {
     double lr;             /* SGD eta = max(alpha / t^p, 1e-4) by caller            */
     int solver;            /* YQ_SOLVE_LLT or YQ_SOLVE_CG                           */
     double cg_tol;
-    int ir_steps;          /* iterative-refinement steps (mixed precision)          */
+    int ir_steps;          /* T-form: CG steps preconditioned by the factor (mixed) */
 } yq_iter_params;
 
 typedef struct {

@@ -36,22 +36,24 @@ struct FFDims {
     size_t P;
 };
 
-// z1, a1 (in place of z1 when !keep_z) and z2 for FF_SB samples into shared memory.
+// z1 = conv(sigma), a1 = logcosh(z1) (each evaluated once) and z2 = W^T a1 for nsb
+// <= FF_SB samples into shared memory.
 __device__ void ff_forward_block(const FFDims& d, const float* __restrict__ ker, const float* __restrict__ Wfc,
-                                 const float* s_sig /*[SB][L]*/, float* s_z1 /*[SB][LC]*/, float* s_z2 /*[SB][F]*/,
-                                 int nsb) {
+                                 const float* s_sig /*[SB][L]*/, float* s_z1 /*[SB][LC]*/, float* s_a1 /*[SB][LC]*/,
+                                 float* s_z2 /*[SB][F]*/, int nsb) {
     const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
     for (int e = tid; e < nsb * d.LC; e += nt) {
         const int s = e / d.LC, q = e % d.LC, oc = q / d.L, r = q % d.L;
         float acc = 0.f;
         for (int ki = 0; ki < d.K; ++ki) acc += ker[ki + d.K * oc] * s_sig[s * d.L + (r + ki - d.K / 2 + d.L) % d.L];
         s_z1[s * d.LC + q] = acc;
+        s_a1[s * d.LC + q] = logcoshf_ref(acc);
     }
     __syncthreads();
     for (int pr = warp; pr < nsb * d.F; pr += nw) {
         const int s = pr / d.F, o = pr % d.F;
         float acc = 0.f;
-        for (int i = lane; i < d.LC; i += 32) acc += logcoshf_ref(s_z1[s * d.LC + i]) * Wfc[i + size_t(d.LC) * o];
+        for (int i = lane; i < d.LC; i += 32) acc += s_a1[s * d.LC + i] * Wfc[i + size_t(d.LC) * o];
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
         if (lane == 0) s_z2[s * d.F + o] = acc;
@@ -66,10 +68,11 @@ __global__ void ff_forward_kernel(FFDims d, int batch, const float* __restrict__
     float* s_sig = sm;                    // SB * L
     float* s_z1 = s_sig + FF_SB * d.L;    // SB * LC
     float* s_z2 = s_z1 + FF_SB * d.LC;    // SB * F
+    float* s_a1 = s_z2 + FF_SB * d.F;     // SB * LC
     const int b0 = blockIdx.x * FF_SB, nsb = min(FF_SB, batch - b0);
     for (int e = threadIdx.x; e < nsb * d.L; e += blockDim.x) s_sig[e] = float(sigma[size_t(b0) * d.L + e]);
     __syncthreads();
-    ff_forward_block(d, params, params + d.KC, s_sig, s_z1, s_z2, nsb);
+    ff_forward_block(d, params, params + d.KC, s_sig, s_z1, s_a1, s_z2, nsb);
     if (threadIdx.x < nsb) {
         double lp = 0.;
         for (int o = 0; o < d.F; ++o) lp += double(logcoshf_ref(s_z2[threadIdx.x * d.F + o]));
@@ -108,12 +111,12 @@ __global__ void ff_adjoint_kernel(FFDims d, int batch, const float* __restrict__
                 s_z2[s * d.F + q - d.LC] = v;
         }
         __syncthreads();
+        for (int e = tid; e < nsb * d.LC; e += nt) s_a1[e] = logcoshf_ref(s_z1[e]);
     } else {
         __syncthreads();
-        ff_forward_block(d, ker, Wfc, s_sig, s_z1, s_z2, nsb);
+        ff_forward_block(d, ker, Wfc, s_sig, s_z1, s_a1, s_z2, nsb);
     }
     for (int e = tid; e < nsb * d.F; e += nt) s_z2[e] = tanhf(s_z2[e]);  // d2 = 1 * tanh(z2)
-    for (int e = tid; e < nsb * d.LC; e += nt) s_a1[e] = logcoshf_ref(s_z1[e]);
     __syncthreads();
     // FullyConnected.hpp:170-172: der_w = a1 d2^T, column-major (LC x F) after the conv block.
     // With KC, LC and P multiples of 4 the block is written as aligned float4 runs
@@ -139,12 +142,21 @@ __global__ void ff_adjoint_kernel(FFDims d, int batch, const float* __restrict__
             }
         }
     }
-    // d1 = W d2, then the LnCosh Jacobian: dz1 = d1 * tanh(z1) (in place of z1)
-    for (int e = tid; e < nsb * d.LC; e += nt) {
-        const int s = e / d.LC, i = e % d.LC;
-        float acc = 0.f;
-        for (int o = 0; o < d.F; ++o) acc += Wfc[i + size_t(d.LC) * o] * s_z2[s * d.F + o];
-        s_z1[e] = acc * tanhf(s_z1[e]);
+    // d1 = W d2, then the LnCosh Jacobian: dz1 = d1 * tanh(z1) (in place of z1); a
+    // thread per input i keeps the block's samples in registers, so each weight is
+    // read once per block
+    for (int i = tid; i < d.LC; i += nt) {
+        float acc[FF_SB];
+#pragma unroll
+        for (int s = 0; s < FF_SB; ++s) acc[s] = 0.f;
+        for (int o = 0; o < d.F; ++o) {
+            const float w = Wfc[i + size_t(d.LC) * o];
+#pragma unroll
+            for (int s = 0; s < FF_SB; ++s) acc[s] += w * s_z2[s * d.F + o];
+        }
+#pragma unroll
+        for (int s = 0; s < FF_SB; ++s)
+            if (s < nsb) s_z1[s * d.LC + i] = acc[s] * tanhf(s_z1[s * d.LC + i]);
     }
     __syncthreads();
     // Conv1D.hpp:197-212: dw(ki, oc) = sum_r in((r + ki - K/2) mod L) dz1(r + oc L)
@@ -165,13 +177,14 @@ __global__ void ff_eloc_tfi_kernel(FFDims d, int batch, double J, double h, cons
     float* s_sig = sm;             // L
     float* s_z1 = s_sig + d.L;     // LC
     float* s_z2 = s_z1 + d.LC;     // F
+    float* s_a1 = s_z2 + d.F;      // LC
     __shared__ double red[32];
     const float* ker = params;
     const float* Wfc = params + d.KC;
     const int b = blockIdx.x, tid = threadIdx.x;
     for (int e = tid; e < d.L; e += blockDim.x) s_sig[e] = float(sigma[size_t(b) * d.L + e]);
     __syncthreads();
-    ff_forward_block(d, ker, Wfc, s_sig, s_z1, s_z2, 1);
+    ff_forward_block(d, ker, Wfc, s_sig, s_z1, s_a1, s_z2, 1);
     double acc = 0.;
     for (int i = tid; i < d.L; i += blockDim.x) {
         const float si = s_sig[i];
@@ -236,7 +249,7 @@ void need_batch(const yq_ff_s* f) {
     if (f->batch <= 0) throw Error(YQ_E_STATE, "feedforward: set a batch first");
 }
 
-size_t fwd_smem(const FFDims& d) { return size_t(FF_SB) * (d.L + d.LC + d.F) * sizeof(float); }
+size_t fwd_smem(const FFDims& d) { return size_t(FF_SB) * (d.L + 2 * d.LC + d.F) * sizeof(float); }
 size_t adj_smem(const FFDims& d) { return size_t(FF_SB) * (d.L + 2 * d.LC + d.F) * sizeof(float); }
 
 void set_smem_attr(const void* fn, size_t bytes) {
@@ -409,7 +422,7 @@ int yq_ff_eloc_tfi(yq_ff f, double J, double h, double* eloc) {
         const FFDims d = dims(f);
         cudaStream_t st = f->ctx->stream;
         f->eloc.ensure(size_t(f->batch) * sizeof(c128));
-        const size_t smem = size_t(d.L + d.LC + d.F) * sizeof(float);
+        const size_t smem = size_t(d.L + 2 * d.LC + d.F) * sizeof(float);
         set_smem_attr(reinterpret_cast<const void*>(ff_eloc_tfi_kernel), smem);
         const int threads = std::max(32, std::min(256, ((d.L + 31) / 32) * 32));
         f->ctx->stage_begin(ST_FF_ELOC);
