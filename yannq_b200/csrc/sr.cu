@@ -119,6 +119,10 @@ __global__ void oloc_reduce_kernel(int n, int m, bool bias, int nsplit, double i
 // their place in [s_i t_j | s | t] and their means are resolved once, then the
 // thread walks O_ROWS rows, reading sigma and t from L1/L2 and storing both values
 // at once (one 16-byte store for complex64 rows of even P, two for complex128).
+// For complex64 the per-row arithmetic is branch-free (s := 1 or t := 1 by a
+// select) and four rows' loads are issued before their stores: 0.63 -> 0.86 of the
+// copy peak on the XXZ workload, where the complex128 rows (32 bytes a thread)
+// measured best one row at a time.
 constexpr int O_ROWS = 16;
 template <typename R>
 __global__ void __launch_bounds__(256) o_writer_kernel(int n, int m, bool bias, size_t P, int ns,
@@ -153,35 +157,70 @@ __global__ void __launch_bounds__(256) o_writer_kernel(int n, int m, bool bias, 
             oli[e] = R(o.im);
         }
     }
-    const bool pair16 = sizeof(R) == 4 && (P % 2) == 0 && kind[1] != 3;
     const int groups = (ns + O_ROWS - 1) / O_ROWS;
-    for (int gi = blockIdx.y; gi < groups; gi += gridDim.y)
-    for (int s = gi * O_ROWS, s1 = min(ns, s + O_ROWS); s < s1; ++s) {
-        const int8_t* sg = sigma + size_t(s) * n;
-        const cplx<R>* ts = t + size_t(s) * m;
-        cplx<R> v[2];
+    if constexpr (sizeof(R) == 4) {
+        constexpr int RU = 4;  // rows whose loads are in flight together
+        const bool pair16 = (P % 2) == 0 && kind[1] != 3;
+        bool use_s[2], use_t[2];
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-            cplx<R> x = mk(R(0), R(0));
-            if (kind[e] == 0) {
-                const R sv = R(sg[ci[e]]);
-                const cplx<R> tv = ts[cj[e]];
-                x = mk(sv * tv.re, sv * tv.im);
-            } else if (kind[e] == 1) {
-                x = mk(R(sg[ci[e]]), R(0));
-            } else if (kind[e] == 2) {
-                x = ts[cj[e]];
+            use_s[e] = kind[e] == 0 || kind[e] == 1;
+            use_t[e] = kind[e] == 0 || kind[e] == 2;
+        }
+        for (int gi = blockIdx.y; gi < groups; gi += gridDim.y)
+            for (int s = gi * O_ROWS, s1 = min(ns, s + O_ROWS); s < s1; s += RU) {
+                cplx<R> v[RU][2];
+#pragma unroll
+                for (int u = 0; u < RU; ++u) {
+                    const int su = min(s + u, s1 - 1);  // a short last group repeats its last row, not stored
+                    const int8_t* sg = sigma + size_t(su) * n;
+                    const cplx<R>* ts = t + size_t(su) * m;
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const R sraw = R(sg[ci[e]]);
+                        const cplx<R> traw = ts[cj[e]];
+                        const R sv = use_s[e] ? sraw : R(1);
+                        const R tr = use_t[e] ? traw.re : R(1), ti = use_t[e] ? traw.im : R(0);
+                        v[u][e] = mk(sv * tr - olr[e], sv * ti - oli[e]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < RU; ++u) {
+                    if (s + u >= s1) break;
+                    cplx<R>* row = O + size_t(s + u) * P;
+                    if (pair16) {
+                        *reinterpret_cast<float4*>(row + p0) =
+                            make_float4(v[u][0].re, v[u][0].im, v[u][1].re, v[u][1].im);
+                    } else {
+                        row[p0] = v[u][0];
+                        if (kind[1] != 3) row[p0 + 1] = v[u][1];
+                    }
+                }
             }
-            v[e] = mk(x.re - olr[e], x.im - oli[e]);
-        }
-        cplx<R>* row = O + size_t(s) * P;
-        if (pair16) {
-            *reinterpret_cast<float4*>(row + p0) =
-                make_float4(float(v[0].re), float(v[0].im), float(v[1].re), float(v[1].im));
-        } else {
-            row[p0] = v[0];
-            if (kind[1] != 3) row[p0 + 1] = v[1];
-        }
+    } else {
+        for (int gi = blockIdx.y; gi < groups; gi += gridDim.y)
+            for (int s = gi * O_ROWS, s1 = min(ns, s + O_ROWS); s < s1; ++s) {
+                const int8_t* sg = sigma + size_t(s) * n;
+                const cplx<R>* ts = t + size_t(s) * m;
+                cplx<R> v[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    cplx<R> x = mk(R(0), R(0));
+                    if (kind[e] == 0) {
+                        const R sv = R(sg[ci[e]]);
+                        const cplx<R> tv = ts[cj[e]];
+                        x = mk(sv * tv.re, sv * tv.im);
+                    } else if (kind[e] == 1) {
+                        x = mk(R(sg[ci[e]]), R(0));
+                    } else if (kind[e] == 2) {
+                        x = ts[cj[e]];
+                    }
+                    v[e] = mk(x.re - olr[e], x.im - oli[e]);
+                }
+                cplx<R>* row = O + size_t(s) * P;
+                row[p0] = v[0];
+                if (kind[1] != 3) row[p0 + 1] = v[1];
+            }
     }
 }
 
