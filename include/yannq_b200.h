@@ -282,6 +282,12 @@ int yq_sr_get(yq_sr sr, int which, double* out);
  * relative-residual tolerance cg_tol.  v (P complex, may be null) receives the
  * solution; iterations/relres (may be null) the CG statistics. */
 int yq_sr_solve(yq_sr sr, double shift, int solver, double cg_tol, double* v, int* iterations, double* relres);
+/* CG steps of the T-form LLT solve of yq_sr_solve (a setting of this library; the
+ * reference solves with Eigen::LLT alone, SRMat.hpp:231-237): 0 applies the
+ * Cholesky factor once, s > 0 runs s + 1 iterations of CG from zero preconditioned
+ * by the factor, on the exact operator with FP64 sums.  -1 (the default) means 2 for
+ * YQ_PREC_MIXED and 0 for YQ_PREC_FP64. */
+int yq_sr_set_solve_steps(yq_sr sr, int steps);
 /* corrMat() -- SRMat.hpp:142-149: the Hermitian matrix the last LLT solve used
  * (S or T, including the shift), lower triangle, dim x dim complex row-major. */
 int yq_sr_matrix(yq_sr sr, int* dim, double* out);
@@ -341,7 +347,7 @@ typedef struct {
     double lr;             /* SGD eta = max(alpha / t^p, 1e-4) by caller            */
     int solver;            /* YQ_SOLVE_LLT or YQ_SOLVE_CG                           */
     double cg_tol;
-    int ir_steps;          /* T-form: CG steps preconditioned by the factor (mixed) */
+    int ir_steps;          /* T-form: CG steps as in yq_sr_set_solve_steps (>= 0)  */
 } yq_iter_params;
 
 typedef struct {

@@ -133,6 +133,7 @@ SIGNATURES = {
     "yq_sr_energy": [_vp, _vp, _vp],
     "yq_sr_get": [_vp, _i, _vp],
     "yq_sr_solve": [_vp, _d, _i, _d, _vp, _vp, _vp],
+    "yq_sr_set_solve_steps": [_vp, _i],
     "yq_sr_matrix": [_vp, _vp, _vp],
     "yq_sr_set_momentum": [_vp, _d, _d],
     "yq_sr_set_grad_clip": [_vp, _d],
@@ -563,6 +564,9 @@ class SR:
         out = np.zeros(size, np.complex128)
         check(lib().yq_sr_get(self.h, which, _p(out)))
         return out
+
+    def set_solve_steps(self, steps):
+        check(lib().yq_sr_set_solve_steps(self.h, int(steps)))
 
     def solve(self, shift, solver=SOLVE_LLT, cg_tol=1e-4):
         v = np.zeros(self.rbm.dim, np.complex128)

@@ -938,10 +938,18 @@ int yq_sr_solve(yq_sr sr, double shift, int solver, double cg_tol, double* v, in
     return guard([&] {
         need(sr, "sr");
         if (solver != YQ_SOLVE_LLT && solver != YQ_SOLVE_CG) throw Error(YQ_E_ARG, "solve: unknown solver");
-        const int ir = sr->precision == YQ_PREC_MIXED ? 2 : 0;
+        const int ir = sr->solve_steps >= 0 ? sr->solve_steps : sr->precision == YQ_PREC_MIXED ? 2 : 0;
         sr_solve(sr, shift, solver, cg_tol, ir, iterations, relres);
         raise_device_status(sr->q->ctx);
         if (v) down(reinterpret_cast<c128*>(v), sr->v.p, sr->q->P, sr->q->ctx->stream);
+    });
+}
+
+int yq_sr_set_solve_steps(yq_sr sr, int steps) {
+    return guard([&] {
+        need(sr, "sr");
+        if (steps < -1 || steps > 64) throw Error(YQ_E_ARG, "set_solve_steps: steps must be -1..64");
+        sr->solve_steps = steps;
     });
 }
 

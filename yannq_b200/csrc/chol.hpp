@@ -33,7 +33,7 @@ constexpr int CHOL_PANEL = 512;
 size_t chol_panel_planes_bytes(int n);
 void chol_factor_panels(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int* status, void* scratch,
                         void* planes, int sm_count, cudaStream_t st);
-// out = (L L^H)^{-1} b; b is overwritten with the solution as well.
+// out = (L L^H)^{-1} b; out may be b.  `scratch` also holds the forward result.
 void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c128* LinvH, c128* b, c128* out,
                       int* status, void* scratch, int sm_count, cudaStream_t st);
 

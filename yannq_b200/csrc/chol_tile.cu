@@ -49,6 +49,12 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 __device__ __forceinline__ void st_release(int* p, int v) {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
@@ -68,13 +74,15 @@ __device__ bool wait_flag(const int* flag, const Sync& S, int* s_ok) {
     if (threadIdx.x == 0) {
         int ok = 1;
         unsigned it = 0;
-        while (ld_acquire(flag) == 0) {
-            if (ld_acquire(S.abort_word) != 0 || ++it > S.cap) {
+        while (ld_relaxed(flag) == 0) {
+            // the abort word every 32 polls: one outstanding load per poll
+            if ((++it & 31u) == 0 && (ld_acquire(S.abort_word) != 0 || it > S.cap)) {
                 ok = 0;
                 break;
             }
-            __nanosleep(64);
+            __nanosleep(32);
         }
+        if (ok) fence_acq_rel();  // with the relaxed read of the flag: an acquire pattern
         if (!ok && it > S.cap) {
             atomicOr(S.status, DS_TIMEOUT);
             atomicExch(S.abort_word, 1);
@@ -427,8 +435,9 @@ struct SolveArgs {
     int nt;
     const c128* Linv;
     const c128* LinvH;
-    c128* b;    // in: right-hand side; forward result written here per block
-    int* flags; // nt
+    const c128* b;  // right-hand side
+    c128* x;        // result, every entry SOLVE_EMPTY until its block is written
+    int* flags;     // nt, set after each block (bookkeeping: no sweep waits on them)
     int* counter;  // block rows are claimed in sweep order from this counter
     Sync S;
 };
@@ -446,11 +455,57 @@ __device__ __forceinline__ int claim_row(const SolveArgs& a, int* s_row) {
 
 // Solve sweeps.  One CTA per 64-row block (persistent over blocks r = blockIdx.x,
 // + gridDim.x, ...).  The L tiles a block needs do not depend on the sweep, so they
-// stream into shared memory (cp.async, two buffers) ahead of the flags; only the
-// 64-entry solution block x_k waits for its flag.  The diagonal inverse is staged
+// stream into shared memory (cp.async, two buffers) ahead of the solution; only
+// the 64-entry solution block x_k is waited for.  The diagonal inverse is staged
 // at the start.  Each chain link is then a shared-memory mat-vec.
+//
+// The solution vector is its own flag: it starts filled with the bit pattern
+// SOLVE_EMPTY (all ones, a NaN that no arithmetic result here has: FP64 operations
+// return the positive canonical NaN, and a result that matched would be stored as
+// that instead), and a waiting CTA polls the 64 entries of block k until none is
+// SOLVE_EMPTY.  Each entry's halves are written and read as single 8-byte strong
+// accesses, so a read that sees a value sees the final one.  A link of the chain
+// thus costs one trip through L2 (the store, seen by the next poll) instead of a
+// fence, a flag store, a flag poll and a load of the block.
+constexpr unsigned long long SOLVE_EMPTY = ~0ull;
 constexpr int SLD = TB + 1;  // staged tile row stride (complex)
 constexpr size_t SM_SOLVE = size_t(3) * TB * SLD * sizeof(c128) + 2 * TB * sizeof(c128);
+
+// Threads 0..63 poll entry k TB + tid of x until it is written (bounded; the abort
+// word every 64 polls) and copy it to dst; false when this or another CTA gave up.
+__device__ bool poll_block(const c128* x, c128* dst, const Sync& S) {
+    int ok = 1;
+    if (threadIdx.x < TB) {
+        const c128* p = x + threadIdx.x;
+        unsigned long long re, im;
+        unsigned it = 0;
+        while (true) {
+            asm volatile("ld.relaxed.gpu.global.v2.b64 {%0, %1}, [%2];" : "=l"(re), "=l"(im) : "l"(p) : "memory");
+            if (re != SOLVE_EMPTY && im != SOLVE_EMPTY) break;
+            if ((++it & 63u) == 0 && (ld_acquire(S.abort_word) != 0 || it > S.cap)) {
+                ok = 0;
+                break;
+            }
+        }
+        if (ok) {
+            dst[threadIdx.x] = mk(__longlong_as_double(static_cast<long long>(re)),
+                                  __longlong_as_double(static_cast<long long>(im)));
+        } else if (it > S.cap) {
+            atomicOr(S.status, DS_TIMEOUT);
+            atomicExch(S.abort_word, 1);
+        }
+    }
+    return __syncthreads_and(ok) != 0;
+}
+
+// Writes one solution entry (never the SOLVE_EMPTY pattern) as two strong 8-byte stores.
+__device__ __forceinline__ void store_entry(c128* x, c128 v) {
+    unsigned long long re = static_cast<unsigned long long>(__double_as_longlong(v.re));
+    unsigned long long im = static_cast<unsigned long long>(__double_as_longlong(v.im));
+    if (re == SOLVE_EMPTY) re = 0x7fffffffffffffffull;
+    if (im == SOLVE_EMPTY) im = 0x7fffffffffffffffull;
+    asm volatile("st.relaxed.gpu.global.v2.b64 [%0], {%1, %2};" ::"l"(x), "l"(re), "l"(im) : "memory");
+}
 
 // Stage the 64 x 64 tile at `src` (row stride ld) into dst[64][SLD].
 __device__ __forceinline__ void stage_tile(c128* dst, const c128* src, size_t ld) {
@@ -483,7 +538,7 @@ __global__ void __launch_bounds__(128, 1) chol_fwd_tile_kernel(SolveArgs a) {
     c128* Li = buf + 2 * TB * SLD;             // diagonal inverse
     c128* xk = Li + TB * SLD;                  // published block
     c128* acc = xk + TB;
-    __shared__ int s_ok, s_row;
+    __shared__ int s_row;
     const int tid = threadIdx.x, row = tid >> 1, half = tid & 1;
     for (int r = claim_row(a, &s_row); r < a.nt; r = claim_row(a, &s_row)) {
         stage_tile(Li, a.Linv + size_t(r) * TB * TB, TB);
@@ -495,11 +550,10 @@ __global__ void __launch_bounds__(128, 1) chol_fwd_tile_kernel(SolveArgs a) {
         for (int k = 0; k < r; ++k) {
             if (k + 1 < r) stage_tile(buf + ((k + 1) & 1) * TB * SLD, a.G + size_t(r) * TB * a.ld + (k + 1) * TB, a.ld);
             cpa_commit();
-            if (!wait_flag(&a.flags[k], a.S, &s_ok)) {
+            if (!poll_block(a.x + k * TB, xk, a.S)) {
                 ok = false;
                 break;
             }
-            if (tid < TB) xk[tid] = a.b[k * TB + tid];
             cpa_wait_one();  // tile k (and everything before it) has landed
             __syncthreads();
             const c128* T = buf + (k & 1) * TB * SLD + row * SLD + half * 32;
@@ -515,7 +569,7 @@ __global__ void __launch_bounds__(128, 1) chol_fwd_tile_kernel(SolveArgs a) {
         c128 v = dot32<false>(Li + row * SLD + half * 32, 1, acc + half * 32);
         v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
         v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
-        if (half == 0) a.b[r * TB + row] = v;
+        if (half == 0) store_entry(a.x + r * TB + row, v);
         publish(&a.flags[r]);
     }
 }
@@ -527,7 +581,7 @@ __global__ void __launch_bounds__(128, 1) chol_bwd_tile_kernel(SolveArgs a) {
     c128* Li = buf + 2 * TB * SLD;
     c128* zk = Li + TB * SLD;
     c128* acc = zk + TB;
-    __shared__ int s_ok, s_row;
+    __shared__ int s_row;
     const int tid = threadIdx.x, col = tid >> 1, half = tid & 1;
     for (int t = claim_row(a, &s_row); t < a.nt; t = claim_row(a, &s_row)) {
         const int r = a.nt - 1 - t;
@@ -540,11 +594,10 @@ __global__ void __launch_bounds__(128, 1) chol_bwd_tile_kernel(SolveArgs a) {
         for (int k = a.nt - 1, i = 0; k > r; --k, ++i) {
             if (k - 1 > r) stage_tile(buf + ((i + 1) & 1) * TB * SLD, a.G + size_t(k - 1) * TB * a.ld + r * TB, a.ld);
             cpa_commit();
-            if (!wait_flag(&a.flags[k], a.S, &s_ok)) {
+            if (!poll_block(a.x + k * TB, zk, a.S)) {
                 ok = false;
                 break;
             }
-            if (tid < TB) zk[tid] = a.b[k * TB + tid];
             cpa_wait_one();
             __syncthreads();
             // acc[col] -= sum_row conj(L[k*64 + row][r*64 + col]) z_k[row]
@@ -562,7 +615,7 @@ __global__ void __launch_bounds__(128, 1) chol_bwd_tile_kernel(SolveArgs a) {
         c128 v = dot32<false>(Li + rowo * SLD + half * 32, 1, acc + half * 32);
         v.re += __shfl_xor_sync(0xffffffffu, v.re, 1);
         v.im += __shfl_xor_sync(0xffffffffu, v.im, 1);
-        if (half == 0) a.b[r * TB + rowo] = v;
+        if (half == 0) store_entry(a.x + r * TB + rowo, v);
         publish(&a.flags[r]);
     }
 }
@@ -578,26 +631,30 @@ int coresident_blocks(const void* fn, int threads, size_t smem, int sm_count) {
 // Scratch layout (ints): [0] tile counter of the full factorisation, [1] abort word
 // of the factorisation, [2] abort word of the solves, [3] / [4] block-row counters
 // of the forward / backward sweeps, [16 .. 16 + nt) tile counters
-// of the panels, then the tile flags (nt x nt), the solve flags (2 nt), and the
-// 16-byte aligned tile list.
+// of the panels, then the tile flags (nt x nt), the solve flags (2 nt), the
+// 16-byte aligned tile list, and the 16-byte aligned forward-sweep result (n c128).
 struct Scratch {
     int* words;
     int* panel_counters;
     int* flags;
     int* sflags;
     int2* items;
+    c128* xs;
     Scratch(void* p, int nt) {
         words = static_cast<int*>(p);
         panel_counters = words + 16;
         flags = panel_counters + nt;
         sflags = flags + size_t(nt) * nt;
         items = reinterpret_cast<int2*>((reinterpret_cast<uintptr_t>(sflags + 2 * size_t(nt)) + 15) & ~uintptr_t(15));
+        xs = reinterpret_cast<c128*>(
+            (reinterpret_cast<uintptr_t>(items + size_t(nt) * (nt + 1) / 2) + 15) & ~uintptr_t(15));
     }
 };
 
 size_t chol_tile_scratch_bytes(int n) {
     const size_t nt = size_t(n) / TB;
-    return (16 + nt + nt * nt + 2 * nt) * sizeof(int) + nt * (nt + 1) / 2 * sizeof(int2) + 256;
+    return (16 + nt + nt * nt + 2 * nt) * sizeof(int) + nt * (nt + 1) / 2 * sizeof(int2) + 256 +
+           size_t(n) * sizeof(c128) + 16;
 }
 
 // Column-major tile order, diagonal first: column j starts at j nt - j (j - 1) / 2.
@@ -700,13 +757,15 @@ void chol_solve_tiled(const c128* G, int n, size_t ld, const c128* Linv, const c
                                                       SM_SOLVE, sm_count));
     const int grid_b = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_bwd_tile_kernel), 128,
                                                       SM_SOLVE, sm_count));
-    SolveArgs fa{G, ld, nt, Linv, LinvH, b, sflags, words + 3, Sync{status, words + 2, 1u << 24}};
+    // forward b -> xs, backward xs -> out (b may be out: it is read by the forward sweep only)
+    YQ_CUDA(cudaMemsetAsync(sc.xs, 0xff, size_t(n) * sizeof(c128), st));
+    SolveArgs fa{G, ld, nt, Linv, LinvH, b, sc.xs, sflags, words + 3, Sync{status, words + 2, 1u << 24}};
     chol_fwd_tile_kernel<<<grid_f, 128, SM_SOLVE, st>>>(fa);
     YQ_LAUNCH_CHECK();
-    SolveArgs ba{G, ld, nt, Linv, LinvH, b, sflags + nt, words + 4, Sync{status, words + 2, 1u << 24}};
+    YQ_CUDA(cudaMemsetAsync(out, 0xff, size_t(n) * sizeof(c128), st));
+    SolveArgs ba{G, ld, nt, Linv, LinvH, sc.xs, out, sflags + nt, words + 4, Sync{status, words + 2, 1u << 24}};
     chol_bwd_tile_kernel<<<grid_b, 128, SM_SOLVE, st>>>(ba);
     YQ_LAUNCH_CHECK();
-    if (out != b) YQ_CUDA(cudaMemcpyAsync(out, b, size_t(n) * sizeof(c128), cudaMemcpyDeviceToDevice, st));
 }
 
 // Failure injection for the bounded waits (tests only): a 4 x 4-tile problem whose
@@ -752,7 +811,8 @@ int chol_debug_unpublished_flag(int which, unsigned cap, int* status, int sm_cou
         YQ_CUDA(cudaMemcpyAsync(sc.words + 3, &one, sizeof(int), cudaMemcpyHostToDevice, st));
         const int grid = std::min(nt, coresident_blocks(reinterpret_cast<const void*>(chol_fwd_tile_kernel), 128,
                                                         SM_SOLVE, sm_count));
-        SolveArgs fa{G.as<c128>(), size_t(n), nt, Li.as<c128>(), LiH.as<c128>(), b.as<c128>(), sc.sflags,
+        YQ_CUDA(cudaMemsetAsync(sc.xs, 0xff, size_t(n) * sizeof(c128), st));
+        SolveArgs fa{G.as<c128>(), size_t(n), nt, Li.as<c128>(), LiH.as<c128>(), b.as<c128>(), sc.xs, sc.sflags,
                      sc.words + 3, Sync{status, sc.words + 2, cap}};
         chol_fwd_tile_kernel<<<grid, 128, SM_SOLVE, st>>>(fa);
         YQ_LAUNCH_CHECK();

@@ -150,6 +150,8 @@ struct yq_sr_s {
     yq::DevBuf favg;         // dim_pad x dim_pad c128 running Fisher average (S-form)
     yq::DevBuf trhs;         // ns c128: right-hand side of a T-form solve with a given gradient
     yq::DevBuf pcg;          // T-form PCG vectors r, z, p, q (dim_pad c128 each) and step scalars
+    yq::DevBuf ohy_sol;      // P c128: O~^H of a T-form solution (the Woodbury form)
+    int solve_steps = -1;    // T-form CG steps of yq_sr_solve (-1: the precision's default)
 };
 
 // A batch of SR problems advanced together (batch.cu).

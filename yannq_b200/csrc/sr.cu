@@ -852,7 +852,7 @@ static void llt_factor(yq_sr_s* sr, const LltPlan& pl) {
     }
 }
 
-// out = (L L^H)^{-1} b (b is overwritten; tmp is scratch for the recursive form).
+// out = (L L^H)^{-1} b (b may be overwritten; tmp is scratch for the recursive form).
 static void llt_apply(yq_sr_s* sr, const LltPlan& pl, c128* b, c128* tmp, c128* out) {
     yq_ctx_s* ctx = sr->q->ctx;
     const size_t dp = size_t(sr->dim_pad);
@@ -903,56 +903,75 @@ __global__ void pcg_p_kernel(size_t n, const double* __restrict__ sc, const c128
 }
 __global__ void pcg_swap_kernel(double* sc) { sc[0] = sc[2]; }
 
-// T-form: sol = (T + shift)^{-1} rhs (dim_pad entries, zero beyond ns) with the
-// Cholesky factor, then `steps` iterations of conjugate gradients preconditioned
-// by that factor, on the exact operator T y = O~ (O~^H y) / Ns + shift y with FP64
-// sums and residuals.  (Plain iterative refinement x += M^{-1} (b - T x) diverges
-// where the BF16x3 factor is a poor approximation of an ill-conditioned T -- at
-// converged parameters of the 12 x 12 workload its second step already moved the
-// solution away -- while CG preconditioned by the same Hermitian positive definite
-// factor converges for any such preconditioner.)  The step scalars stay on the
-// device, so the sequence has no host round trip and can be captured in a graph.
+// ohy += a w over the P parameters, a = <r, z> / <p, q> as in pcg_xr_kernel (read
+// before the scalars move on).
+__global__ void pcg_w_kernel(size_t n, const double* __restrict__ sc, const c128* __restrict__ w,
+                             c128* __restrict__ ohy) {
+    const double a = sc[1] != 0.0 ? sc[0] / sc[1] : 0.0;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        ohy[i] = ohy[i] + a * w[i];
+}
+
+// T-form: sol = (T + shift)^{-1} rhs (dim_pad entries, zero beyond ns) and
+// ohy = O~^H sol (P entries).  steps = 0: one application of the Cholesky factor.
+// steps = s > 0: s + 1 iterations of conjugate gradients from zero, preconditioned
+// by the factor, on the exact operator T y = O~ (O~^H y) / Ns + shift y with FP64
+// sums and residuals; each iteration applies the factor once and T once, and
+// O~^H sol is accumulated from the O~^H p of those products (x = sum a_k p_k), so
+// no product over O~ is spent on the solution itself.  (Plain iterative
+// refinement x += M^{-1} (b - T x) diverges where the BF16x3 factor is a poor
+// approximation of an ill-conditioned T -- at converged parameters of the 12 x 12
+// workload its second step already moved the solution away -- while CG
+// preconditioned by the same Hermitian positive definite factor converges for any
+// such preconditioner.)  The step scalars stay on the device, so the sequence has
+// no host round trip and can be captured in a graph.
 template <typename R>
-static void t_solve(yq_sr_s* sr, const LltPlan& pl, double shift, const c128* rhs, c128* sol, int steps) {
+static void t_solve(yq_sr_s* sr, const LltPlan& pl, double shift, const c128* rhs, c128* sol, c128* ohy,
+                    int steps) {
     cudaStream_t st = sr->q->ctx->stream;
     const size_t dp = size_t(sr->dim_pad);
+    const size_t P = sr->q->P;
     const int ns = sr->ns;
     c128* b = sr->rhs.as<c128>();
     c128* tmp = sr->s2.as<c128>();
-    YQ_CUDA(cudaMemcpyAsync(b, rhs, dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
-    llt_apply(sr, pl, b, tmp, sol);
-    if (steps <= 0) return;
+    if (steps <= 0) {
+        YQ_CUDA(cudaMemcpyAsync(b, rhs, dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+        llt_apply(sr, pl, b, tmp, sol);
+        op_ohy<R>(sr, sol, 1.0, ohy, nullptr, 0.0);
+        return;
+    }
     sr->pcg.ensure(4 * dp * sizeof(c128) + 8 * sizeof(double));
     c128* r = sr->pcg.as<c128>();
     c128* z = r + dp;
     c128* p = z + dp;
     c128* q = p + dp;
     double* sc = reinterpret_cast<double*>(q + dp);
+    c128* w = sr->work_p.as<c128>();
     const unsigned g = std::min(148u * 8, cdiv_u(dp, 256));
-    auto apply_T = [&](const c128* x, c128* out) {  // out = T x (+ shift x), zero beyond ns
-        YQ_CUDA(cudaMemsetAsync(out, 0, dp * sizeof(c128), st));
-        op_ohy<R>(sr, x, 1.0, sr->work_p.as<c128>(), nullptr, 0.0);
-        op_ox<R>(sr, sr->work_p.as<c128>(), 1.0 / ns, out);
-        axpy_kernel<<<cdiv_u(ns, 256), 256, 0, st>>>(size_t(ns), mk(shift, 0.0), x, out);
-        YQ_LAUNCH_CHECK();
-    };
+    const unsigned gp = std::min(148u * 8, cdiv_u(P, 256));
     auto precond = [&](const c128* in, c128* out) {  // out = M^{-1} in (in kept)
         YQ_CUDA(cudaMemcpyAsync(out, in, dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
         llt_apply(sr, pl, out, tmp, out);
     };
-    apply_T(sol, q);
-    residual_kernel<<<g, 256, 0, st>>>(dp, rhs, q, r);
-    YQ_LAUNCH_CHECK();
+    YQ_CUDA(cudaMemcpyAsync(r, rhs, dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
+    YQ_CUDA(cudaMemsetAsync(sol, 0, dp * sizeof(c128), st));
+    YQ_CUDA(cudaMemsetAsync(ohy, 0, P * sizeof(c128), st));
     precond(r, z);
     YQ_CUDA(cudaMemcpyAsync(p, z, dp * sizeof(c128), cudaMemcpyDeviceToDevice, st));
     dot_re_kernel<<<1, 1024, 0, st>>>(dp, r, z, sc + 0);
     YQ_LAUNCH_CHECK();
-    for (int k = 0; k < steps; ++k) {
-        apply_T(p, q);
+    const int iters = steps + 1;
+    for (int k = 0; k < iters; ++k) {
+        // w = O~^H p ; q = T p = O~ w / Ns + shift p (zero beyond ns)
+        op_ohy<R>(sr, p, 1.0, w, nullptr, 0.0);
+        YQ_CUDA(cudaMemsetAsync(q, 0, dp * sizeof(c128), st));
+        op_ox<R>(sr, w, 1.0 / ns, q);
+        axpy_kernel<<<cdiv_u(ns, 256), 256, 0, st>>>(size_t(ns), mk(shift, 0.0), p, q);
         dot_re_kernel<<<1, 1024, 0, st>>>(dp, p, q, sc + 1);
         pcg_xr_kernel<<<g, 256, 0, st>>>(dp, sc, p, q, sol, r);
+        pcg_w_kernel<<<gp, 256, 0, st>>>(P, sc, w, ohy);
         YQ_LAUNCH_CHECK();
-        if (k + 1 < steps) {
+        if (k + 1 < iters) {
             precond(r, z);
             dot_re_kernel<<<1, 1024, 0, st>>>(dp, r, z, sc + 2);
             pcg_p_kernel<<<g, 256, 0, st>>>(dp, sc, z, p);
@@ -997,17 +1016,16 @@ static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps, const c128* rhs
         c128* sol = sr->s1.as<c128>();
         if (!rhs) {
             // y = (T + shift)^{-1} (E - <E>) / Ns ; v = O~^H y   (push-through identity)
-            t_solve<R>(sr, pl, shift, sr->y.as<c128>(), sol, ir_steps);
-            op_ohy<R>(sr, sol, 1.0, sr->v.as<c128>(), nullptr, 0.0);
+            t_solve<R>(sr, pl, shift, sr->y.as<c128>(), sol, sr->v.as<c128>(), ir_steps);
         } else {
             // v = (g - O~^H (T + shift)^{-1} O~ g / Ns) / shift
             sr->trhs.ensure(dp * sizeof(c128));
             c128* b = sr->trhs.as<c128>();
             YQ_CUDA(cudaMemsetAsync(b, 0, dp * sizeof(c128), st));
             op_ox<R>(sr, rhs, 1.0 / ns, b);
-            t_solve<R>(sr, pl, shift, b, sol, ir_steps);
-            op_ohy<R>(sr, sol, 1.0, sr->work_p.as<c128>(), nullptr, 0.0);
-            woodbury_kernel<<<cdiv_u(P, 256), 256, 0, st>>>(P, 1.0 / shift, rhs, sr->work_p.as<c128>(),
+            sr->ohy_sol.ensure(P * sizeof(c128));
+            t_solve<R>(sr, pl, shift, b, sol, sr->ohy_sol.as<c128>(), ir_steps);
+            woodbury_kernel<<<cdiv_u(P, 256), 256, 0, st>>>(P, 1.0 / shift, rhs, sr->ohy_sol.as<c128>(),
                                                            sr->v.as<c128>());
             YQ_LAUNCH_CHECK();
         }
@@ -1024,6 +1042,7 @@ static void solve_llt_t(yq_sr_s* sr, double shift, int ir_steps, const c128* rhs
 void sr_solve(yq_sr_s* sr, double shift, int solver, double cg_tol, int ir_steps, int* iters, double* relres) {
     if (!sr->constructed) throw Error(YQ_E_STATE, "solve: call construct first");
     YQ_CHECK_ARG(shift >= 0.0, "solve: shift must be >= 0");
+    YQ_CHECK_ARG(ir_steps <= 64, "solve: at most 64 CG steps");
     if (solver == YQ_SOLVE_CG) {
         sr->q->ctx->stage_begin(ST_SOLVE);
         if (sr->q->dtype == YQ_C64)
@@ -1061,6 +1080,7 @@ void sr_solve_runner(yq_sr_s* sr, double shift, int solver, double cg_tol, int i
                      double* cg_err) {
     if (!sr->constructed) throw Error(YQ_E_STATE, "solve: call construct first");
     YQ_CHECK_ARG(shift >= 0.0, "solve: shift must be >= 0");
+    YQ_CHECK_ARG(ir_steps <= 64, "solve: at most 64 CG steps");
     *cg_err = 0.;
     const bool c64 = sr->q->dtype == YQ_C64;
     const bool use_cg = solver == YQ_SOLVE_CG && sr->beta2 == 0.0;  // RunRBM.hpp:184
