@@ -680,9 +680,13 @@ static int tile_grid() {
 
 // Ordinary launch: tiles are handed out by the counter to running CTAs only, so the
 // grid needs no co-residency and can share the device with other work.  Small
-// matrices get a grid proportional to their tile columns.
+// matrices get a grid proportional to their tile columns: the factorisation is a
+// chain of one diagonal tile per column (~80 us each), and about 1.5 CTAs per tile
+// column keep the tiles of the current column ahead of it; every CTA beyond that
+// only waits on flags while holding an SM (one CTA per SM) that the kernels of
+// other problems sharing the device could use.
 static void launch_tiles(const TileArgs& a, int nitems, int sm_count, cudaStream_t st) {
-    const int grid = std::min({tile_grid() * sm_count, std::max(1, nitems), std::max(8, 4 * a.nt)});
+    const int grid = std::min({tile_grid() * sm_count, std::max(1, nitems), std::max(16, a.nt + a.nt / 2)});
     chol_tile_kernel<<<grid, 128, SM_TILE, st>>>(a);
     YQ_LAUNCH_CHECK();
 }
