@@ -10,9 +10,11 @@ then per iteration 8 decorrelation + 8 recorded sweeps -> 8192 samples; SR in
 the sample-space form T = O~ O~^H / Ns + 1e-3 I (Ns < P), Cholesky, SGD lr 0.01.
 
   mixed: complex64 sampling / E_loc / O, BF16x3 tcgen05 Gram with FP32
-         accumulation, FP64 Cholesky as the preconditioner of 2 CG steps with FP64
+         accumulation, panel Cholesky (FP64 tile panels, BF16x3 tcgen05 trailing
+         updates) as the preconditioner of three CG iterations with FP64
          residuals, FP64 means.
-  fp64:  complex128 end to end, FP64 SIMT Gram, FP64 Cholesky.
+  fp64:  complex128 end to end, FP64 DMMA (tensor-core m8n8k4) Gram, FP64 tile
+         Cholesky.
 
 --impl reference times the CPU restatement of the reference path (OpenMP
 oracle + numpy BLAS/LAPACK for the dense algebra) on a bounded sample of the

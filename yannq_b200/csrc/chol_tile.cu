@@ -8,7 +8,7 @@
 //   i >  j:  L_ij = F L_jj^{-H}
 // and publishes a flag.  A tile waits only on tiles with smaller numbers (left
 // columns, or the diagonal of its own column), which were handed out earlier to
-// co-resident CTAs, so the schedule cannot deadlock.  Every wait is bounded: a
+// running CTAs, so the schedule cannot deadlock.  Every wait is bounded: a
 // timeout sets DS_TIMEOUT and an abort word that makes every CTA stop.
 //
 // The solves use the same scheme with 64-row blocks: the forward sweep of block
@@ -104,22 +104,25 @@ __device__ void publish(int* flag) {
     }
 }
 
-// c (4 x 4 sub-tiles of the warp's 32 x 32 block) += A B^H over K = 4 * nk,
-// A and B read from shared memory rows (row stride lda / ldb complex).
-__device__ __forceinline__ void warp_mma(const c128* A, int lda, const c128* B, int ldb, int nk, int wm, int wn, int fr,
+// c += A B^H over K = 4 * nk for the warp's sub-tiles p < 4, q < NQ: rows
+// 8 (rb + p) .. + 7 and columns 8 (cb + q) .. + 7 of the 64 x 64 product; with
+// LOWER only the sub-tiles on or below the diagonal (p >= q, for rb == cb).  A and
+// B are read from shared memory rows (row stride lda / ldb complex).
+template <int NQ, bool LOWER>
+__device__ __forceinline__ void warp_mma(const c128* A, int lda, const c128* B, int ldb, int nk, int rb, int cb, int fr,
                                          int fk, double (&cre)[4][4][2], double (&cim)[4][4][2]) {
     for (int ks = 0; ks < nk; ++ks) {
         const int k = ks * 4 + fk;
-        double ar[4], ai[4], br[4], bi[4], bn[4];
+        double ar[4], ai[4], br[NQ], bi[NQ], bn[NQ];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const c128 v = A[(wm * 32 + i * 8 + fr) * lda + k];
+            const c128 v = A[((rb + i) * 8 + fr) * lda + k];
             ar[i] = v.re;
             ai[i] = v.im;
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const c128 v = B[(wn * 32 + j * 8 + fr) * ldb + k];
+        for (int j = 0; j < NQ; ++j) {
+            const c128 v = B[((cb + j) * 8 + fr) * ldb + k];
             br[j] = v.re;
             bi[j] = v.im;
             bn[j] = -v.im;
@@ -127,11 +130,76 @@ __device__ __forceinline__ void warp_mma(const c128* A, int lda, const c128* B, 
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                dmma(cre[i][j], ar[i], br[j]);
-                dmma(cre[i][j], ai[i], bi[j]);
-                dmma(cim[i][j], ai[i], br[j]);
-                dmma(cim[i][j], ar[i], bn[j]);
+            for (int j = 0; j < NQ; ++j) {
+                if (!LOWER || i >= j) {
+                    dmma(cre[i][j], ar[i], br[j]);
+                    dmma(cre[i][j], ai[i], bi[j]);
+                    dmma(cim[i][j], ai[i], br[j]);
+                    dmma(cim[i][j], ar[i], bn[j]);
+                }
+            }
+    }
+}
+
+// Sub-tiles of a warp in the sums F = A_ij - sum_k L_ik L_jk^H.  Off-diagonal
+// tiles: warp (wm, wn) owns the 32 x 32 block (wm, wn) (kind 0).  Diagonal tiles
+// need only the lower triangle, 36 of the 64 sub-tiles, spread 10 / 10 / 8 / 8
+// over the warps: the two diagonal 32 x 32 blocks' lower halves (kind 1) and the
+// lower-left block as two 32 x 16 halves (kind 2), so the critical diagonal update
+// costs 10 sub-tile products per warp instead of 16.
+struct WarpTiles {
+    int rb, cb, kind;
+    __device__ __forceinline__ int nq() const { return kind == 2 ? 2 : 4; }
+    __device__ __forceinline__ bool has(int p, int q) const { return q < nq() && (kind != 1 || p >= q); }
+};
+__device__ __forceinline__ WarpTiles warp_tiles(int warp, bool diag) {
+    if (!diag) return WarpTiles{4 * (warp >> 1), 4 * (warp & 1), 0};
+    if (warp < 2) return WarpTiles{4 * warp, 4 * warp, 1};
+    return WarpTiles{4, 2 * (warp - 2), 2};
+}
+__device__ __forceinline__ void warp_mma_tiles(const WarpTiles& wt, const c128* A, int lda, const c128* B, int ldb,
+                                               int nk, int fr, int fk, double (&cre)[4][4][2],
+                                               double (&cim)[4][4][2]) {
+    if (wt.kind == 0) warp_mma<4, false>(A, lda, B, ldb, nk, wt.rb, wt.cb, fr, fk, cre, cim);
+    else if (wt.kind == 1) warp_mma<4, true>(A, lda, B, ldb, nk, wt.rb, wt.cb, fr, fk, cre, cim);
+    else warp_mma<2, false>(A, lda, B, ldb, nk, wt.rb, wt.cb, fr, fk, cre, cim);
+}
+
+// L_ij = F X^H with X = L_jj^{-1} lower triangular: column block cb (columns
+// 8 cb .. 8 cb + 7) sums over k < 8 (cb + 1) only.  Warp w owns the column blocks
+// 7 - w and w over all 64 rows, 9 blocks of K work for every warp, 576 DMMA per
+// warp instead of 1024 for the full product.
+__device__ __forceinline__ void trsm_mma(const c128* F, const c128* X, int warp, int fr, int fk,
+                                         double (&cre)[8][2][2], double (&cim)[8][2][2]) {
+    const int cbs[2] = {7 - warp, warp};
+    const int nk0 = 2 * (8 - warp), nk1 = 2 * (warp + 1);
+    for (int ks = 0; ks < nk0; ++ks) {
+        const int k = ks * 4 + fk;
+        const bool two = ks < nk1;
+        double ar[8], ai[8], br[2], bi[2], bn[2];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const c128 v = F[(i * 8 + fr) * FLS + k];
+            ar[i] = v.re;
+            ai[i] = v.im;
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const c128 v = (j == 0 || two) ? X[(cbs[j] * 8 + fr) * FLS + k] : mk(0., 0.);
+            br[j] = v.re;
+            bi[j] = v.im;
+            bn[j] = -v.im;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                if (j == 0 || two) {
+                    dmma(cre[i][j], ar[i], br[j]);
+                    dmma(cre[i][j], ai[i], bi[j]);
+                    dmma(cim[i][j], ai[i], br[j]);
+                    dmma(cim[i][j], ar[i], bn[j]);
+                }
             }
     }
 }
@@ -151,55 +219,59 @@ __device__ __forceinline__ void warp_mma(const c128* A, int lda, const c128* B, 
 // r = l >> 2 and columns q0 = l & 3, q1 = q0 + 4.  Right-looking factorisation:
 // per column one pivot broadcast and three complex shuffles (the column entries of
 // this lane's row and of its two columns), then the rank-1 update of the lane's
-// elements; the inverse by right-looking substitution from the identity (row k
-// is final after its scaling by 1 / L_kk, then rows below subtract L_rk X_k).
-__device__ __forceinline__ void leaf8(c128* F, c128* X, int o, int* status) {
+// elements, e -= a_rc conj(a_qc) / d with the product formed before the pivot's
+// reciprocal square root is known; the inverse by right-looking substitution from
+// the identity (row k is final after its scaling by 1 / L_kk, then rows below
+// subtract L_rk X_k).  Every lane takes the same instruction stream (selects, no
+// divergent branches), and the function is not inlined, so the leaves of one
+// factorisation run one copy of the code that stays in the instruction cache:
+// single-warp timings on a B200, 4.8k cycles per leaf with branches and inlined
+// at each call site, 3.1k in this form once its code is cached.
+__device__ __noinline__ void leaf8(c128* F, c128* X, int o, int* status) {
     const int lane = threadIdx.x & 31, r = lane >> 2, q0 = lane & 3;
     const int qq[2] = {q0, q0 + 4};
     c128 e[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) e[h] = qq[h] <= r ? F[(o + r) * FLS + o + qq[h]] : mk(0., 0.);
     double sc[8];  // 1 / L_cc
+    bool bad = false;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         const int hc = c >> 2, lc = c & 3;
         double d = __shfl_sync(0xffffffffu, e[hc].re, 4 * c + lc);
-        if (!(d > 0.0)) {
-            if (lane == 0) atomicOr(status, DS_NOT_PD);
-            d = 1.0;  // unit pivot keeps the launch well defined
-        }
+        bad |= !(d > 0.0);
+        d = d > 0.0 ? d : 1.0;  // unit pivot keeps the launch well defined
         const double s = rsqrt(d);
         sc[c] = s;
-        c128 arc, aqc[2];
-        arc.re = __shfl_sync(0xffffffffu, e[hc].re, 4 * r + lc);
-        arc.im = __shfl_sync(0xffffffffu, e[hc].im, 4 * r + lc);
+        const double are = __shfl_sync(0xffffffffu, e[hc].re, 4 * r + lc);
+        const double aim = __shfl_sync(0xffffffffu, e[hc].im, 4 * r + lc);
+        double pre[2], pim[2];  // a_rc conj(a_qc)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            aqc[h].re = __shfl_sync(0xffffffffu, e[hc].re, 4 * qq[h] + lc);
-            aqc[h].im = __shfl_sync(0xffffffffu, e[hc].im, 4 * qq[h] + lc);
+            const double bre = __shfl_sync(0xffffffffu, e[hc].re, 4 * qq[h] + lc);
+            const double bim = __shfl_sync(0xffffffffu, e[hc].im, 4 * qq[h] + lc);
+            pre[h] = are * bre + aim * bim;
+            pim[h] = aim * bre - are * bim;
         }
-        const c128 Lrc = s * arc;
+        const double s2 = s * s;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int q = qq[h];
-            if (q == c) {
-                if (r == c) e[h] = mk(d * s, 0.0);
-                else if (r > c) e[h] = Lrc;
-            } else if (q > c && r >= q) {
-                e[h] = e[h] - Lrc * conj(s * aqc[h]);
-            }
+            const c128 upd = mk(fma(-s2, pre[h], e[h].re), fma(-s2, pim[h], e[h].im));
+            const c128 col = r == c ? mk(d * s, 0.0) : (r > c ? mk(s * are, s * aim) : e[h]);
+            e[h] = (q > c && r >= q) ? upd : (q == c ? col : e[h]);
         }
     }
+    if (bad && lane == 0) atomicOr(status, DS_NOT_PD);
     c128 y[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) y[h] = mk(qq[h] == r ? 1.0 : 0.0, 0.0);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int hk = k >> 2, lk = k & 3;
-        if (r == k) {
+        const double f = r == k ? sc[k] : 1.0;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) y[h] = sc[k] * y[h];
-        }
+        for (int h = 0; h < 2; ++h) y[h] = f * y[h];
         c128 lrk, xk[2];
         lrk.re = __shfl_sync(0xffffffffu, e[hk].re, 4 * r + lk);
         lrk.im = __shfl_sync(0xffffffffu, e[hk].im, 4 * r + lk);
@@ -208,9 +280,10 @@ __device__ __forceinline__ void leaf8(c128* F, c128* X, int o, int* status) {
             xk[h].re = __shfl_sync(0xffffffffu, y[h].re, 4 * k + q0);
             xk[h].im = __shfl_sync(0xffffffffu, y[h].im, 4 * k + q0);
         }
-        if (r > k) {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) y[h] = y[h] - lrk * xk[h];
+        for (int h = 0; h < 2; ++h) {
+            const c128 nv = y[h] - lrk * xk[h];
+            y[h] = r > k ? nv : y[h];
         }
     }
 #pragma unroll
@@ -323,7 +396,7 @@ __global__ void __launch_bounds__(128, 1) chol_tile_kernel(TileArgs a) {
     c128* T = X + TB * FLS;
     __shared__ int s_item, s_ok;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int wm = warp >> 1, wn = warp & 1, fr = lane >> 2, fk = lane & 3;
+    const int fr = lane >> 2, fk = lane & 3;
     for (;;) {
         if (tid == 0) s_item = ld_acquire(a.S.abort_word) ? a.nitems : atomicAdd(a.counter, 1);
         __syncthreads();
@@ -331,6 +404,11 @@ __global__ void __launch_bounds__(128, 1) chol_tile_kernel(TileArgs a) {
         __syncthreads();
         if (w >= a.nitems) break;
         const int i = a.items[w].x, j = a.items[w].y;
+        const WarpTiles wt = warp_tiles(warp, i == j);
+        // A_ij is read once the sum over k is done: start bringing it into L2 now
+        // (64 rows of 1 KiB, one 128-byte line per thread and step).
+        for (int e = tid; e < TB * 8; e += blockDim.x)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(a.G + size_t(i * TB + (e >> 3)) * a.ld + j * TB + (e & 7) * 8));
         double cre[4][4][2], cim[4][4][2];
 #pragma unroll
         for (int p = 0; p < 4; ++p)
@@ -369,34 +447,41 @@ __global__ void __launch_bounds__(128, 1) chol_tile_kernel(TileArgs a) {
                 cpa_wait_all();
             }
             __syncthreads();
-            warp_mma(&As[buf][0][0], SLS, &Bs[buf][0][0], SLS, KC / 4, wm, wn, fr, fk, cre, cim);
+            warp_mma_tiles(wt, &As[buf][0][0], SLS, &Bs[buf][0][0], SLS, KC / 4, fr, fk, cre, cim);
             __syncthreads();
         }
         cpa_wait_all();
         __syncthreads();
         if (!ok) break;
+        // (a diagonal tile's sub-tiles above its diagonal are left unset: the
+        // factorisation reads and writes back only the lower triangle)
 #pragma unroll
         for (int p = 0; p < 4; ++p)
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < 4; ++q) {
+                if (!wt.has(p, q)) continue;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const int r = wm * 32 + p * 8 + fr, c = wn * 32 + q * 8 + 2 * fk + h;
+                    const int r = (wt.rb + p) * 8 + fr, c = (wt.cb + q) * 8 + 2 * fk + h;
                     const c128 g = a.G[size_t(i * TB + r) * a.ld + j * TB + c];
                     F[r * FLS + c] = mk(g.re - cre[p][q][h], g.im - cim[p][q][h]);
                 }
+            }
         __syncthreads();
         if (i == j) {
             factor_tile(F, X, T, a.S.status);
             c128* Li = a.Linv + size_t(j) * TB * TB;
             c128* LiH = a.LinvH + size_t(j) * TB * TB;
+            // The column's other tiles read only L_jj^{-1}: it is published first.
+            // L_jj itself and L_jj^{-H} serve the triangular solves, which run
+            // after this launch.
+            for (int e = tid; e < TB * TB; e += blockDim.x) Li[e] = X[(e / TB) * FLS + e % TB];
+            publish(&a.flags[j * a.nt + j]);
             for (int e = tid; e < TB * TB; e += blockDim.x) {
                 const int r = e / TB, c = e % TB;
                 if (c <= r) a.G[size_t(j * TB + r) * a.ld + j * TB + c] = F[r * FLS + c];
-                Li[e] = X[r * FLS + c];
                 LiH[e] = conj(X[c * FLS + r]);
             }
-            publish(&a.flags[j * a.nt + j]);
         } else {
             if (!wait_flag(&a.flags[j * a.nt + j], a.S, &s_ok)) break;
             // X <- L_jj^{-1} (rows r, K-contiguous): L_ij = F (L_jj^{-1})^H
@@ -408,19 +493,20 @@ __global__ void __launch_bounds__(128, 1) chol_tile_kernel(TileArgs a) {
             cpa_commit();
             cpa_wait_all();
             __syncthreads();
+            double tre[8][2][2], tim[8][2][2];
 #pragma unroll
-            for (int p = 0; p < 4; ++p)
+            for (int p = 0; p < 8; ++p)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) cre[p][q][0] = cre[p][q][1] = cim[p][q][0] = cim[p][q][1] = 0.0;
-            warp_mma(F, FLS, X, FLS, TB / 4, wm, wn, fr, fk, cre, cim);
+                for (int q = 0; q < 2; ++q) tre[p][q][0] = tre[p][q][1] = tim[p][q][0] = tim[p][q][1] = 0.0;
+            trsm_mma(F, X, warp, fr, fk, tre, tim);
 #pragma unroll
-            for (int p = 0; p < 4; ++p)
+            for (int p = 0; p < 8; ++p)
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
+                for (int q = 0; q < 2; ++q)
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
-                        const int r = wm * 32 + p * 8 + fr, c = wn * 32 + q * 8 + 2 * fk + h;
-                        a.G[size_t(i * TB + r) * a.ld + j * TB + c] = mk(cre[p][q][h], cim[p][q][h]);
+                        const int r = p * 8 + fr, c = (q == 0 ? 7 - warp : warp) * 8 + 2 * fk + h;
+                        a.G[size_t(i * TB + r) * a.ld + j * TB + c] = mk(tre[p][q][h], tim[p][q][h]);
                     }
             publish(&a.flags[i * a.nt + j]);
         }
