@@ -326,6 +326,71 @@ __device__ __forceinline__ void tile_prod(c128* out, const c128* A, const c128* 
     }
 }
 
+// The four products of the top level (H = 32, four warps) with their triangular
+// shapes: the zero halves of L11^{-1} and L22^{-1} are skipped and the Hermitian
+// update forms only its lower 8 x 8 tiles, so each warp issues at most 24 of the
+// 32 tile k-steps of a full product (a full 32^3 product took 2.7k cycles on one
+// SM).  Work per 8 x 8 output tile (ti, tj), in k-steps of 4:
+//   P_UPPER_BH  out = A X^H, X lower:  k < 8 (tj + 1)   warp w owns row ti = w
+//   P_LOWER_B   out = A X,   X lower:  k >= 8 tj         warp w owns row ti = w
+//   P_LLOWER_B  out = X B,   X lower:  k < 8 (ti + 1)    warp w owns column tj = w
+// (each warp 20 k-steps), and P_HERM out += alpha A A^H for ti >= tj (3 / 3 / 2 / 2
+// tiles per warp of 8 k-steps each).
+enum { P_UPPER_BH = 0, P_HERM = 1, P_LOWER_B = 2, P_LLOWER_B = 3 };
+template <int MODE>
+__device__ __forceinline__ void tile_prod32(c128* out, const c128* A, const c128* B, double alpha, bool acc) {
+    constexpr int H = 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fk = lane & 3;
+    // P_HERM tile lists, 4 ti + tj in 4 bits per tile, 12 bits per warp: warp 0
+    // (0,0) (1,0) (1,1); warp 1 (2,0) (2,1) (2,2); warp 2 (3,0) (3,1); warp 3 (3,2) (3,3)
+    constexpr unsigned long long herm_tiles = 0xfe0dca98540ull;
+    int ti[4], tj[4], lo[4], hi[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        if (MODE == P_UPPER_BH) { ti[u] = warp; tj[u] = u; lo[u] = 0; hi[u] = 2 * (u + 1); }
+        else if (MODE == P_LOWER_B) { ti[u] = warp; tj[u] = u; lo[u] = 2 * u; hi[u] = H / 4; }
+        else if (MODE == P_LLOWER_B) { ti[u] = u; tj[u] = warp; lo[u] = 0; hi[u] = 2 * (u + 1); }
+        else {
+            const bool on = u < (warp < 2 ? 3 : 2);
+            const int code = on ? int((herm_tiles >> (12 * warp + 4 * u)) & 15u) : 0;
+            ti[u] = code >> 2;
+            tj[u] = code & 3;
+            lo[u] = 0;
+            hi[u] = on ? H / 4 : 0;
+        }
+    }
+    double cre[4][2], cim[4][2];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) cre[u][0] = cre[u][1] = cim[u][0] = cim[u][1] = 0.;
+#pragma unroll
+    for (int ks = 0; ks < H / 4; ++ks) {
+        const int k = ks * 4 + fk;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (ks >= lo[u] && ks < hi[u]) {
+                const c128 a = A[(ti[u] * 8 + fr) * FLS + k];
+                const c128 b = (MODE == P_UPPER_BH || MODE == P_HERM) ? conj(B[(tj[u] * 8 + fr) * FLS + k])
+                                                                     : B[k * FLS + tj[u] * 8 + fr];
+                dmma(cre[u], a.re, b.re);
+                dmma(cre[u], -a.im, b.im);
+                dmma(cim[u], a.re, b.im);
+                dmma(cim[u], a.im, b.re);
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        if (hi[u] > lo[u]) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                c128* po = out + (ti[u] * 8 + fr) * FLS + tj[u] * 8 + 2 * fk + h;
+                const c128 v = mk(alpha * cre[u][h], alpha * cim[u][h]);
+                *po = acc ? *po + v : v;
+            }
+        }
+    }
+}
+
 template <int N>
 __device__ __forceinline__ void level_sync() {
     if (N <= 16) __syncwarp();
@@ -349,18 +414,22 @@ __device__ void chol_rec(c128* F, c128* X, c128* T, int o, int* status) {
         c128* W = T + o * FLS + o + H;       // upper scratch: L21 X11
         chol_rec<H>(F, X, T, o, status);
         level_sync<N>();
-        if (active) tile_prod<H, OP_BH>(L21, A21, X11, 1.0, false, nw);
+        if constexpr (H == 32) tile_prod32<P_UPPER_BH>(L21, A21, X11, 1.0, false);
+        else if (active) tile_prod<H, OP_BH>(L21, A21, X11, 1.0, false, nw);
         level_sync<N>();
         if (active) {
             for (int e = threadIdx.x; e < H * H; e += 32 * nw) A21[(e / H) * FLS + e % H] = L21[(e / H) * FLS + e % H];
-            tile_prod<H, OP_BH>(A22, L21, L21, -1.0, true, nw);
+            if constexpr (H == 32) tile_prod32<P_HERM>(A22, L21, L21, -1.0, true);
+            else tile_prod<H, OP_BH>(A22, L21, L21, -1.0, true, nw);
         }
         level_sync<N>();
         chol_rec<H>(F, X, T, o + H, status);
         level_sync<N>();
-        if (active) tile_prod<H, OP_B>(W, L21, X11, 1.0, false, nw);
+        if constexpr (H == 32) tile_prod32<P_LOWER_B>(W, L21, X11, 1.0, false);
+        else if (active) tile_prod<H, OP_B>(W, L21, X11, 1.0, false, nw);
         level_sync<N>();
-        if (active) tile_prod<H, OP_B>(X21, X22, W, -1.0, false, nw);
+        if constexpr (H == 32) tile_prod32<P_LLOWER_B>(X21, X22, W, -1.0, false);
+        else if (active) tile_prod<H, OP_B>(X21, X22, W, -1.0, false, nw);
         level_sync<N>();
     }
 }
