@@ -453,6 +453,10 @@ struct TileArgs {
     int* counter;
     int* flags;  // nt x nt
     Sync S;
+    // BF16 planes of the panel's rows below it for the trailing update (null: none):
+    // row i TB + r - r0, K index (j - kbeg) TB + c and kp / 2 + that (kp = 2 x panel width)
+    uint16_t *xh, *xl, *yh, *yl;
+    int r0, kp;
 };
 
 __global__ void __launch_bounds__(128, 1) chol_tile_kernel(TileArgs a) {
@@ -577,6 +581,32 @@ __global__ void __launch_bounds__(128, 1) chol_tile_kernel(TileArgs a) {
                         const int r = p * 8 + fr, c = (q == 0 ? 7 - warp : warp) * 8 + 2 * fk + h;
                         a.G[size_t(i * TB + r) * a.ld + j * TB + c] = mk(tre[p][q][h], tim[p][q][h]);
                     }
+            if (a.xh && i * TB >= a.r0) {
+                // The trailing update's operands straight from the registers: X = [Re | Im],
+                // Y = [Im | -Re] of the FP64 values rounded to FP32, each split into BF16 hi + lo;
+                // the two adjacent columns of a lane go out as one 4-byte store per plane.
+                const int hk = a.kp >> 1;
+#pragma unroll
+                for (int p = 0; p < 8; ++p)
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const int r = p * 8 + fr, c = (q == 0 ? 7 - warp : warp) * 8 + 2 * fk;
+                        const size_t e = size_t(i * TB + r - a.r0) * a.kp + size_t(j - a.kbeg) * TB + c;
+                        uint16_t h0, l0, h1, l1;
+                        auto put = [&](uint16_t* hi, uint16_t* lo, size_t at, float v0, float v1) {
+                            split_bf16(v0, h0, l0);
+                            split_bf16(v1, h1, l1);
+                            *reinterpret_cast<uint32_t*>(hi + at) = uint32_t(h0) | (uint32_t(h1) << 16);
+                            *reinterpret_cast<uint32_t*>(lo + at) = uint32_t(l0) | (uint32_t(l1) << 16);
+                        };
+                        const float re0 = float(tre[p][q][0]), re1 = float(tre[p][q][1]);
+                        const float im0 = float(tim[p][q][0]), im1 = float(tim[p][q][1]);
+                        put(a.xh, a.xl, e, re0, re1);
+                        put(a.xh, a.xl, e + hk, im0, im1);
+                        put(a.yh, a.yl, e, im0, im1);
+                        put(a.yh, a.yl, e + hk, -re0, -re1);
+                    }
+            }
             publish(&a.flags[i * a.nt + j]);
         }
     }
@@ -884,15 +914,22 @@ void chol_factor_panels(c128* G, int n, size_t ld, c128* Linv, c128* LinvH, int*
         const int j1 = std::min(nt, j0 + pw);
         int count = 0;
         for (int j = j0; j < j1; ++j) count += nt - j;
+        // the panel's rows below it go to the trailing update, whose BF16 planes
+        // (K = 2 w) the panel's tiles write as they form those rows; the planes'
+        // padding rows (n2 .. rows_pad) are zeroed here
+        const int r0 = j1 * TB, n2 = n - r0, w = (j1 - j0) * TB;
+        const size_t rows_pad = ((size_t(std::max(n2, 1)) + TC_BM - 1) / TC_BM) * TC_BM;
+        const bool trail = j1 < nt;
+        if (trail && rows_pad > size_t(n2)) {
+            const size_t off = size_t(n2) * 2 * w, cnt = (rows_pad - size_t(n2)) * 2 * w * sizeof(uint16_t);
+            for (uint16_t* pl : {xh, xl, yh, yl}) YQ_CUDA(cudaMemsetAsync(pl + off, 0, cnt, st));
+        }
         TileArgs a{G, ld, nt, j0, Linv, LinvH, sc.items + first, count, sc.panel_counters + p, sc.flags,
-                   Sync{status, sc.words + 1, 1u << 24}};
+                   Sync{status, sc.words + 1, 1u << 24}, trail ? xh : nullptr, xl, yh, yl, r0, 2 * w};
         launch_tiles(a, count, sm_count, st);
         first += count;
-        if (j1 == nt) break;
+        if (!trail) break;
         // trailing update  G[r0:, r0:] -= L21 L21^H  on the tensor cores
-        const int r0 = j1 * TB, n2 = n - r0, w = (j1 - j0) * TB;
-        const size_t rows_pad = ((size_t(n2) + TC_BM - 1) / TC_BM) * TC_BM;
-        herk_tc_split_block(G, ld, r0, j0 * TB, n2, w, rows_pad, xh, xl, yh, yl, st);
         herk_tc_launch(xh, xl, yh, yl, n2, rows_pad, size_t(2 * w), G + size_t(r0) * ld + r0, ld, -1.0, 0.0, true,
                        status, sm_count, nullptr, tc_split_enabled() ? split_ws : nullptr, TRAIL_SPLIT_BYTES, st);
     }

@@ -29,15 +29,6 @@
 namespace yq {
 
 // ---------------------------------------------------------------------------
-// Operand split: X = [Re | Im], Y = [Im | -Re]; x = hi + lo with hi = bf16(x),
-// lo = bf16(x - hi).
-__device__ __forceinline__ void split_bf16(float v, uint16_t& hi, uint16_t& lo) {
-    __nv_bfloat16 h = __float2bfloat16_rn(v);
-    __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
-    hi = __bfloat16_as_ushort(h);
-    lo = __bfloat16_as_ushort(l);
-}
-
 // Row s of O~ (the O writer's centred value, complex64) and its four planes:
 // k = p holds (Re, Im), k = P + p holds (Im, -Re); rows >= ns and k >= 2P are zero.
 __global__ void o_and_operands_kernel(int n, int m, bool bias, size_t P, int ns, size_t rows_pad, size_t kpad,
@@ -175,41 +166,6 @@ void gram_tc_write_o_and_operands(int n, int m, bool bias, size_t P, int ns, con
     }
     dim3 g(std::min<unsigned>(64u, cdiv_u(P, 256)), unsigned(std::min<size_t>(rows, 65535)));
     o_and_operands_kernel<<<g, 256, 0, st>>>(n, m, bias, P, ns, rows, kpad, sigma, t, oloc, O, xh, xl, yh, yl);
-    YQ_LAUNCH_CHECK();
-}
-
-// Block split of a complex FP64 panel (the L21 of the Cholesky), K = 2 w.
-__global__ void split_block_kernel(const c128* __restrict__ G, size_t ld, int r0, int c0, int n, int w,
-                                   size_t rows_pad, uint16_t* __restrict__ xh, uint16_t* __restrict__ xl,
-                                   uint16_t* __restrict__ yh, uint16_t* __restrict__ yl) {
-    const size_t kp = size_t(2 * w);
-    const size_t total = rows_pad * kp;
-    for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < total; q += size_t(gridDim.x) * blockDim.x) {
-        const size_t row = q / kp;
-        const int k = int(q - row * kp);
-        float xv = 0.f, yv = 0.f;
-        if (row < size_t(n)) {
-            const int c = k < w ? k : k - w;
-            const c128 v = G[(size_t(r0) + row) * ld + size_t(c0) + c];
-            xv = float(k < w ? v.re : v.im);
-            yv = float(k < w ? v.im : -v.re);
-        }
-        uint16_t a, b;
-        split_bf16(xv, a, b);
-        xh[q] = a;
-        xl[q] = b;
-        split_bf16(yv, a, b);
-        yh[q] = a;
-        yl[q] = b;
-    }
-}
-
-void herk_tc_split_block(const c128* G, size_t ld, int r0, int c0, int n, int w, size_t rows_pad, uint16_t* xh,
-                         uint16_t* xl, uint16_t* yh, uint16_t* yl, cudaStream_t st) {
-    YQ_CHECK_ARG(w > 0 && w % 32 == 0 && rows_pad % TC_BM == 0 && size_t(n) <= rows_pad, "herk split: block shape");
-    const size_t total = rows_pad * size_t(2 * w);
-    split_block_kernel<<<std::max(1u, std::min(148u * 16, cdiv_u(total, 256))), 256, 0, st>>>(G, ld, r0, c0, n, w,
-                                                                                              rows_pad, xh, xl, yh, yl);
     YQ_LAUNCH_CHECK();
 }
 

@@ -7,12 +7,23 @@
 // Gram matrix T = O~ O~^H / Ns + shift I and applies the trailing updates
 // C -= L21 L21^H of the panel Cholesky.
 #pragma once
+#include <cuda_bf16.h>
+
 #include <cstddef>
 #include <cstdint>
 
 #include "common.cuh"
 
 namespace yq {
+
+// Operand split: X = [Re | Im], Y = [Im | -Re]; x = hi + lo with hi = bf16(x),
+// lo = bf16(x - hi).
+__device__ __forceinline__ void split_bf16(float v, uint16_t& hi, uint16_t& lo) {
+    __nv_bfloat16 h = __float2bfloat16_rn(v);
+    __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+}
 
 constexpr int TC_BM = 128;  // rows of a tile (TMEM lanes)
 constexpr int TC_BK = 64;   // K per stage: 64 BF16 = one 128-byte swizzle atom row
@@ -53,10 +64,5 @@ void herk_tc_launch(const uint16_t* xh, const uint16_t* xl, const uint16_t* yh, 
                     size_t rows_pad, size_t kpad, c128* C, size_t ldc, double alpha, double shift, bool accumulate,
                     int* d_status, int sm_count, DevBuf* ws, float2* ws_fixed, size_t ws_fixed_bytes,
                     cudaStream_t st);
-
-// Split the complex FP64 block G[r0 .. r0 + n), [c0 .. c0 + w) (row stride ld) into
-// the four planes with K = 2 w; rows n .. rows_pad are written as zeros.
-void herk_tc_split_block(const c128* G, size_t ld, int r0, int c0, int n, int w, size_t rows_pad, uint16_t* xh,
-                         uint16_t* xl, uint16_t* yh, uint16_t* yl, cudaStream_t st);
 
 }  // namespace yq
