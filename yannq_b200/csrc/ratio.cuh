@@ -102,18 +102,36 @@ __device__ __forceinline__ cplx<R> factor2(cplx<R> tj, cplx<R> tx, cplx<R> ty, R
 }
 
 // prod_j (1 - s_k t_j tau_jk) with tau given transposed (tauT[j * n + k]); t and theta
-// with stride ts; W column-major (m x n).
+// with stride ts; W column-major (m x n).  For complex64 the tau loads of four
+// consecutive units are issued before their factors are formed (the rare
+// re-evaluation in logcosh form is a call the compiler does not move loads across):
+// E_loc of the 12 x 12 workload 0.95 -> 0.82 ms.  Complex128 keeps one unit at a time
+// (four raised its registers to 112 and its E_loc from 0.99 to 1.13 ms).  The
+// product keeps its order either way.
+template <typename R>
+struct ProdUnroll {
+    static constexpr int value = sizeof(R) == 4 ? 4 : 1;
+};
 template <typename R>
 __device__ __forceinline__ ScaledProd<R> prod1(int k, R sk, int n, int m, const cplx<R>* t, const cplx<R>* th,
                                               int ts, const cplx<R>* tauT, const cplx<R>* W) {
+    constexpr int PU = ProdUnroll<R>::value;
     ScaledProd<R> P;
     P.init();
-    for (int j = 0; j < m; ++j) {
-        bool ex;
-        cplx<R> d = factor1<R>(t[size_t(j) * ts], tauT[size_t(j) * n + k], sk, th[size_t(j) * ts],
-                               W + size_t(k) * m + j, ex);
-        P.p = P.p * d;
-        renorm_if(P, j, RenormChunk<R>::mask);
+    for (int j0 = 0; j0 < m; j0 += PU) {
+        cplx<R> tv[PU];
+#pragma unroll
+        for (int u = 0; u < PU; ++u) tv[u] = j0 + u < m ? tauT[size_t(j0 + u) * n + k] : one<R>();
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const int j = j0 + u;
+            if (j < m) {
+                bool ex;
+                cplx<R> d = factor1<R>(t[size_t(j) * ts], tv[u], sk, th[size_t(j) * ts], W + size_t(k) * m + j, ex);
+                P.p = P.p * d;
+                renorm_if(P, j, RenormChunk<R>::mask);
+            }
+        }
     }
     P.renorm();
     return P;
@@ -122,16 +140,28 @@ __device__ __forceinline__ ScaledProd<R> prod1(int k, R sk, int n, int m, const 
 template <typename R>
 __device__ __forceinline__ ScaledProd<R> prod2(int k, R sk, int l, R sl, int n, int m, const cplx<R>* t,
                                               const cplx<R>* th, int ts, const cplx<R>* tauT, const cplx<R>* W) {
+    constexpr int PU = ProdUnroll<R>::value;
     ScaledProd<R> P;
     P.init();
-    for (int j = 0; j < m; ++j) {
-        cplx<R> tx = sk * tauT[size_t(j) * n + k];
-        cplx<R> ty = sl * tauT[size_t(j) * n + l];
-        bool ex;
-        cplx<R> d = factor2<R>(t[size_t(j) * ts], tx, ty, sk, sl, th[size_t(j) * ts], W + size_t(k) * m + j,
-                               W + size_t(l) * m + j, ex);
-        P.p = P.p * d;
-        renorm_if(P, j, RenormChunk<R>::mask);
+    for (int j0 = 0; j0 < m; j0 += PU) {
+        cplx<R> tk[PU], tl[PU];
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            tk[u] = j0 + u < m ? tauT[size_t(j0 + u) * n + k] : one<R>();
+            tl[u] = j0 + u < m ? tauT[size_t(j0 + u) * n + l] : one<R>();
+        }
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const int j = j0 + u;
+            if (j < m) {
+                const cplx<R> tx = sk * tk[u], ty = sl * tl[u];
+                bool ex;
+                cplx<R> d = factor2<R>(t[size_t(j) * ts], tx, ty, sk, sl, th[size_t(j) * ts], W + size_t(k) * m + j,
+                                       W + size_t(l) * m + j, ex);
+                P.p = P.p * d;
+                renorm_if(P, j, RenormChunk<R>::mask);
+            }
+        }
     }
     P.renorm();
     return P;
