@@ -77,16 +77,27 @@ __global__ void __launch_bounds__(256) oloc_partial_kernel(int n, int m, int ns,
     if (i0 > n || j > m) return;
     const int s0 = split * chunk, s1 = min(ns, s0 + chunk);
     double ar[4] = {0., 0., 0., 0.}, ai[4] = {0., 0., 0., 0.};
+    // the four spins of a thread as one 4-byte load when the rows allow it (n a
+    // multiple of 4, all four inside the row); the spin row is the same for the
+    // warp's 32 threads
+    const bool packed = (n & 3) == 0 && i0 + 4 <= n;
     for (int s = s0; s < s1; ++s) {
         const cplx<R> tv = (j < m) ? t[size_t(s) * m + j] : mk(R(1), R(0));
         const double tr = double(tv.re), ti = double(tv.im);
         const int8_t* sg = sigma + size_t(s) * n;
+        double sv[4];
+        if (packed) {
+            const uint32_t w = *reinterpret_cast<const uint32_t*>(sg + i0);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) sv[k] = double(int8_t((w >> (8 * k)) & 0xffu));
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) sv[k] = (i0 + k < n) ? double(sg[i0 + k]) : 1.0;
+        }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const int i = i0 + k;
-            const double sv = (i < n) ? double(sg[i]) : 1.0;
-            ar[k] += sv * tr;
-            ai[k] += sv * ti;
+            ar[k] += sv[k] * tr;
+            ai[k] += sv[k] * ti;
         }
     }
 #pragma unroll
