@@ -57,11 +57,14 @@ def test_forward_and_adjoint_match_oracle(ctx, orc):
     f.close()
 
 
-def test_adjoint_vs_central_differences(ctx, orc):
+@pytest.mark.parametrize("net_seed,cfg_seed", [(5, 1), (11, 2), (23, 3), (37, 4)])
+def test_adjoint_vs_central_differences(ctx, orc, net_seed, cfg_seed):
+    """The adjoint row against central differences of the oracle's forward pass,
+    for several networks and spin configurations."""
     from yannq_b200 import api
 
-    f, p = _net(api, ctx, seed=5)
-    rng = np.random.default_rng(1)
+    f, p = _net(api, ctx, seed=net_seed)
+    rng = np.random.default_rng(cfg_seed)
     s = rng.choice(np.array([-1, 1], np.int8), size=(1, L))
     f.set_batch(s)
     f.forward()
